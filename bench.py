@@ -1,0 +1,309 @@
+"""Benchmark: particle-steps/s of the SMC filter on the SEIR 20x2 workload.
+
+One step = one complete particle filter over the workload (J particles, T
+observation intervals of K Euler substeps, weighting, log-sum-exp
+normalisation, systematic resampling and log-likelihood accumulation at every
+interval).  ``value`` is measured with the inputs resident in HBM (a captured
+plan replayed), ``e2e`` through the one-shot C-ABI call plomgpu_smc_run with
+host buffers (upload of every input, run, download of the results).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload seir20x2|sir]
+
+With torchrun (N > 1) every rank runs an independent filter (replicas, no
+collective in the data path); time is the max over ranks.
+"""
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, 'iterated-inference-pipeline_b200'))
+
+WORKLOADS = {
+    # name: (model library, J, observation intervals, dt in days)
+    'seir20x2': ('seir20x2', 100000, 520, 1.0),
+    'sir': ('sir', 1000, 52, 1.0),
+}
+METRIC = 'particle-steps/s at matched loglik error'
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+def workload_problem(name, precision=32, seed=0, J=None, nb_obs=-1):
+    from plomgpu import workloads, model, problem
+    lib, J0, T, dt = WORKLOADS[name]
+    c, p, l, th = workloads.load(lib)
+    m = model.PlomModel(c, p, l)
+    return problem.Problem(m, m.settings(), th, J=J or J0, dt=dt, precision=precision, seed=seed, nb_obs=nb_obs)
+
+
+def state_words(prob):
+    m = prob.model
+    return len(m.par_sv) * m.N_CAC + len(m.drift_par_proc) * m.N_CAC + m.N_TS_INC_UNIQUE
+
+
+def bytes_per_particle_step(prob, b_state):
+    # algorithmic bytes: state read + write, log-weight write + read, ancestor write + read
+    return 2 * state_words(prob) * b_state + 2 * 4 + 2 * 4
+
+
+class Clocks(object):
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.dev), '--query-gpu=' + self.FIELDS, '--format=csv,noheader,nounits',
+                 '-lms', '200'], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in self.out:
+            f = [x.strip() for x in line.split(',')]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith('active'):
+                    reasons.add(nm)
+        if not sm:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled'], 'samples': 0}
+        return {'sm_mhz': statistics.median(sm), 'sm_max_mhz': max(mx), 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def ncu_traffic(workload):
+    """Per-launch DRAM bytes of the propagate kernel from the committed ncu summary, scaled to J."""
+    path = os.path.join(ROOT, 'profiles', 'k_propagate_%s.json' % workload)
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d['dram_bytes_per_particle']) * WORKLOADS[workload][1]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_baseline(workload, budget_s=12.0, threads=0):
+    """Times the FP64 oracle (OpenMP, all host threads) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    from oracle import Oracle
+    lib = WORKLOADS[workload][0]
+    orc = Oracle(lib)
+    J0 = WORKLOADS[workload][1]
+    J = min(J0, 20000)
+    n = 1
+    while True:
+        p = workload_problem(workload, precision=64, seed=3, J=J, nb_obs=n)
+        t = time.perf_counter()
+        orc.smc(p, n_threads=threads)
+        el = time.perf_counter() - t
+        if el > budget_s / 4 or n >= WORKLOADS[workload][2]:
+            break
+        n = min(WORKLOADS[workload][2], max(n + 1, int(n * (budget_s / 3) / max(el, 1e-3))))
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return {'value': p.J * p.n_obs / el, 'unit': 'particle-steps/s', 'cores': cores, 'kind': 'port',
+            'sample': '%s: J=%d particles x %d observation intervals (%d Euler substeps each), FP64 oracle, %.2f s'
+                      % (workload, p.J, p.n_obs, int(p.n_sub[0]), el)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    base = cpu_baseline(args.workload, budget_s=8.0)
+    vals = []
+    for _ in range(args.warmup):
+        pass
+    lib, J0, T, dt = WORKLOADS[args.workload]
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    from oracle import Oracle
+    orc = Oracle(lib)
+    J = min(J0, 20000)
+    n = max(1, min(T, int(round(base['value'] * 4.0 / J))))
+    p = workload_problem(args.workload, precision=64, seed=4, J=J, nb_obs=n)
+    for _ in range(max(args.warmup, 1)):
+        orc.smc(p)
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        orc.smc(p)
+        vals.append(time.perf_counter() - t)
+    ms = 1000.0 * statistics.mean(vals)
+    v = p.J * p.n_obs / (ms / 1000.0)
+    base['value'] = v
+    base['sample'] = '%s: J=%d x %d intervals per step, FP64 oracle (reference CPU path restated), all host threads' % (
+        args.workload, p.J, p.n_obs)
+    line = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'particle-steps/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': {'workload': args.workload, 'J': WORKLOADS[args.workload][1],
+                       'T': WORKLOADS[args.workload][2], 'sample_J': p.J, 'sample_T': p.n_obs},
+            'cpu_baseline': base,
+            'e2e': {'value': v, 'unit': 'particle-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == 'reference':
+        return run_reference(args)
+    import numpy as np
+    import torch
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    from plomgpu.native import Engine, Plan
+    from plomgpu import build
+    lib = WORKLOADS[args.workload][0]
+    eng = Engine(lib)
+    prob = workload_problem(args.workload, precision=32, seed=1000 + rank)
+    plan = Plan(eng, prob, timing=True)
+    stream = torch.cuda.ExternalStream(plan.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        plan.launch()
+    barrier()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    prop_ms = []
+    with Clocks(local) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            plan.launch()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms_total = start.elapsed_time(end)
+    tot_prop, n_prop = plan.propagate_time()  # last launch
+    res = plan.results()
+    ms_step = ms_total / args.steps
+    t = torch.tensor([ms_step], device='cuda')
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item())
+    psteps = prob.J * prob.n_obs
+    value = psteps * world / (ms_step / 1000.0)
+    kernels_per_step = plan.kernel_count
+    plan.close()
+
+    # end to end through the one-shot C ABI call with host buffers
+    from plomgpu.native import DescHolder
+    e2e_times = []
+    for i in range(max(1, min(args.steps, 3))):
+        barrier()
+        t0 = time.perf_counter()
+        out = eng.smc(prob)
+        e2e_times.append(time.perf_counter() - t0)
+    h = DescHolder(prob)
+    h2d = sum(a.nbytes for a in h.arrays.values())
+    d2h = 8 * 2 * prob.n_obs + 16
+    e2e_s = statistics.median(e2e_times)
+    tt = torch.tensor([e2e_s], device='cuda')
+    if dist is not None:
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    e2e_value = psteps * world / float(tt.item())
+
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        B = bytes_per_particle_step(prob, 4)
+        avg_prop_ms = tot_prop / max(n_prop, 1)
+        achieved = B * prob.J / (avg_prop_ms / 1000.0) / 1e9
+        traffic = ncu_traffic(args.workload)
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'particle-steps/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
+            'config': {'workload': args.workload, 'J': prob.J, 'T': prob.n_obs, 'K': int(prob.n_sub[0]),
+                       'state_words': state_words(prob), 'noise': 'sde full (demographic + environmental)',
+                       'parallelism': 'replicas' if world > 1 else 'single GPU',
+                       'l2': 'inputs larger than L2 (two state generations of %.0f MB)' %
+                             (2 * state_words(prob) * 4 * prob.J / 1e6)},
+            'loglik': res.loglik,
+            'euler_substeps_per_s': value * float(np.mean(prob.n_sub)),
+            'gpu_launches': kernels_per_step * args.steps,
+            'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                         'frac': achieved / peak, 'traffic': traffic,
+                         'kernel': 'k_propagate', 'bytes_per_particle_step': B,
+                         'avg_launch_ms': avg_prop_ms, 'peak_kind': peak_kind,
+                         'propagate_share': tot_prop / (ms_total / args.steps)},
+            'clocks': clk.summary(),
+            'e2e': {'value': e2e_value, 'unit': 'particle-steps/s', 'h2d_bytes_per_step': h2d,
+                    'd2h_bytes_per_step': d2h, 'call': 'plomgpu_smc_run (host buffers, one-shot)'},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line['cpu_baseline'] = cpu_baseline(args.workload)
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,163 @@
+/*
+ * plomgpu: C ABI of the sm_100a sequential Monte Carlo engine for one
+ * generated plom model.
+ *
+ * One shared library is built per model (libplomgpu_<model>.so), as the
+ * reference builds one libplomtpl.a per model (model_builder/C/templates/
+ * Makefile:9-14).  Every library exports the same symbols; the model's
+ * dimensions are compile-time constants reported by plomgpu_get_model_info().
+ *
+ * All arrays are plain host pointers in row-major order; sizes follow from
+ * the descriptor's J / n_obs / n_sub and from plomgpu_get_model_info().  No call
+ * exits the process: every entry point returns a status code
+ * (PLOMGPU_OK = 0) and plomgpu_last_error() describes the last failure of
+ * the calling thread.  The reference terminates with print_err + exit
+ * (model_builder/C/core/print.c:247-268) instead.
+ */
+#ifndef PLOMGPU_H
+#define PLOMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum plomgpu_status {
+    PLOMGPU_OK = 0,
+    PLOMGPU_EINVAL = 1,      /* bad argument or size */
+    PLOMGPU_ECUDA = 2,       /* CUDA runtime error */
+    PLOMGPU_ENOMEM = 3,      /* device allocation failed */
+    PLOMGPU_ETIMEOUT = 4,    /* a bounded device wait ran out (the filter result is invalid) */
+    PLOMGPU_ENODEV = 5       /* no CUDA device */
+};
+
+/* noises_off bits, same values as enum plom_noises_off (model_builder/C/core/plom.h:66) */
+enum plomgpu_noises_off {
+    PLOMGPU_NO_DEM_STO = 1 << 0,
+    PLOMGPU_NO_ENV_STO = 1 << 1,
+    PLOMGPU_NO_DRIFT = 1 << 2
+};
+
+typedef struct plomgpu_model_info {
+    int n_par_sv, n_c, n_ac, n_cac;
+    int n_ts, n_ts_inc_unique, n_obs_inc, n_obs_prev;
+    int n_drift;          /* drifted parameters; each owns n_cac state words */
+    int off_drift, off_inc, n_state;   /* state layout: [sv*cac | drift*cac | incidences] */
+    int n_par_proc, n_par_obs, n_cov_cac, n_cov_ts;
+    int n_reac, n_white_noise;
+    int coupled;          /* 1 if the model reads a cac x cac coupling matrix */
+    int pop_size_eq_sum_sv;
+    const char *name;
+} plomgpu_model_info;
+
+/* Back-transform of one group of a drifted parameter (back_transform_x,
+ * model_builder/C/core/transform.c:462-481). f_inv: 0 id, 1 exp, 2 inv-logit,
+ * 3 inv-logit_ab; scale: 0 id, 1 pow10, 2 pow10 of the negative. */
+typedef struct plomgpu_back_transform {
+    int f_inv;
+    int scale;
+    int is_duration;
+    int pad;
+    double a, b;
+    double multiplier;
+} plomgpu_back_transform;
+
+/* One particle filter (the arguments of run_SMC, model_builder/C/core/smc.c:204-210,
+ * flattened to arrays). */
+typedef struct plomgpu_smc_desc {
+    int J;                    /* particles */
+    int n_obs;                /* observation intervals (nb_obs) */
+    const int *n_sub;         /* [n_obs] Euler substeps in interval n */
+    const double *t_sub;      /* [sum n_sub] start time of every substep (t += dt replayed on the host) */
+    const double *t_obs;      /* [n_obs] end time t1 of interval n (time of observation n) */
+    double dt;                /* integration step (1/round(1/dt), build.c:1303) */
+    const double *data;       /* [n_obs][n_ts]; NaN = missing */
+    const double *par_cac;    /* [n_par_proc][n_cac] natural process parameters */
+    const double *par_ts;     /* [n_par_obs][n_ts] natural observation parameters */
+    const double *cov_cac;    /* [sum n_sub][n_cov_cac][n_cac] covariates at the substep times */
+    const double *cov_ts;     /* [n_obs][n_cov_ts][n_ts] observation covariates at t_obs */
+    const double *coupling;   /* [n_cac][n_cac] or NULL when the model is not coupled */
+    const int *drift_group;   /* [n_drift][n_cac] group of each cac, or NULL */
+    const int *drift_ngroups; /* [n_drift] */
+    const plomgpu_back_transform *drift_bt;  /* [n_drift][n_cac] per group */
+    const double *drift_vol;  /* [n_drift][n_cac] volatility per group (natural) */
+    const double *x0;         /* [n_state] initial particle (replicated to all J) */
+    int noises_off;           /* plomgpu_noises_off bits */
+    int filter;               /* 0 = propagate only (smc -t) */
+    double like_min;          /* LIKE_MIN (smc -l), default 1e-17 */
+    uint64_t seed;            /* Philox key; ignored with CRN draws */
+    int precision;            /* 32: FP32 state and log-weights; 64: FP64 everywhere */
+    /* Common random numbers (optional): when crn_normals is set, every normal
+     * is read from it: [n][j][k][d] for interval n, particle j, substep k and
+     * draw d < plomgpu_draws_per_substep(noises_off) in the reference's draw
+     * order (cac-major, dem_sto__* then white_noise__*, then drift words
+     * [n_drift][n_cac]).  crn_uniforms[n] in [0,1) gives the systematic
+     * resampling offset U = u/J of interval n. */
+    const double *crn_normals;
+    const double *crn_uniforms;
+} plomgpu_smc_desc;
+
+typedef struct plomgpu_smc_result {
+    double loglik;            /* Llike_best */
+    int n_all_fail;
+    int status;
+    double *llike_n;          /* [n_obs] optional: log(mean weight) per interval (0 when not weighted) */
+    double *ess_n;            /* [n_obs] optional */
+    uint32_t *ancestors;      /* [n_obs][J] optional: select[n][j] (identity when not resampled) */
+    double *x_pred;           /* [n_obs][n_state][J] optional: propagated particles before resampling */
+    double *x_final;          /* [n_state][J] optional: particles after the last interval (resampled) */
+} plomgpu_smc_result;
+
+/* Model dimensions of this library. */
+int plomgpu_get_model_info(plomgpu_model_info *out);
+
+/* Normals one particle draws per substep for a noises_off value. */
+int plomgpu_draws_per_substep(int noises_off);
+
+/* Runs one filter: replaces run_SMC (model_builder/C/core/smc.c:204-307) and
+ * the per-particle loop of worker_routine_smc_inproc
+ * (model_builder/C/core/worker_inproc.c:21-102).  Host buffers in and out;
+ * allocates its device workspace for the call. */
+int plomgpu_smc_run(const plomgpu_smc_desc *desc, plomgpu_smc_result *result);
+
+/* Reusable plan: device buffers, uploaded inputs and a CUDA graph of the
+ * whole time loop, for callers that evaluate many likelihoods of the same
+ * shape (pmcmc, C/pmcmc/pmcmc.c:214; mif, C/mif/mif.c:128-200). */
+typedef struct plomgpu_plan plomgpu_plan;
+
+int plomgpu_plan_create(const plomgpu_smc_desc *desc, plomgpu_plan **out);
+/* flags: PLOMGPU_PLAN_TIMING records CUDA events around every propagate
+ * launch inside the graph, read back with plomgpu_plan_propagate_time(). */
+enum { PLOMGPU_PLAN_TIMING = 1 };
+int plomgpu_plan_create_ex(const plomgpu_smc_desc *desc, int flags, plomgpu_plan **out);
+/* Device time of the propagate launches of the last plomgpu_plan_launch
+ * (sum over launches, milliseconds) and their number. */
+int plomgpu_plan_propagate_time(plomgpu_plan *plan, double *total_ms, int *launches);
+/* Uploads new parameters / initial state / seed from host memory (pinned or
+ * pageable) on the plan's stream; pointers may be NULL to keep the previous
+ * values. */
+int plomgpu_plan_update(plomgpu_plan *plan, const double *par_cac, const double *par_ts,
+                        const double *x0, uint64_t seed);
+/* Enqueues one filter run on the plan's stream; inputs must be resident. */
+int plomgpu_plan_launch(plomgpu_plan *plan);
+/* Waits for the plan's stream and copies the results to host memory. */
+int plomgpu_plan_results(plomgpu_plan *plan, plomgpu_smc_result *result);
+/* Stream of the plan (a cudaStream_t), for timing with CUDA events. */
+void *plomgpu_plan_stream(plomgpu_plan *plan);
+/* Kernels launched by one plomgpu_plan_launch. */
+int plomgpu_plan_kernel_count(plomgpu_plan *plan);
+void plomgpu_plan_destroy(plomgpu_plan *plan);
+
+/* Test hook: the first J systematic-resampling points of offset U computed by
+ * the device-side closed form (GPU) into out[J]. */
+int plomgpu_debug_systematic_points(double U, int J, double *out);
+
+const char *plomgpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLOMGPU_H */

@@ -1,0 +1,630 @@
+// C ABI of the SMC engine for one generated model (declared in include/plomgpu.h).
+//
+// Host orchestration of the time loop of run_SMC (model_builder/C/core/smc.c:
+// 204-307): per observation interval one propagate launch, and, when the
+// data row has a value and filtering is on, the weight / scan / search
+// launches.  The whole loop is captured once into a CUDA graph per plan and
+// replayed per likelihood evaluation.
+#include PLOM_MODEL_HEADER
+#include "smc_engine.cuh"
+#include "plomgpu.h"
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+#include <vector>
+
+using namespace plomgpu;
+
+static_assert(sizeof(plomgpu_back_transform) == sizeof(plomrt::BackTransform), "back-transform layout");
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) {                                                                  \
+      return fail(e_ == cudaErrorMemoryAllocation ? PLOMGPU_ENOMEM : PLOMGPU_ECUDA,           \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+    }                                                                                         \
+  } while (0)
+
+constexpr bool kSmem = (M::S > 48);
+constexpr int kBtProp = 128;
+constexpr int kBtWeight = 256;
+constexpr int kBtScan = 256;
+constexpr int kIptScan = 8;
+constexpr int kTile = kBtScan * kIptScan;
+constexpr int kBtSearch = 256;
+constexpr int kMaxWeightBlocks = 592;
+
+int variant_of(int noises_off) { return noises_off & 3; }
+bool drift_on(int noises_off) { return M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT); }
+
+int draws_per_substep(int noises_off) {
+  return M::N_CAC * M::draws_per_cac(variant_of(noises_off)) + (drift_on(noises_off) ? M::N_DRIFT * M::N_CAC : 0);
+}
+
+}  // namespace
+
+struct plomgpu_plan {
+  int J = 0, n_obs = 0, sub_total = 0, precision = 32, noises_off = 0, filter = 1;
+  bool crn = false, want_anc = false, want_xpred = false, want_llike = true;
+  double dt = 1.0, like_min = 1e-17, thresh = 0.0, log_like_min = 0.0;
+  std::vector<int> n_sub, sub0;
+  std::vector<double> t_obs, crn_u;
+  std::vector<char> weigh;
+  int nblk_weight = 1, ntiles = 1;
+  int kernels = 0;
+  size_t tsize = 4;
+  cudaStream_t stream = nullptr;
+  // device buffers
+  void* X[2] = {nullptr, nullptr};
+  void* lw = nullptr;
+  double* C = nullptr;
+  uint32_t* anc[2] = {nullptr, nullptr};
+  LseAcc* part = nullptr;
+  StepState* st = nullptr;
+  FilterAcc* acc = nullptr;
+  TileStatus* tstat = nullptr;
+  void* par_cac = nullptr;        // T
+  double* par_cac_d = nullptr;    // double staging
+  void* cov_cac = nullptr;        // T
+  void* coupling = nullptr;       // T
+  void* drift_vol = nullptr;      // T
+  int* drift_group = nullptr;
+  int* drift_ngroups = nullptr;
+  plomrt::BackTransform* drift_bt = nullptr;
+  double* par_ts = nullptr;
+  double* t_sub = nullptr;
+  double* cov_ts = nullptr;
+  double* data = nullptr;
+  double* x0 = nullptr;
+  double* crn_tab = nullptr;
+  uint64_t* seed = nullptr;
+  double* llike = nullptr;
+  double* ess = nullptr;
+  uint32_t* anc_hist = nullptr;
+  double* x_hist = nullptr;
+  double* x_final = nullptr;
+  // pinned host mirror of the accumulator
+  FilterAcc* acc_h = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // optional timing events around every propagate launch (event record nodes of the graph)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;  // [2 * n_obs]: before / after propagate n
+};
+
+namespace {
+
+template <class T>
+__global__ void k_convert(const double* __restrict__ in, T* __restrict__ out, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (T)in[i];
+}
+
+template <class T>
+int upload_as(const double* h, size_t n, void** d, cudaStream_t s) {
+  if (n == 0) return PLOMGPU_OK;
+  std::vector<T> tmp(n);
+  for (size_t i = 0; i < n; ++i) tmp[i] = (T)h[i];
+  CK(cudaMalloc(d, n * sizeof(T)));
+  CK(cudaMemcpyAsync(*d, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return PLOMGPU_OK;
+}
+
+template <class U>
+int upload(const U* h, size_t n, U** d, cudaStream_t s) {
+  if (n == 0 || h == nullptr) return PLOMGPU_OK;
+  CK(cudaMalloc((void**)d, n * sizeof(U)));
+  CK(cudaMemcpyAsync(*d, h, n * sizeof(U), cudaMemcpyHostToDevice, s));
+  return PLOMGPU_OK;
+}
+
+template <class T>
+using PropKernel = void (*)(const Tables<T>, const StepArgs);
+
+template <class T, int V, bool DRIFT, bool CRN>
+PropKernel<T> pick4() {
+  return &k_propagate<T, V, DRIFT, CRN, kSmem, kBtProp>;
+}
+
+template <class T, bool CRN>
+PropKernel<T> pick_v(int v, bool drift) {
+  if (drift) {
+    if constexpr (M::N_DRIFT > 0) {
+      switch (v) {
+        case 0: return pick4<T, 0, true, CRN>();
+        case 1: return pick4<T, 1, true, CRN>();
+        case 2: return pick4<T, 2, true, CRN>();
+        default: return pick4<T, 3, true, CRN>();
+      }
+    }
+  }
+  switch (v) {
+    case 0: return pick4<T, 0, false, CRN>();
+    case 1: return pick4<T, 1, false, CRN>();
+    case 2: return pick4<T, 2, false, CRN>();
+    default: return pick4<T, 3, false, CRN>();
+  }
+}
+
+template <class T>
+PropKernel<T> pick_prop(int noises_off, bool crn) {
+  const int v = variant_of(noises_off);
+  const bool d = drift_on(noises_off);
+  if (crn) {
+    if constexpr (std::is_same<T, double>::value) return pick_v<T, true>(v, d);
+    return nullptr;
+  }
+  return pick_v<T, false>(v, d);
+}
+
+template <class T>
+int enqueue_filter(plomgpu_plan* p) {
+  cudaStream_t s = p->stream;
+  const int J = p->J;
+  int kernels = 0;
+  Tables<T> tb;
+  tb.par_cac = (const T*)p->par_cac;
+  tb.cov_cac = (const T*)p->cov_cac;
+  tb.coupling = (const T*)p->coupling;
+  tb.drift_group = p->drift_group;
+  tb.drift_ngroups = p->drift_ngroups;
+  tb.drift_bt = p->drift_bt;
+  tb.drift_vol = (const T*)p->drift_vol;
+  tb.par_ts = p->par_ts;
+  tb.t_sub = p->t_sub;
+  tb.dt = p->dt;
+  tb.like_min = p->like_min;
+  tb.seed = p->seed;
+  tb.filter_id = 0;
+  tb.J = J;
+
+  PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn);
+  if (!kp) return fail(PLOMGPU_EINVAL, "common random numbers need precision 64");
+  const size_t smem = kSmem ? (size_t)M::S * kBtProp * sizeof(T) : 0;
+  if (smem > 0) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+  const int n_par = M::N_PAR_PROC * M::N_CAC;
+  if (n_par > 0) {
+    k_convert<T><<<(n_par + 255) / 256, 256, 0, s>>>(p->par_cac_d, (T*)p->par_cac, n_par);
+    ++kernels;
+  }
+  k_reset_acc<<<1, 1, 0, s>>>(p->acc);
+  ++kernels;
+  {
+    const size_t total = (size_t)M::OFF_INC * J;
+    const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+    k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, J, (T*)p->X[0]);
+    ++kernels;
+  }
+  const int D = p->crn ? draws_per_substep(p->noises_off) : 0;
+  size_t crn_off = 0;
+  int cur = 0;           // generation holding the particles before interval n
+  int anc_cur = -1;      // ancestors to apply when loading (index into p->anc), -1 = identity
+  const int gprop = (J + kBtProp - 1) / kBtProp;
+  for (int n = 0; n < p->n_obs; ++n) {
+    StepArgs a;
+    a.n = n;
+    a.n_sub = p->n_sub[n];
+    a.sub0 = p->sub0[n];
+    a.weigh = p->weigh[n];
+    a.t_obs = p->t_obs[n];
+    a.y = p->data + (size_t)n * M::N_TS;
+    a.cov_ts = p->cov_ts ? p->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS : nullptr;
+    a.X_prev = p->X[cur];
+    a.X_next = p->X[cur ^ 1];
+    a.anc = anc_cur >= 0 ? p->anc[anc_cur] : nullptr;
+    a.lw = p->lw;
+    a.crn = p->crn ? p->crn_tab + crn_off : nullptr;
+    a.crn_d = D;
+    a.x_hist = p->x_hist ? p->x_hist + (size_t)n * M::S * J : nullptr;
+    a.write_inc = (p->x_final != nullptr && n == p->n_obs - 1) ? 1 : 0;
+    crn_off += (size_t)J * p->n_sub[n] * D;
+    if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
+    kp<<<gprop, kBtProp, smem, s>>>(tb, a);
+    if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n + 1], s, cudaEventRecordExternal));
+    ++kernels;
+    cur ^= 1;
+    if (a.weigh) {
+      const int nxt = (anc_cur == 0) ? 1 : 0;
+      const double Uc = p->crn ? p->crn_u[n] : -1.0;
+      k_weight<T, kBtWeight><<<p->nblk_weight, kBtWeight, 0, s>>>(
+          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->st, p->acc, p->tstat, p->ntiles, n, Uc,
+          p->seed, 0u, p->llike, p->ess);
+      k_scan<T, kBtScan, kIptScan><<<p->ntiles, kBtScan, 0, s>>>((const T*)p->lw, J, p->thresh, p->st, p->tstat,
+                                                                  p->acc, p->C);
+      k_search<kBtSearch><<<(J + kBtSearch - 1) / kBtSearch, kBtSearch, 0, s>>>(
+          p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+      kernels += 3;
+      anc_cur = nxt;
+    } else {
+      if (p->anc_hist) {
+        k_identity<<<(J + 255) / 256, 256, 0, s>>>(p->anc_hist + (size_t)n * J, J);
+        ++kernels;
+      }
+      anc_cur = -1;
+    }
+  }
+  if (p->x_final) {
+    const size_t total = (size_t)M::S * J;
+    const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+    k_gather_final<T><<<g, 256, 0, s>>>((const T*)p->X[cur], anc_cur >= 0 ? p->anc[anc_cur] : nullptr, J, M::S,
+                                        p->x_final);
+    ++kernels;
+  }
+  CK(cudaGetLastError());
+  p->kernels = kernels;
+  return PLOMGPU_OK;
+}
+
+int check_desc(const plomgpu_smc_desc* d) {
+  if (!d) return fail(PLOMGPU_EINVAL, "null descriptor");
+  if (d->J < 1) return fail(PLOMGPU_EINVAL, "J must be >= 1");
+  if (d->n_obs < 0) return fail(PLOMGPU_EINVAL, "n_obs must be >= 0");
+  if (d->precision != 32 && d->precision != 64) return fail(PLOMGPU_EINVAL, "precision must be 32 or 64");
+  if (d->n_obs > 0 && (!d->n_sub || !d->t_obs || !d->data)) return fail(PLOMGPU_EINVAL, "missing n_sub / t_obs / data");
+  if (!d->x0) return fail(PLOMGPU_EINVAL, "missing x0");
+  if (M::N_PAR_PROC > 0 && !d->par_cac) return fail(PLOMGPU_EINVAL, "missing par_cac");
+  if (M::N_PAR_OBS > 0 && !d->par_ts) return fail(PLOMGPU_EINVAL, "missing par_ts");
+  if (M::COUPLED && !d->coupling) return fail(PLOMGPU_EINVAL, "coupled model needs a coupling matrix");
+  if (drift_on(d->noises_off) && (!d->drift_group || !d->drift_ngroups || !d->drift_bt || !d->drift_vol))
+    return fail(PLOMGPU_EINVAL, "drift tables missing");
+  if (d->crn_normals && d->precision != 64) return fail(PLOMGPU_EINVAL, "common random numbers need precision 64");
+  if (d->crn_normals && !d->crn_uniforms) return fail(PLOMGPU_EINVAL, "crn_uniforms missing");
+  if (!(d->dt > 0.0)) return fail(PLOMGPU_EINVAL, "dt must be > 0");
+  if (!(d->like_min > 0.0)) return fail(PLOMGPU_EINVAL, "like_min must be > 0");
+  long long sub_total = 0;
+  for (int n = 0; n < d->n_obs; ++n) {
+    if (d->n_sub[n] < 0) return fail(PLOMGPU_EINVAL, "negative substep count");
+    if ((long long)d->n_sub[n] * (M::N_CAC + 1) >= (1LL << 20))
+      return fail(PLOMGPU_EINVAL, "too many substeps per interval for the draw counter layout");
+    sub_total += d->n_sub[n];
+  }
+  if (sub_total > 0 && !d->t_sub) return fail(PLOMGPU_EINVAL, "missing t_sub");
+  if (sub_total > 0 && M::N_COV_CAC > 0 && !d->cov_cac) return fail(PLOMGPU_EINVAL, "missing cov_cac");
+  if (d->n_obs > 0 && M::N_COV_TS > 0 && !d->cov_ts) return fail(PLOMGPU_EINVAL, "missing cov_ts");
+  if (drift_on(d->noises_off)) {
+    for (int i = 0; i < M::N_DRIFT; ++i) {
+      if (d->drift_ngroups[i] < 1 || d->drift_ngroups[i] > M::N_CAC) return fail(PLOMGPU_EINVAL, "bad drift group count");
+      for (int c = 0; c < M::N_CAC; ++c) {
+        const int g = d->drift_group[i * M::N_CAC + c];
+        if (g < 0 || g >= d->drift_ngroups[i]) return fail(PLOMGPU_EINVAL, "bad drift group index");
+      }
+    }
+  }
+  return PLOMGPU_OK;
+}
+
+template <class T>
+int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
+  cudaStream_t s = p->stream;
+  const int J = d->J;
+  p->tsize = sizeof(T);
+  int rc;
+  CK(cudaMalloc(&p->X[0], (size_t)M::S * J * sizeof(T)));
+  CK(cudaMalloc(&p->X[1], (size_t)M::S * J * sizeof(T)));
+  CK(cudaMalloc(&p->lw, (size_t)J * sizeof(T)));
+  CK(cudaMalloc((void**)&p->C, (size_t)J * sizeof(double)));
+  CK(cudaMalloc((void**)&p->anc[0], (size_t)J * sizeof(uint32_t)));
+  CK(cudaMalloc((void**)&p->anc[1], (size_t)J * sizeof(uint32_t)));
+  p->nblk_weight = (J + kBtWeight * 4 - 1) / (kBtWeight * 4);
+  if (p->nblk_weight > kMaxWeightBlocks) p->nblk_weight = kMaxWeightBlocks;
+  if (p->nblk_weight < 1) p->nblk_weight = 1;
+  p->ntiles = (J + kTile - 1) / kTile;
+  CK(cudaMalloc((void**)&p->part, (size_t)p->nblk_weight * sizeof(LseAcc)));
+  CK(cudaMalloc((void**)&p->st, sizeof(StepState)));
+  CK(cudaMalloc((void**)&p->acc, sizeof(FilterAcc)));
+  CK(cudaMemsetAsync(p->acc, 0, sizeof(FilterAcc), s));
+  CK(cudaMalloc((void**)&p->tstat, (size_t)p->ntiles * sizeof(TileStatus)));
+  CK(cudaMemsetAsync(p->tstat, 0, (size_t)p->ntiles * sizeof(TileStatus), s));
+  CK(cudaMallocHost((void**)&p->acc_h, sizeof(FilterAcc)));
+
+  const size_t n_par = (size_t)M::N_PAR_PROC * M::N_CAC;
+  if (n_par > 0) {
+    CK(cudaMalloc(&p->par_cac, n_par * sizeof(T)));
+    if ((rc = upload<double>(d->par_cac, n_par, &p->par_cac_d, s))) return rc;
+  }
+  if ((rc = upload_as<T>(d->cov_cac, (size_t)p->sub_total * M::N_COV_CAC * M::N_CAC, &p->cov_cac, s))) return rc;
+  if (M::COUPLED) {
+    if ((rc = upload_as<T>(d->coupling, (size_t)M::N_CAC * M::N_CAC, &p->coupling, s))) return rc;
+  }
+  if (drift_on(d->noises_off)) {
+    if ((rc = upload_as<T>(d->drift_vol, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_vol, s))) return rc;
+    if ((rc = upload<int>(d->drift_group, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_group, s))) return rc;
+    if ((rc = upload<int>(d->drift_ngroups, (size_t)M::N_DRIFT, &p->drift_ngroups, s))) return rc;
+    if ((rc = upload<plomrt::BackTransform>((const plomrt::BackTransform*)d->drift_bt, (size_t)M::N_DRIFT * M::N_CAC,
+                                            &p->drift_bt, s)))
+      return rc;
+  }
+  if ((rc = upload<double>(d->par_ts, (size_t)M::N_PAR_OBS * M::N_TS, &p->par_ts, s))) return rc;
+  if ((rc = upload<double>(d->t_sub, (size_t)p->sub_total, &p->t_sub, s))) return rc;
+  if ((rc = upload<double>(d->cov_ts, (size_t)d->n_obs * M::N_COV_TS * M::N_TS, &p->cov_ts, s))) return rc;
+  {
+    // data rows: at least one row so that every interval has a valid pointer
+    std::vector<double> rows((size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS, NAN);
+    if (d->n_obs > 0) memcpy(rows.data(), d->data, (size_t)d->n_obs * M::N_TS * sizeof(double));
+    if ((rc = upload<double>(rows.data(), rows.size(), &p->data, s))) return rc;
+    CK(cudaStreamSynchronize(s));
+  }
+  if ((rc = upload<double>(d->x0, (size_t)M::S, &p->x0, s))) return rc;
+  CK(cudaMalloc((void**)&p->seed, sizeof(uint64_t)));
+  CK(cudaMemcpyAsync(p->seed, &d->seed, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  if (d->crn_normals) {
+    const size_t nd = (size_t)J * p->sub_total * draws_per_substep(d->noises_off);
+    if ((rc = upload<double>(d->crn_normals, nd, &p->crn_tab, s))) return rc;
+  }
+  if (p->want_llike) {
+    CK(cudaMalloc((void**)&p->llike, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double)));
+    CK(cudaMalloc((void**)&p->ess, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double)));
+    CK(cudaMemsetAsync(p->llike, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double), s));
+    CK(cudaMemsetAsync(p->ess, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double), s));
+  }
+  if (p->want_anc) CK(cudaMalloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
+  if (p->want_xpred) CK(cudaMalloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
+  if (p->timing) {
+    p->ev.assign(2 * (size_t)d->n_obs, nullptr);
+    for (auto& e : p->ev) CK(cudaEventCreate(&e));
+  }
+  CK(cudaStreamSynchronize(s));
+
+  // capture the time loop
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  rc = enqueue_filter<T>(p);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(s, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  CK(ce);
+  p->graph = g;
+  CK(cudaGraphInstantiate(&p->exec, g, 0));
+  return PLOMGPU_OK;
+}
+
+void plan_free(plomgpu_plan* p) {
+  if (!p) return;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  void* bufs[] = {p->X[0], p->X[1], p->lw, p->C, p->anc[0], p->anc[1], p->part, p->st, p->acc, p->tstat,
+                  p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
+                  p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
+                  p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (p->acc_h) cudaFreeHost(p->acc_h);
+  for (cudaEvent_t e : p->ev)
+    if (e) cudaEventDestroy(e);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+}
+
+int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bool want_xpred, bool want_final,
+                bool timing = false) {
+  *out = nullptr;
+  int rc = check_desc(d);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PLOMGPU_ENODEV, "no CUDA device");
+  plomgpu_plan* p = new plomgpu_plan();
+  p->J = d->J;
+  p->n_obs = d->n_obs;
+  p->precision = d->precision;
+  p->noises_off = d->noises_off;
+  p->filter = d->filter;
+  p->crn = d->crn_normals != nullptr;
+  p->want_anc = want_anc;
+  p->want_xpred = want_xpred;
+  p->timing = timing;
+  p->dt = d->dt;
+  p->like_min = d->like_min;
+  p->thresh = pow(d->like_min, (double)M::N_TS);
+  p->log_like_min = log(d->like_min);
+  p->n_sub.assign(d->n_sub, d->n_sub + d->n_obs);
+  p->t_obs.assign(d->t_obs, d->t_obs + d->n_obs);
+  p->sub0.resize(d->n_obs);
+  p->weigh.resize(d->n_obs);
+  int tot = 0;
+  for (int n = 0; n < d->n_obs; ++n) {
+    p->sub0[n] = tot;
+    tot += d->n_sub[n];
+    bool any = false;
+    for (int ts = 0; ts < M::N_TS; ++ts)
+      if (!isnan(d->data[(size_t)n * M::N_TS + ts])) any = true;
+    p->weigh[n] = (d->filter && any) ? 1 : 0;
+  }
+  p->sub_total = tot;
+  if (p->crn) p->crn_u.assign(d->crn_uniforms, d->crn_uniforms + d->n_obs);
+  cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete p;
+    return fail(PLOMGPU_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  if (want_final) {
+    e = cudaMalloc((void**)&p->x_final, (size_t)M::S * d->J * sizeof(double));
+    if (e != cudaSuccess) {
+      plan_free(p);
+      return fail(PLOMGPU_ENOMEM, "x_final allocation failed");
+    }
+  }
+  rc = (d->precision == 64) ? plan_build<double>(d, p) : plan_build<float>(d, p);
+  if (rc) {
+    std::string keep = g_err;
+    plan_free(p);
+    g_err = keep;
+    return rc;
+  }
+  *out = p;
+  return PLOMGPU_OK;
+}
+
+int plan_results(plomgpu_plan* p, plomgpu_smc_result* r) {
+  CK(cudaMemcpyAsync(p->acc_h, p->acc, sizeof(FilterAcc), cudaMemcpyDeviceToHost, p->stream));
+  if (r->llike_n && p->llike && p->n_obs > 0)
+    CK(cudaMemcpyAsync(r->llike_n, p->llike, (size_t)p->n_obs * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  if (r->ess_n && p->ess && p->n_obs > 0)
+    CK(cudaMemcpyAsync(r->ess_n, p->ess, (size_t)p->n_obs * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  if (r->ancestors && p->anc_hist)
+    CK(cudaMemcpyAsync(r->ancestors, p->anc_hist, (size_t)p->n_obs * p->J * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       p->stream));
+  if (r->x_pred && p->x_hist)
+    CK(cudaMemcpyAsync(r->x_pred, p->x_hist, (size_t)p->n_obs * M::S * p->J * sizeof(double), cudaMemcpyDeviceToHost,
+                       p->stream));
+  if (r->x_final && p->x_final)
+    CK(cudaMemcpyAsync(r->x_final, p->x_final, (size_t)M::S * p->J * sizeof(double), cudaMemcpyDeviceToHost,
+                       p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  r->loglik = p->acc_h->loglik;
+  r->n_all_fail = p->acc_h->n_all_fail;
+  if (p->acc_h->error) {
+    r->status = PLOMGPU_ETIMEOUT;
+    return fail(PLOMGPU_ETIMEOUT, (p->acc_h->error & ERR_SCAN_WAIT) ? "cumulative-weight scan wait ran out"
+                                                                      : "systematic point table overflow");
+  }
+  r->status = PLOMGPU_OK;
+  return PLOMGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int plomgpu_get_model_info(plomgpu_model_info* o) {
+  if (!o) return fail(PLOMGPU_EINVAL, "null");
+  o->n_par_sv = M::N_PAR_SV;
+  o->n_c = M::N_C;
+  o->n_ac = M::N_AC;
+  o->n_cac = M::N_CAC;
+  o->n_ts = M::N_TS;
+  o->n_ts_inc_unique = M::N_TS_INC_UNIQUE;
+  o->n_obs_inc = M::N_OBS_INC;
+  o->n_obs_prev = M::N_OBS_PREV;
+  o->n_drift = M::N_DRIFT;
+  o->off_drift = M::OFF_DRIFT;
+  o->off_inc = M::OFF_INC;
+  o->n_state = M::S;
+  o->n_par_proc = M::N_PAR_PROC;
+  o->n_par_obs = M::N_PAR_OBS;
+  o->n_cov_cac = M::N_COV_CAC;
+  o->n_cov_ts = M::N_COV_TS;
+  o->n_reac = M::N_REAC;
+  o->n_white_noise = M::N_WN;
+  o->coupled = M::COUPLED ? 1 : 0;
+  o->pop_size_eq_sum_sv = M::POP_SIZE_EQ_SUM_SV ? 1 : 0;
+  o->name = M::NAME;
+  return PLOMGPU_OK;
+}
+
+int plomgpu_draws_per_substep(int noises_off) { return draws_per_substep(noises_off); }
+
+int plomgpu_plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out) {
+  if (!out) return fail(PLOMGPU_EINVAL, "null output");
+  return plan_create(d, out, false, false, false);
+}
+
+int plomgpu_plan_create_ex(const plomgpu_smc_desc* d, int flags, plomgpu_plan** out) {
+  if (!out) return fail(PLOMGPU_EINVAL, "null output");
+  return plan_create(d, out, false, false, false, (flags & PLOMGPU_PLAN_TIMING) != 0);
+}
+
+int plomgpu_plan_propagate_time(plomgpu_plan* p, double* total_ms, int* launches) {
+  if (!p || !total_ms || !launches) return fail(PLOMGPU_EINVAL, "null argument");
+  if (!p->timing) return fail(PLOMGPU_EINVAL, "plan was created without PLOMGPU_PLAN_TIMING");
+  CK(cudaStreamSynchronize(p->stream));
+  double tot = 0.0;
+  for (int n = 0; n < p->n_obs; ++n) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, p->ev[2 * n], p->ev[2 * n + 1]));
+    tot += ms;
+  }
+  *total_ms = tot;
+  *launches = p->n_obs;
+  return PLOMGPU_OK;
+}
+
+int plomgpu_plan_update(plomgpu_plan* p, const double* par_cac, const double* par_ts, const double* x0,
+                        uint64_t seed) {
+  if (!p) return fail(PLOMGPU_EINVAL, "null plan");
+  if (par_cac && M::N_PAR_PROC > 0)
+    CK(cudaMemcpyAsync(p->par_cac_d, par_cac, (size_t)M::N_PAR_PROC * M::N_CAC * sizeof(double),
+                       cudaMemcpyHostToDevice, p->stream));
+  if (par_ts && M::N_PAR_OBS > 0)
+    CK(cudaMemcpyAsync(p->par_ts, par_ts, (size_t)M::N_PAR_OBS * M::N_TS * sizeof(double), cudaMemcpyHostToDevice,
+                       p->stream));
+  if (x0) CK(cudaMemcpyAsync(p->x0, x0, (size_t)M::S * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  // the seed is copied from a host temporary: make that copy synchronous w.r.t. the host
+  static thread_local uint64_t seed_h;
+  seed_h = seed;
+  CK(cudaMemcpyAsync(p->seed, &seed_h, sizeof(uint64_t), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return PLOMGPU_OK;
+}
+
+int plomgpu_plan_launch(plomgpu_plan* p) {
+  if (!p) return fail(PLOMGPU_EINVAL, "null plan");
+  CK(cudaGraphLaunch(p->exec, p->stream));
+  return PLOMGPU_OK;
+}
+
+int plomgpu_plan_results(plomgpu_plan* p, plomgpu_smc_result* r) {
+  if (!p || !r) return fail(PLOMGPU_EINVAL, "null argument");
+  return plan_results(p, r);
+}
+
+void* plomgpu_plan_stream(plomgpu_plan* p) { return p ? (void*)p->stream : nullptr; }
+
+int plomgpu_plan_kernel_count(plomgpu_plan* p) { return p ? p->kernels : 0; }
+
+void plomgpu_plan_destroy(plomgpu_plan* p) { plan_free(p); }
+
+int plomgpu_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r) {
+  if (!r) return fail(PLOMGPU_EINVAL, "null result");
+  plomgpu_plan* p = nullptr;
+  int rc = plan_create(d, &p, r->ancestors != nullptr, r->x_pred != nullptr, r->x_final != nullptr);
+  if (rc) {
+    r->status = rc;
+    return rc;
+  }
+  rc = plomgpu_plan_launch(p);
+  if (!rc) rc = plan_results(p, r);
+  std::string keep = g_err;
+  plan_free(p);
+  g_err = keep;
+  r->status = rc;
+  return rc;
+}
+
+int plomgpu_debug_systematic_points(double U, int J, double* out) {
+  if (J < 1 || !out) return fail(PLOMGPU_EINVAL, "bad arguments");
+  double* d = nullptr;
+  int* err = nullptr;
+  CK(cudaMalloc((void**)&d, (size_t)J * sizeof(double)));
+  CK(cudaMalloc((void**)&err, sizeof(int)));
+  CK(cudaMemset(err, 0, sizeof(int)));
+  k_sys_points<<<1, 256>>>(U, J, d, err);
+  CK(cudaGetLastError());
+  int herr = 0;
+  CK(cudaMemcpy(out, d, (size_t)J * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost));
+  cudaFree(d);
+  cudaFree(err);
+  if (herr) return fail(PLOMGPU_EINVAL, "systematic point table overflow");
+  return PLOMGPU_OK;
+}
+
+const char* plomgpu_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

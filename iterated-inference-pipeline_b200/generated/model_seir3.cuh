@@ -1,0 +1,152 @@
+// Generated by plomgpu.emit for model "seir3".  Do not edit.
+#pragma once
+#include "plom_rt.h"
+namespace plomgen {
+struct Model {
+  static constexpr const char* NAME = "seir3";
+  static constexpr int N_PAR_SV = 4, N_C = 3, N_AC = 2, N_CAC = 6;
+  static constexpr int N_TS = 3, N_TS_INC_UNIQUE = 3, N_OBS_INC = 1, N_OBS_PREV = 0;
+  static constexpr int N_DRIFT = 0;  // drifted parameters, N_CAC words each
+  static constexpr int OFF_DRIFT = N_PAR_SV*N_CAC, OFF_INC = OFF_DRIFT + N_DRIFT*N_CAC;
+  static constexpr int S = OFF_INC + N_TS_INC_UNIQUE;  // words per particle
+  static constexpr int N_PAR_PROC = 6, N_PAR_OBS = 2, N_COV_CAC = 1, N_COV_TS = 1;
+  static constexpr int N_REAC = 8, N_WN = 1;
+  static constexpr bool COUPLED = true;
+  static constexpr bool POP_SIZE_EQ_SUM_SV = true;
+  static constexpr int COV_N = 0;  // index of N among cac covariates, -1 if none
+  // normals drawn per cac and substep for a noise variant (bit0 no dem, bit1 no env)
+  static constexpr PLOM_HD int draws_per_cac(int v) { return ((v & 1) ? 0 : N_REAC) + ((v & 2) ? 0 : N_WN); }
+  static constexpr int N_INC_LINKS = 6;
+  static constexpr int INC_PER_CAC = 1;
+  PLOM_HD static int inc_link(int cac, int k) {
+    constexpr int tab[N_CAC][INC_PER_CAC] = {{0},{0},{1},{1},{2},{2}};
+    return tab[cac][k];
+  }
+  template <int V, bool DRIFT, class T, class X, class E, class D>
+  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {
+    (void)t;
+    constexpr int NW = draws_per_cac(V);
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    T yf_I[N_CAC];
+PLOM_UNROLL
+    for (int c2 = 0; c2 < N_CAC; ++c2) {
+      yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
+    }
+    PLOM_PRAGMA_CAC
+    for (int cac = 0; cac < N_CAC; ++cac) {
+      const T xo_S = x[0*N_CAC+cac];
+      const T xo_E = x[1*N_CAC+cac];
+      const T xo_I = x[2*N_CAC+cac];
+      const T xo_R = x[3*N_CAC+cac];
+      T foi_I = T(0);
+PLOM_UNROLL
+      for (int c2 = 0; c2 < N_CAC; ++c2) foi_I += e.coupling(cac, c2) * yf_I[c2];
+      const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
+      const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
+      const T r2 = e.par(2, cac);
+      const T r3 = e.par(1, cac);
+      const T r4 = e.par(5, cac);
+      T nz[NW > 0 ? NW : 1];
+      draws.template normals<NW>(cac, nz);
+      const T sqdt = sqrt(dt);
+      (void)sqdt;
+      int q = 0; (void)q;
+      const T dem_0 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_1 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_2 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_3 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_4 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_5 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_6 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T dem_7 = (V & 1) ? T(0) : sqdt*nz[q++];
+      const T wn_0 = (V & 2) ? T(0) : sqdt*nz[q++];
+      T incterm_0;
+      switch (V) {
+        case 0: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
+        case 1: incterm_0 = (+ (r3*xo_I))*dt; break;
+        case 2: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
+        case 3: incterm_0 = (+ (r3*xo_I))*dt; break;
+      }
+      T f_S;
+      switch (V) {
+        case 0: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0 - (r1*xo_S)*e.par(3, cac)*wn_0; break;
+        case 1: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - (r1*xo_S)*e.par(3, cac)*wn_0; break;
+        case 2: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0; break;
+        case 3: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt; break;
+      }
+      T f_E;
+      switch (V) {
+        case 0: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1 + (r1*xo_S)*e.par(3, cac)*wn_0; break;
+        case 1: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt + (r1*xo_S)*e.par(3, cac)*wn_0; break;
+        case 2: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1; break;
+        case 3: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt; break;
+      }
+      T f_I;
+      switch (V) {
+        case 0: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
+        case 1: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
+        case 2: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
+        case 3: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
+      }
+      T f_R;
+      switch (V) {
+        case 0: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
+        case 1: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
+        case 2: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
+        case 3: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
+      }
+PLOM_UNROLL
+      for (int k = 0; k < INC_PER_CAC; ++k) {
+        const int l = inc_link(cac, k);
+        if (l < 0) break;
+        const int o = l >> 10, w = l & 1023;
+PLOM_UNROLL
+        for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {
+          if (ww == w) {
+            if (o == 0) inc_acc[ww] += incterm_0;
+          }
+        }
+      }
+      x[0*N_CAC+cac] = (f_S < T(0)) ? T(0) : f_S;
+      x[1*N_CAC+cac] = (f_E < T(0)) ? T(0) : f_E;
+      x[2*N_CAC+cac] = (f_I < T(0)) ? T(0) : f_I;
+      x[3*N_CAC+cac] = (f_R < T(0)) ? T(0) : f_R;
+    }
+PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {
+      const T f = x[OFF_INC+w] + inc_acc[w];
+      x[OFF_INC+w] = (f < T(0)) ? T(0) : f;
+    }
+    if (DRIFT) {
+      // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)
+      PLOM_UNROLL
+      for (int i = 0; i < N_DRIFT; ++i) {
+        const int ng = e.drift_ngroups(i);
+        PLOM_UNROLL
+        for (int g = 0; g < N_CAC; ++g) {
+          if (g < ng) x[OFF_DRIFT+i*N_CAC+g] += e.drift_vol(i, g)*sqrt(dt)*draws.drift_normal(i, g);
+        }
+      }
+    }
+  }
+  template <class T, class X>
+  PLOM_HD static void proj2obs(const X& x, double* obs) {
+    obs[0] = (double)x[OFF_INC+0];
+    obs[1] = (double)x[OFF_INC+1];
+    obs[2] = (double)x[OFF_INC+2];
+  }
+  // observation model, evaluated in double (Ccoder.print_like)
+  template <class E>
+  PLOM_HD static double obs_mean(const double x, const int ts, const double t, const E& e) {
+    typedef double T; (void)x; (void)ts; (void)t; (void)e;
+    return e.cov_ts(0, ts)*e.par_ts(0, ts)*x;
+  }
+  template <class E>
+  PLOM_HD static double obs_var(const double x, const int ts, const double t, const E& e) {
+    typedef double T; (void)x; (void)ts; (void)t; (void)e;
+    return (e.par_ts(1, ts)*e.par_ts(1, ts))*(e.cov_ts(0, ts)*e.cov_ts(0, ts))*(e.par_ts(0, ts)*e.par_ts(0, ts))*(x*x) + e.cov_ts(0, ts)*e.par_ts(0, ts)*x*(T(1.0) - e.par_ts(0, ts));
+  }
+};
+}  // namespace plomgen

@@ -1,0 +1,99 @@
+"""Per-model build: emit the model header and compile the sm_100a engine.
+
+Mirrors the reference's per-model build (``pmbuilder`` renders the model's C
+then ``make`` builds ``libplomtpl.a`` and the binaries,
+model_builder/Builder.py:286-344, model_builder/C/templates/Makefile:9-14):
+here the emitter writes ``generated/model_<name>.cuh`` and nvcc builds
+``lib/libplomgpu_<name>.so`` for sm_100a.
+"""
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+
+from .emit import Emitter
+from .model import PlomModel
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REPO_ROOT = os.path.dirname(PKG_ROOT)
+CSRC = os.path.join(PKG_ROOT, 'csrc')
+GEN = os.path.join(PKG_ROOT, 'generated')
+LIB = os.path.join(PKG_ROOT, 'lib')
+INCLUDE = os.path.join(REPO_ROOT, 'include')
+
+NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+SMEM_STATE_WORDS = 48
+
+
+def header_path(name):
+    return os.path.join(GEN, 'model_%s.cuh' % name)
+
+
+def lib_path(name):
+    return os.path.join(LIB, 'libplomgpu_%s.so' % name)
+
+
+def write_header(model, name):
+    """Writes the model header if its text changed; returns (path, n_state_words)."""
+    os.makedirs(GEN, exist_ok=True)
+    em = Emitter(model)
+    text = em.header(name)
+    path = header_path(name)
+    old = open(path).read() if os.path.exists(path) else None
+    if old != text:
+        with open(path, 'w') as f:
+            f.write(text)
+    nd = len(model.drift_par_proc)
+    S = len(model.par_sv) * model.N_CAC + nd * model.N_CAC + model.N_TS_INC_UNIQUE
+    return path, S
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in ('plom_rt.h', 'smc_engine.cuh', 'plomgpu_api.cu')] + \
+        [os.path.join(INCLUDE, 'plomgpu.h')]
+
+
+def _stamp(name, extra):
+    h = hashlib.sha256()
+    for p in _sources() + [header_path(name)]:
+        with open(p, 'rb') as f:
+            h.update(f.read())
+    h.update(json.dumps(extra, sort_keys=True).encode())
+    return h.hexdigest()
+
+
+def nvcc_command(name, S, out=None, verbose_ptxas=False):
+    smem = 1 if S > SMEM_STATE_WORDS else 0
+    cmd = [NVCC] + ARCH + ['-lineinfo', '-O3', '-std=c++17', '--expt-relaxed-constexpr',
+                           '-Xcompiler', '-fPIC', '-shared',
+                           '-DPLOM_MODEL_HEADER="model_%s.cuh"' % name, '-DPLOM_SMEM_STATE=%d' % smem,
+                           '-I', CSRC, '-I', GEN, '-I', INCLUDE,
+                           os.path.join(CSRC, 'plomgpu_api.cu'), '-o', out or lib_path(name)]
+    if verbose_ptxas:
+        cmd.insert(1, '-Xptxas=-v')
+    return cmd
+
+
+def build_model(model, name, force=False, verbose=False):
+    """Emit + compile; skips the compile when sources and header are unchanged."""
+    _, S = write_header(model, name)
+    os.makedirs(LIB, exist_ok=True)
+    out = lib_path(name)
+    stamp_file = out + '.stamp'
+    stamp = _stamp(name, {'S': S, 'arch': ARCH})
+    if not force and os.path.exists(out) and os.path.exists(stamp_file) and open(stamp_file).read() == stamp:
+        return out
+    cmd = nvcc_command(name, S)
+    if verbose:
+        print(' '.join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    with open(stamp_file, 'w') as f:
+        f.write(stamp)
+    return out
+
+
+def build_from_files(context, process, link, name, **kw):
+    return build_model(PlomModel(context, process, link), name, **kw)

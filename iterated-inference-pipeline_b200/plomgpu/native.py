@@ -1,0 +1,247 @@
+"""ctypes binding of the C ABI in include/plomgpu.h.
+
+The CUDA library is mandatory: loading fails loudly when it is missing or
+when no GPU is present at call time; nothing falls back to a CPU path.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+
+class PlomGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        RuntimeError.__init__(self, 'plomgpu error %d: %s' % (code, msg))
+        self.code = code
+
+
+class ModelInfo(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        'n_par_sv', 'n_c', 'n_ac', 'n_cac', 'n_ts', 'n_ts_inc_unique', 'n_obs_inc', 'n_obs_prev',
+        'n_drift', 'off_drift', 'off_inc', 'n_state', 'n_par_proc', 'n_par_obs', 'n_cov_cac', 'n_cov_ts',
+        'n_reac', 'n_white_noise', 'coupled', 'pop_size_eq_sum_sv')] + [('name', C.c_char_p)]
+
+
+class BackTransform(C.Structure):
+    _fields_ = [('f_inv', C.c_int), ('scale', C.c_int), ('is_duration', C.c_int), ('pad', C.c_int),
+                ('a', C.c_double), ('b', C.c_double), ('multiplier', C.c_double)]
+
+
+_P = C.POINTER
+_dp = _P(C.c_double)
+_ip = _P(C.c_int)
+_up = _P(C.c_uint32)
+
+
+class SmcDesc(C.Structure):
+    _fields_ = [('J', C.c_int), ('n_obs', C.c_int), ('n_sub', _ip), ('t_sub', _dp), ('t_obs', _dp),
+                ('dt', C.c_double), ('data', _dp), ('par_cac', _dp), ('par_ts', _dp), ('cov_cac', _dp),
+                ('cov_ts', _dp), ('coupling', _dp), ('drift_group', _ip), ('drift_ngroups', _ip),
+                ('drift_bt', _P(BackTransform)), ('drift_vol', _dp), ('x0', _dp), ('noises_off', C.c_int),
+                ('filter', C.c_int), ('like_min', C.c_double), ('seed', C.c_uint64), ('precision', C.c_int),
+                ('crn_normals', _dp), ('crn_uniforms', _dp)]
+
+
+class SmcResult(C.Structure):
+    _fields_ = [('loglik', C.c_double), ('n_all_fail', C.c_int), ('status', C.c_int),
+                ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp)]
+
+
+API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_smc_run', 'plomgpu_plan_create',
+               'plomgpu_plan_create_ex', 'plomgpu_plan_propagate_time',
+               'plomgpu_plan_update', 'plomgpu_plan_launch', 'plomgpu_plan_results', 'plomgpu_plan_stream',
+               'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
+               'plomgpu_last_error']
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class DescHolder(object):
+    """Keeps the numpy arrays of a descriptor alive."""
+
+    def __init__(self, problem, crn_normals=None, crn_uniforms=None, precision=None):
+        p = problem
+        self.arrays = {}
+
+        def keep(name, arr, dtype):
+            if arr is None:
+                return None
+            a = np.ascontiguousarray(arr, dtype=dtype)
+            self.arrays[name] = a
+            return a
+
+        n_sub = keep('n_sub', p.n_sub, np.int32)
+        t_sub = keep('t_sub', p.t_sub if len(p.t_sub) else np.zeros(1), np.float64)
+        t_obs = keep('t_obs', p.t_obs if len(p.t_obs) else np.zeros(1), np.float64)
+        data = keep('data', p.data if p.data.size else np.full((1,), np.nan), np.float64)
+        par_cac = keep('par_cac', p.par_cac if p.par_cac.size else np.zeros(1), np.float64)
+        par_ts = keep('par_ts', p.par_ts if p.par_ts.size else np.zeros(1), np.float64)
+        cov_cac = keep('cov_cac', p.cov_cac if p.cov_cac.size else np.zeros(1), np.float64)
+        cov_ts = keep('cov_ts', p.cov_ts if p.cov_ts.size else np.zeros(1), np.float64)
+        coupling = keep('coupling', p.coupling, np.float64) if p.coupling is not None else None
+        dg = keep('drift_group', p.drift_group, np.int32)
+        dng = keep('drift_ngroups', p.drift_ngroups, np.int32)
+        dvol = keep('drift_vol', p.drift_vol, np.float64)
+        nd, ncac = len(p.drift_bt), len(p.drift_bt[0])
+        bts = (BackTransform * (nd * ncac))()
+        for i in range(nd):
+            for c in range(ncac):
+                f, s, dur, a, b, mult = p.drift_bt[i][c]
+                bts[i * ncac + c] = BackTransform(int(f), int(s), int(dur), 0, float(a), float(b), float(mult))
+        self.bts = bts
+        x0 = keep('x0', p.x0, np.float64)
+        crn = keep('crn', crn_normals, np.float64) if crn_normals is not None else None
+        crnu = keep('crnu', crn_uniforms, np.float64) if crn_uniforms is not None else None
+        self.desc = SmcDesc(
+            J=p.J, n_obs=p.n_obs, n_sub=_ptr(n_sub, _ip), t_sub=_ptr(t_sub, _dp), t_obs=_ptr(t_obs, _dp),
+            dt=p.dt, data=_ptr(data, _dp), par_cac=_ptr(par_cac, _dp), par_ts=_ptr(par_ts, _dp),
+            cov_cac=_ptr(cov_cac, _dp), cov_ts=_ptr(cov_ts, _dp), coupling=_ptr(coupling, _dp),
+            drift_group=_ptr(dg, _ip), drift_ngroups=_ptr(dng, _ip), drift_bt=C.cast(bts, _P(BackTransform)),
+            drift_vol=_ptr(dvol, _dp), x0=_ptr(x0, _dp), noises_off=p.noises_off, filter=1 if p.filter else 0,
+            like_min=p.like_min, seed=p.seed, precision=precision or p.precision,
+            crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp))
+
+
+class Outputs(object):
+    def __init__(self, J, n_obs, S, ancestors=False, x_pred=False, x_final=False):
+        self.llike_n = np.zeros(max(n_obs, 1))
+        self.ess_n = np.zeros(max(n_obs, 1))
+        self.ancestors = np.zeros((n_obs, J), dtype=np.uint32) if ancestors else None
+        self.x_pred = np.zeros((n_obs, S, J)) if x_pred else None
+        self.x_final = np.zeros((S, J)) if x_final else None
+        self.res = SmcResult(0.0, 0, 0, _ptr(self.llike_n, _dp), _ptr(self.ess_n, _dp),
+                             _ptr(self.ancestors, _up), _ptr(self.x_pred, _dp), _ptr(self.x_final, _dp))
+
+    @property
+    def loglik(self):
+        return self.res.loglik
+
+    @property
+    def n_all_fail(self):
+        return self.res.n_all_fail
+
+
+def _declare(lib):
+    lib.plomgpu_get_model_info.argtypes = [_P(ModelInfo)]
+    lib.plomgpu_draws_per_substep.argtypes = [C.c_int]
+    lib.plomgpu_smc_run.argtypes = [_P(SmcDesc), _P(SmcResult)]
+    lib.plomgpu_plan_create.argtypes = [_P(SmcDesc), _P(C.c_void_p)]
+    lib.plomgpu_plan_create_ex.argtypes = [_P(SmcDesc), C.c_int, _P(C.c_void_p)]
+    lib.plomgpu_plan_propagate_time.argtypes = [C.c_void_p, _dp, _ip]
+    lib.plomgpu_plan_update.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_uint64]
+    lib.plomgpu_plan_launch.argtypes = [C.c_void_p]
+    lib.plomgpu_plan_results.argtypes = [C.c_void_p, _P(SmcResult)]
+    lib.plomgpu_plan_stream.argtypes = [C.c_void_p]
+    lib.plomgpu_plan_stream.restype = C.c_void_p
+    lib.plomgpu_plan_kernel_count.argtypes = [C.c_void_p]
+    lib.plomgpu_plan_destroy.argtypes = [C.c_void_p]
+    lib.plomgpu_plan_destroy.restype = None
+    lib.plomgpu_debug_systematic_points.argtypes = [C.c_double, C.c_int, _dp]
+    lib.plomgpu_last_error.restype = C.c_char_p
+    return lib
+
+
+_LIBS = {}
+
+
+def load(name, path=None):
+    """Loads libplomgpu_<name>.so (raises if it is not built)."""
+    path = path or _build.lib_path(name)
+    if path in _LIBS:
+        return _LIBS[path]
+    if not os.path.exists(path):
+        raise PlomGpuError(-1, 'CUDA library %s is not built (run __graft_entry__.build())' % path)
+    lib = _declare(C.CDLL(path))
+    _LIBS[path] = lib
+    return lib
+
+
+def check(lib, rc):
+    if rc != 0:
+        raise PlomGpuError(rc, lib.plomgpu_last_error().decode())
+
+
+def model_info(lib):
+    mi = ModelInfo()
+    check(lib, lib.plomgpu_get_model_info(C.byref(mi)))
+    return mi
+
+
+class Engine(object):
+    """The GPU engine of one model library."""
+
+    def __init__(self, name, path=None):
+        self.lib = load(name, path)
+        self.info = model_info(self.lib)
+
+    def smc(self, problem, crn_normals=None, crn_uniforms=None, ancestors=False, x_pred=False, x_final=False,
+            precision=None):
+        h = DescHolder(problem, crn_normals, crn_uniforms, precision)
+        out = Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final)
+        check(self.lib, self.lib.plomgpu_smc_run(C.byref(h.desc), C.byref(out.res)))
+        return out
+
+    def draws_per_substep(self, noises_off):
+        return self.lib.plomgpu_draws_per_substep(noises_off)
+
+    def systematic_points(self, U, J):
+        out = np.zeros(J)
+        check(self.lib, self.lib.plomgpu_debug_systematic_points(U, J, _ptr(out, _dp)))
+        return out
+
+
+class Plan(object):
+    """A captured filter (plomgpu_plan_*), for repeated likelihood evaluations."""
+
+    def __init__(self, engine, problem, precision=None, timing=False):
+        self.engine = engine
+        self.lib = engine.lib
+        self.h = DescHolder(problem, precision=precision)
+        self.p = C.c_void_p()
+        check(self.lib, self.lib.plomgpu_plan_create_ex(C.byref(self.h.desc), 1 if timing else 0, C.byref(self.p)))
+        self.problem = problem
+
+    def propagate_time(self):
+        """(total ms, launches) of the propagate kernels of the last launch."""
+        ms, n = C.c_double(), C.c_int()
+        check(self.lib, self.lib.plomgpu_plan_propagate_time(self.p, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def update(self, par_cac=None, par_ts=None, x0=None, seed=0):
+        def ptr(a):
+            return None if a is None else np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(_dp)
+        keep = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None for a in (par_cac, par_ts, x0)]
+        check(self.lib, self.lib.plomgpu_plan_update(
+            self.p, *(k.ctypes.data_as(_dp) if k is not None else None for k in keep), C.c_uint64(seed)))
+
+    def launch(self):
+        check(self.lib, self.lib.plomgpu_plan_launch(self.p))
+
+    def results(self):
+        out = Outputs(self.problem.J, self.problem.n_obs, self.engine.info.n_state)
+        check(self.lib, self.lib.plomgpu_plan_results(self.p, C.byref(out.res)))
+        return out
+
+    @property
+    def stream(self):
+        return self.lib.plomgpu_plan_stream(self.p)
+
+    @property
+    def kernel_count(self):
+        return self.lib.plomgpu_plan_kernel_count(self.p)
+
+    def close(self):
+        if self.p:
+            self.lib.plomgpu_plan_destroy(self.p)
+            self.p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

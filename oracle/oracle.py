@@ -1,0 +1,105 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+Used by tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py
+as the checker; the product never imports it.
+"""
+
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), 'iterated-inference-pipeline_b200'))
+
+from plomgpu import native  # noqa: E402  (descriptor structs shared with the C ABI)
+
+from build_oracle import build as _build, lib_path  # noqa: E402
+
+_dp = C.POINTER(C.c_double)
+
+
+class Oracle(object):
+    def __init__(self, name, build=True):
+        path = _build(name) if build else lib_path(name)
+        self.lib = C.CDLL(path)
+        L = self.lib
+        L.oracle_model_info.argtypes = [C.POINTER(native.ModelInfo)]
+        L.oracle_draws_per_substep.argtypes = [C.c_int]
+        L.oracle_smc_run.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.SmcResult), C.c_int]
+        L.oracle_systematic_points_sequential.argtypes = [C.c_double, C.c_int, _dp]
+        L.oracle_systematic_points_sequential.restype = None
+        L.oracle_systematic_points_table.argtypes = [C.c_double, C.c_int, _dp]
+        L.oracle_step.argtypes = [_dp, C.c_double, C.c_double, C.c_int, C.POINTER(native.SmcDesc), C.c_int, _dp]
+        L.oracle_obs_loglik.argtypes = [_dp, C.POINTER(native.SmcDesc), C.c_int]
+        L.oracle_obs_loglik.restype = C.c_double
+        L.oracle_obs_moments.argtypes = [C.c_double, C.c_int, C.c_double, C.POINTER(native.SmcDesc), _dp, _dp]
+        L.oracle_obs_moments.restype = None
+        L.oracle_like.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
+        L.oracle_like.restype = C.c_double
+        L.oracle_weight_and_resample.argtypes = [_dp, C.c_int, C.c_double, C.c_double, _dp, _dp,
+                                                 C.POINTER(C.c_uint32)]
+        L.oracle_proj2obs.argtypes = [_dp, _dp]
+        L.oracle_proj2obs.restype = None
+        self.info = native.ModelInfo()
+        L.oracle_model_info(C.byref(self.info))
+
+    def draws_per_substep(self, noises_off):
+        return self.lib.oracle_draws_per_substep(noises_off)
+
+    def smc(self, problem, crn_normals=None, crn_uniforms=None, ancestors=False, x_pred=False, x_final=False,
+            n_threads=0):
+        h = native.DescHolder(problem, crn_normals, crn_uniforms, precision=64)
+        out = native.Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final)
+        rc = self.lib.oracle_smc_run(C.byref(h.desc), C.byref(out.res), n_threads)
+        if rc:
+            raise RuntimeError('oracle failed: %d' % rc)
+        return out
+
+    def weight_and_resample(self, likes, U, like_min=1e-17):
+        """weight() then systematic_sampling() on linear likelihoods: (normalised, select, llike_n, ess, all_fail)."""
+        w = np.ascontiguousarray(likes, dtype=np.float64).copy()
+        sel = np.zeros(len(w), dtype=np.uint32)
+        ll, ess = C.c_double(), C.c_double()
+        fail = self.lib.oracle_weight_and_resample(w.ctypes.data_as(_dp), len(w), like_min, U, C.byref(ll),
+                                                   C.byref(ess), sel.ctypes.data_as(C.POINTER(C.c_uint32)))
+        return w, sel, ll.value, ess.value, fail
+
+    def systematic_points(self, U, J, table=False):
+        out = np.zeros(J)
+        if table:
+            ns = self.lib.oracle_systematic_points_table(U, J, out.ctypes.data_as(_dp))
+            if ns < 0:
+                raise RuntimeError('systematic table overflow')
+        else:
+            self.lib.oracle_systematic_points_sequential(U, J, out.ctypes.data_as(_dp))
+        return out
+
+    def step(self, problem, x, t, sub, normals, noises_off=0):
+        h = native.DescHolder(problem, precision=64)
+        x = np.ascontiguousarray(x, dtype=np.float64).copy()
+        nz = np.ascontiguousarray(normals, dtype=np.float64)
+        self.lib.oracle_step(x.ctypes.data_as(_dp), t, problem.dt, noises_off, C.byref(h.desc), sub,
+                             nz.ctypes.data_as(_dp))
+        return x
+
+    def obs_loglik(self, problem, x, n):
+        h = native.DescHolder(problem, precision=64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        return self.lib.oracle_obs_loglik(x.ctypes.data_as(_dp), C.byref(h.desc), n)
+
+    def obs_moments(self, problem, x, ts, t):
+        h = native.DescHolder(problem, precision=64)
+        mu, var = C.c_double(), C.c_double()
+        self.lib.oracle_obs_moments(x, ts, t, C.byref(h.desc), C.byref(mu), C.byref(var))
+        return mu.value, var.value
+
+    def like(self, y, mu, var, like_min):
+        return self.lib.oracle_like(y, mu, var, like_min)
+
+    def proj2obs(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        obs = np.zeros(self.info.n_ts)
+        self.lib.oracle_proj2obs(x.ctypes.data_as(_dp), obs.ctypes.data_as(_dp))
+        return obs

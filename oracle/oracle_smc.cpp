@@ -1,0 +1,421 @@
+// ORACLE — test infrastructure only.  CPU FP64 restatement of the
+// reference's SMC path, used by tests/ (parity), __graft_entry__.smoke() and
+// the CPU-baseline leg of bench.py.  Nothing in the product links it.
+//
+// Restates, in order of the loop body of run_SMC
+// (model_builder/C/core/smc.c:204-307):
+//   * replicate_J_p_X_0                         smc.c:167-176
+//   * copy X[n] -> X[n+1], reset_inc            smc.c:250-253, prediction_util.c:25-33
+//   * f_prediction_sde_* (while t < t1 step)    prediction_util.c:197-287
+//     with the generated step of the model (the emitted header, whose text
+//     follows core_template.c:215-339 and Ccoder.py:366-508)
+//   * proj2obs, get_log_likelihood, exp()       core_template.c:52-102, likelihood.c:56-70, smc.c:271-273
+//   * weight()                                  smc.c:27-83   (linear space, as the reference)
+//   * systematic_sampling()                     smc.c:90-112  (sequential cumulative sum and ran += inc)
+//   * resample_X()                              smc.c:142-161 (AoS gather)
+// Particles are AoS like struct s_X (plom.h:476-483); the particle loop runs
+// under OpenMP like run_SMC with FLAG_OMP (smc.c:255-274); weighting and
+// resampling are serial like the reference.
+//
+// Draws: either the common-random-number table of the descriptor (every
+// normal and every resampling uniform injected), or Philox4x32-10 with the
+// same counter layout as the GPU's FP64 mode.  The GSL mt19937 / ranlxs0
+// streams of the reference (build.c:1019-1030) cannot be matched by a
+// parallel device and are not reproduced.
+//
+// Deviation kept on purpose: systematic_sampling stops at the last particle
+// when rounding leaves ran above the final cumulative weight (the reference
+// would read past the end of prob[]).
+#include PLOM_MODEL_HEADER
+#include "plomgpu.h"
+
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef plomgen::Model M;
+
+namespace {
+
+struct HostState {
+  static constexpr bool DYNAMIC = true;
+  double* b;
+  double& operator[](int i) const { return b[i]; }
+};
+
+struct HostEnv {
+  const double* par_;
+  const double* cov_;
+  const double* coup_;
+  const int* dgroup_;
+  const int* dng_;
+  const plomgpu_back_transform* dbt_;
+  const double* dvol_;
+  double par(int p, int cac) const { return par_[p * M::N_CAC + cac]; }
+  double cov(int k, int cac) const { return cov_[k * M::N_CAC + cac]; }
+  double coupling(int a, int b) const { return coup_[a * M::N_CAC + b]; }
+  int drift_group(int i, int cac) const { return dgroup_[i * M::N_CAC + cac]; }
+  int drift_ngroups(int i) const { return dng_[i]; }
+  double drift_vol(int i, int g) const { return dvol_[i * M::N_CAC + g]; }
+  double drift_value(int i, int g, double xw) const {
+    plomrt::BackTransform bt;
+    memcpy(&bt, &dbt_[i * M::N_CAC + g], sizeof(bt));
+    return plomrt::back_transform<double>(xw, bt);
+  }
+};
+
+struct HostObsEnv {
+  const double* par_ts_;
+  const double* cov_ts_;
+  double par_ts(int p, int ts) const { return par_ts_[p * M::N_TS + ts]; }
+  double cov_ts(int k, int ts) const { return cov_ts_[k * M::N_TS + ts]; }
+};
+
+template <int V>
+struct TableSource {
+  const double* p;
+  template <int N>
+  void normals(int cac, double* out) const {
+    for (int i = 0; i < N; ++i) out[i] = p[cac * N + i];
+  }
+  double drift_normal(int i, int g) const { return p[M::N_CAC * M::draws_per_cac(V) + i * M::N_CAC + g]; }
+};
+
+template <int V>
+struct PhiloxSource {
+  plomrt::PhiloxKey key;
+  uint32_t j, n, sub;
+  template <int N>
+  void normals(int cac, double* out) const {
+    plomrt::NormalGen<double>::fill<N>(key, j, n, (sub * (uint32_t)(M::N_CAC + 1) + (uint32_t)cac) << 12, out);
+  }
+  double drift_normal(int i, int g) const {
+    double z[1];
+    plomrt::NormalGen<double>::fill<1>(
+        key, j, n, ((sub * (uint32_t)(M::N_CAC + 1) + (uint32_t)M::N_CAC) << 12) + (uint32_t)(i * M::N_CAC + g), z);
+    return z[0];
+  }
+};
+
+int draws_per_substep(int noises_off) {
+  const bool drift = M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT);
+  return M::N_CAC * M::draws_per_cac(noises_off & 3) + (drift ? M::N_DRIFT * M::N_CAC : 0);
+}
+
+template <int V, bool DRIFT>
+void propagate(double* x, const plomgpu_smc_desc* d, int n, int j, int sub0, const double* crn_interval, int D) {
+  HostEnv e;
+  e.par_ = d->par_cac;
+  e.coup_ = d->coupling;
+  e.dgroup_ = d->drift_group;
+  e.dng_ = d->drift_ngroups;
+  e.dbt_ = d->drift_bt;
+  e.dvol_ = d->drift_vol;
+  HostState xs;
+  xs.b = x;
+  const int K = d->n_sub[n];
+  for (int k = 0; k < K; ++k) {
+    const int sub = sub0 + k;
+    e.cov_ = d->cov_cac ? d->cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC : nullptr;
+    const double t = d->t_sub[sub];
+    if (crn_interval) {
+      TableSource<V> src;
+      src.p = crn_interval + ((size_t)j * K + k) * D;
+      M::step<V, DRIFT, double>(xs, t, d->dt, e, src);
+    } else {
+      PhiloxSource<V> src;
+      src.key = plomrt::make_key(d->seed, 0u);
+      src.j = (uint32_t)j;
+      src.n = (uint32_t)n;
+      src.sub = (uint32_t)k;
+      M::step<V, DRIFT, double>(xs, t, d->dt, e, src);
+    }
+  }
+}
+
+typedef void (*PropFn)(double*, const plomgpu_smc_desc*, int, int, int, const double*, int);
+
+PropFn pick(int noises_off) {
+  const int v = noises_off & 3;
+  const bool drift = M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT);
+  if (drift) {
+    switch (v) {
+      case 0: return &propagate<0, true>;
+      case 1: return &propagate<1, true>;
+      case 2: return &propagate<2, true>;
+      default: return &propagate<3, true>;
+    }
+  }
+  switch (v) {
+    case 0: return &propagate<0, false>;
+    case 1: return &propagate<1, false>;
+    case 2: return &propagate<2, false>;
+    default: return &propagate<3, false>;
+  }
+}
+
+double log_likelihood(const double* x, const plomgpu_smc_desc* d, int n) {
+  double obs[M::N_TS];
+  HostState xs;
+  xs.b = const_cast<double*>(x);
+  M::proj2obs<double>(xs, obs);
+  HostObsEnv oe;
+  oe.par_ts_ = d->par_ts;
+  oe.cov_ts_ = d->cov_ts ? d->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS : nullptr;
+  const double* y = d->data + (size_t)n * M::N_TS;
+  double ll = 0.0;
+  for (int ts = 0; ts < M::N_TS; ++ts) {
+    if (isnan(y[ts])) continue;
+    const double mu = M::obs_mean(obs[ts], ts, d->t_obs[n], oe);
+    const double var = M::obs_var(obs[ts], ts, d->t_obs[n], oe);
+    ll += log(plomrt::disc_normal_like(y[ts], mu, var, d->like_min));
+  }
+  return ll;
+}
+
+// weight(), smc.c:27-83
+int weight(std::vector<double>& w, int J, double like_min, double* llike_n, double* ess, double* Llike,
+           int* n_all_fail, uint32_t* select) {
+  double like_tot = 0.0;
+  int nfail = 0;
+  double e = 0.0;
+  const double thresh = pow(like_min, (double)M::N_TS);
+  for (int j = 0; j < J; ++j) {
+    if (w[j] <= thresh) {
+      w[j] = 0.0;
+      nfail += 1;
+    } else {
+      like_tot += w[j];
+      e += w[j] * w[j];
+    }
+  }
+  int success = 1;
+  if (nfail == J) {
+    success = 0;
+    *n_all_fail += 1;
+    *llike_n = log(like_min) * M::N_TS;
+    const double invJ = 1.0 / (double)J;
+    for (int j = 0; j < J; ++j) {
+      w[j] = invJ;
+      select[j] = (uint32_t)j;
+    }
+    e = 0.0;
+  } else {
+    for (int j = 0; j < J; ++j) w[j] /= like_tot;
+    *llike_n = log(like_tot / (double)J);
+    e = (like_tot * like_tot) / e;
+  }
+  *ess = e;
+  *Llike += *llike_n;
+  return success;
+}
+
+// systematic_sampling(), smc.c:90-112, with the end-of-array guard
+void systematic_sampling(const std::vector<double>& prob, int J, double U, uint32_t* select) {
+  const double inc = 1.0 / (double)J;
+  double ran = U;
+  int i = 0;
+  double weight_cum = prob[0];
+  for (int j = 0; j < J; ++j) {
+    while (ran > weight_cum && i < J - 1) {
+      i++;
+      weight_cum += prob[i];
+    }
+    select[j] = (uint32_t)i;
+    ran += inc;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_model_info(plomgpu_model_info* o) {
+  o->n_par_sv = M::N_PAR_SV;
+  o->n_c = M::N_C;
+  o->n_ac = M::N_AC;
+  o->n_cac = M::N_CAC;
+  o->n_ts = M::N_TS;
+  o->n_ts_inc_unique = M::N_TS_INC_UNIQUE;
+  o->n_obs_inc = M::N_OBS_INC;
+  o->n_obs_prev = M::N_OBS_PREV;
+  o->n_drift = M::N_DRIFT;
+  o->off_drift = M::OFF_DRIFT;
+  o->off_inc = M::OFF_INC;
+  o->n_state = M::S;
+  o->n_par_proc = M::N_PAR_PROC;
+  o->n_par_obs = M::N_PAR_OBS;
+  o->n_cov_cac = M::N_COV_CAC;
+  o->n_cov_ts = M::N_COV_TS;
+  o->n_reac = M::N_REAC;
+  o->n_white_noise = M::N_WN;
+  o->coupled = M::COUPLED ? 1 : 0;
+  o->pop_size_eq_sum_sv = M::POP_SIZE_EQ_SUM_SV ? 1 : 0;
+  o->name = M::NAME;
+  return 0;
+}
+
+int oracle_draws_per_substep(int noises_off) { return draws_per_substep(noises_off); }
+
+// run_SMC restated.  n_threads <= 0: OpenMP default.
+int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threads) {
+  const int J = d->J, S = M::S;
+  if (J < 1 || d->precision != 64 && d->precision != 32) return PLOMGPU_EINVAL;
+#ifdef _OPENMP
+  if (n_threads > 0) omp_set_num_threads(n_threads);
+#endif
+  const PropFn prop = pick(d->noises_off);
+  const int D = d->crn_normals ? draws_per_substep(d->noises_off) : 0;
+  // AoS particles: proj[S] per particle, two generations
+  std::vector<double> X((size_t)J * S), Xn((size_t)J * S);
+  for (int j = 0; j < J; ++j)
+    for (int w = 0; w < S; ++w) X[(size_t)j * S + w] = (w < M::OFF_INC) ? d->x0[w] : 0.0;
+  std::vector<double> wts(J);
+  std::vector<uint32_t> select(J);
+  double Llike = 0.0;
+  int n_all_fail = 0;
+  size_t crn_off = 0;
+  int sub0 = 0;
+  for (int n = 0; n < d->n_obs; ++n) {
+    const double* y = d->data + (size_t)n * M::N_TS;
+    int n_nonan = 0;
+    for (int ts = 0; ts < M::N_TS; ++ts)
+      if (!isnan(y[ts])) ++n_nonan;
+    const bool weigh = d->filter && n_nonan > 0;
+    const double* crn_n = d->crn_normals ? d->crn_normals + crn_off : nullptr;
+#pragma omp parallel for schedule(static)
+    for (int j = 0; j < J; ++j) {
+      double* x = &Xn[(size_t)j * S];
+      memcpy(x, &X[(size_t)j * S], sizeof(double) * S);
+      for (int w = M::OFF_INC; w < S; ++w) x[w] = 0.0;  // reset_inc
+      prop(x, d, n, j, sub0, crn_n, D);
+      if (n_nonan) wts[j] = exp(log_likelihood(x, d, n));
+    }
+    if (r->x_pred) {
+      for (int j = 0; j < J; ++j)
+        for (int w = 0; w < S; ++w) r->x_pred[((size_t)n * S + w) * J + j] = Xn[(size_t)j * S + w];
+    }
+    crn_off += (size_t)J * d->n_sub[n] * D;
+    sub0 += d->n_sub[n];
+    double llike_n = 0.0, ess = 0.0;
+    if (weigh) {
+      if (weight(wts, J, d->like_min, &llike_n, &ess, &Llike, &n_all_fail, select.data())) {
+        double u;
+        if (d->crn_normals) {
+          u = d->crn_uniforms[n];
+        } else {
+          u = plomrt::resample_uniform(plomrt::make_key(d->seed, 0u), (uint32_t)n);
+        }
+        const double U = (1.0 / (double)J) * u;
+        systematic_sampling(wts, J, U, select.data());
+      }
+      // resample_X: gather the state words (incidences are reset next interval)
+      for (int j = 0; j < J; ++j) {
+        const size_t s = (size_t)select[j] * S;
+        for (int w = 0; w < S; ++w) X[(size_t)j * S + w] = Xn[s + w];
+      }
+    } else {
+      for (int j = 0; j < J; ++j) select[j] = (uint32_t)j;
+      X.swap(Xn);
+    }
+    if (r->llike_n) r->llike_n[n] = llike_n;
+    if (r->ess_n) r->ess_n[n] = ess;
+    if (r->ancestors) memcpy(r->ancestors + (size_t)n * J, select.data(), sizeof(uint32_t) * J);
+  }
+  if (r->x_final) {
+    for (int j = 0; j < J; ++j)
+      for (int w = 0; w < S; ++w) r->x_final[(size_t)w * J + j] = X[(size_t)j * S + w];
+  }
+  r->loglik = Llike;
+  r->n_all_fail = n_all_fail;
+  r->status = 0;
+  return 0;
+}
+
+// weight() + systematic_sampling() on given likelihoods (known-answer tests).
+int oracle_weight_and_resample(double* w, int J, double like_min, double U, double* llike_n, double* ess,
+                               uint32_t* select) {
+  std::vector<double> v(w, w + J);
+  double Llike = 0.0;
+  int n_all_fail = 0;
+  if (weight(v, J, like_min, llike_n, ess, &Llike, &n_all_fail, select)) systematic_sampling(v, J, U, select);
+  memcpy(w, v.data(), sizeof(double) * J);
+  return n_all_fail;
+}
+
+// Systematic points exactly as the reference walks them (ran += inc).
+void oracle_systematic_points_sequential(double U, int J, double* out) {
+  const double inc = 1.0 / (double)J;
+  double ran = U;
+  for (int j = 0; j < J; ++j) {
+    out[j] = ran;
+    ran += inc;
+  }
+}
+
+// The closed form shared with the device code, evaluated on the host.
+int oracle_systematic_points_table(double U, int J, double* out) {
+  static plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  const int ns = plomrt::systematic_table(U, 1.0 / (double)J, J, seg, plomrt::SYS_MAX_SEG);
+  if (ns < 0) return -1;
+  for (int j = 0; j < J; ++j) out[j] = plomrt::systematic_point(seg, ns, j);
+  return ns;
+}
+
+// One generated Euler step of one particle with injected normals (golden-vector checks).
+int oracle_step(double* x, double t, double dt, int noises_off, const plomgpu_smc_desc* d, int sub,
+                const double* normals) {
+  HostEnv e;
+  e.par_ = d->par_cac;
+  e.cov_ = d->cov_cac ? d->cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC : nullptr;
+  e.coup_ = d->coupling;
+  e.dgroup_ = d->drift_group;
+  e.dng_ = d->drift_ngroups;
+  e.dbt_ = d->drift_bt;
+  e.dvol_ = d->drift_vol;
+  HostState xs;
+  xs.b = x;
+  const int v = noises_off & 3;
+  const bool drift = M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT);
+#define ORACLE_STEP(VV, DD)              \
+  {                                      \
+    TableSource<VV> src;                 \
+    src.p = normals;                     \
+    M::step<VV, DD, double>(xs, t, dt, e, src); \
+  }
+  if (drift) {
+    if (v == 0) ORACLE_STEP(0, true) else if (v == 1) ORACLE_STEP(1, true) else if (v == 2) ORACLE_STEP(2, true) else ORACLE_STEP(3, true)
+  } else {
+    if (v == 0) ORACLE_STEP(0, false) else if (v == 1) ORACLE_STEP(1, false) else if (v == 2) ORACLE_STEP(2, false) else ORACLE_STEP(3, false)
+  }
+#undef ORACLE_STEP
+  return 0;
+}
+
+// Observation density of one series (golden-vector checks).
+double oracle_obs_loglik(const double* x, const plomgpu_smc_desc* d, int n) { return log_likelihood(x, d, n); }
+
+// Mean and variance of the observation model of series ts at time t (golden-vector checks).
+void oracle_obs_moments(double x, int ts, double t, const plomgpu_smc_desc* d, double* mu, double* var) {
+  HostObsEnv oe;
+  oe.par_ts_ = d->par_ts;
+  oe.cov_ts_ = d->cov_ts;
+  *mu = M::obs_mean(x, ts, t, oe);
+  *var = M::obs_var(x, ts, t, oe);
+}
+
+double oracle_like(double y, double mu, double var, double like_min) {
+  return plomrt::disc_normal_like(y, mu, var, like_min);
+}
+
+void oracle_proj2obs(const double* x, double* obs) {
+  HostState xs;
+  xs.b = const_cast<double*>(x);
+  M::proj2obs<double>(xs, obs);
+}
+
+}  // extern "C"

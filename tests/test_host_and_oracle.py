@@ -1,0 +1,178 @@
+"""CPU tests: the C ABI library loads and exports its header, the host-side
+parameter / time / covariate logic, and known answers of the oracle."""
+
+import ctypes
+import math
+import os
+import re
+
+import numpy as np
+import pytest
+
+import models
+from plomgpu import native, problem, theta, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, 'include', 'plomgpu.h')).read()
+    return sorted(set(re.findall(r'\b(plomgpu_\w+)\s*\(', text)))
+
+
+def test_header_symbols_are_bound():
+    assert header_symbols() == sorted(native.API_SYMBOLS)
+
+
+@pytest.mark.parametrize('name', ['sir', 'seir3'])
+def test_library_loads_and_exports_every_symbol(name):
+    path = models.build_gpu(name)
+    lib = ctypes.CDLL(path)
+    for sym in header_symbols():
+        assert hasattr(lib, sym), sym
+    eng = native.Engine(models.lib_name(name))
+    m = models.plom_model(name)
+    info = eng.info
+    assert info.n_cac == m.N_CAC and info.n_ts == m.N_TS and info.n_par_sv == len(m.par_sv)
+    assert info.n_state == len(m.par_sv) * m.N_CAC + len(m.drift_par_proc) * m.N_CAC + m.N_TS_INC_UNIQUE
+    assert eng.draws_per_substep(0) == m.N_CAC * (len(m.proc_model) + len(m.white_noise))
+    assert eng.draws_per_substep(3) == 0
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip('a GPU is present')
+    except ImportError:
+        pass
+    eng = models.engine('sir')
+    p = models.make_problem('sir', J=16, dt=1.0)
+    with pytest.raises(native.PlomGpuError) as e:
+        eng.smc(p)
+    assert e.value.code in (2, 5)
+
+
+def test_bad_descriptor_is_rejected():
+    eng = models.engine('sir')
+    p = models.make_problem('sir', J=16, dt=1.0)
+    p.J = 0
+    with pytest.raises(native.PlomGpuError) as e:
+        eng.smc(p)
+    assert e.value.code == 1
+
+
+# ------------------------------------------------------------------ host logic
+def test_units_and_transforms():
+    # rate_as_duration 5 days in data unit days -> 1/(1e-5 + 5) (transform.c:462-481)
+    r = theta.Router('v', {'unit': 'D', 'type': 'rate_as_duration', 'transformation': 'log',
+                           'group': {'all': {'min': {'value': 5}, 'max': {'value': 5}, 'guess': {'value': 5}}}},
+                     {'group': [{'id': 'all', 'population_id': ['a']}]}, ['a'], 'population_id')
+    assert r.natural(0) == pytest.approx(1.0 / (1e-5 + 5.0), rel=1e-15)
+    # a rate per year in day units
+    assert theta.get_multiplier('D', {'unit': 'Y'}) == pytest.approx(1.0 / 365.0)
+    # logit round trip and its clamps
+    for x in (1e-20, 0.3, 0.999999999999):
+        z = theta.f_forward('logit', x, 0, 0)
+        back = theta.back_transform(z, (2, 0, 0, 0.0, 0.0, 1.0))
+        assert back == pytest.approx(min(max(x, theta.ZERO_LOG), theta.ONE_LOGIT), rel=1e-9)
+    # logit_ab stays in [a, b]
+    for z in (-50.0, -1.0, 0.0, 2.0, 50.0):
+        v = theta.back_transform(z, (3, 0, 0, 2.0, 7.0, 1.0))
+        assert 2.0 <= v <= 7.0
+
+
+def test_dt_rounding_and_substeps():
+    assert problem.round_dt(0.3) == 1.0 / 3.0
+    assert problem.round_dt(1.0) == 1.0
+    # replaying ``while (t < t1) t += dt`` (prediction_util.c:275-287): 0.1 accumulates
+    # rounding and gives one extra step over 7 days
+    assert len(problem.substep_times(0, 7, 1.0)) == 7
+    n = len(problem.substep_times(0, 7, 0.1))
+    t, k = 0.0, 0
+    while t < 7:
+        t += 0.1
+        k += 1
+    assert n == k
+
+
+def test_natural_cubic_spline_matches_definition():
+    x = [0.0, 7.0, 14.0, 21.0, 35.0, 50.0]
+    y = [1.0, 3.0, 2.0, 5.0, 4.0, 4.5]
+    sp = problem.Spline(x, y)
+    for xi, yi in zip(x, y):
+        assert sp(xi) == pytest.approx(yi, abs=1e-12)
+    # second derivative vanishes at the ends and is continuous inside
+    h = 1e-4
+    d2 = lambda t: (sp(t + h) - 2 * sp(t) + sp(t - h)) / h ** 2
+    assert abs(d2(0.0 + 2 * h)) < 1e-3 and abs(d2(50.0 - 2 * h)) < 1e-3
+    assert d2(7.0 - 1e-3) == pytest.approx(d2(7.0 + 1e-3), abs=5e-3)
+    lin = problem.Spline([0.0, 10.0], [1.0, 3.0])
+    assert lin(5.0) == pytest.approx(2.0)
+    assert problem.Spline([0.0], [4.0])(123.0) == 4.0
+
+
+def test_initial_conditions_and_tables():
+    p = models.make_problem('sir', J=8, dt=1.0)
+    assert p.x0[:3] == pytest.approx([4e5, 100.0, 599900.0])
+    assert p.x0[3] == 0.0
+    m = p.model
+    assert p.par_cac.shape == (len(m.par_proc), m.N_CAC)
+    assert p.cov_cac.shape[0] == int(p.n_sub.sum())
+
+
+# ------------------------------------------------------------------ oracle known answers
+def test_systematic_sampling_known_answer():
+    orc = models.build_oracle('sir')
+    likes = [0.1, 0.2, 0.3, 0.4]
+    w, sel, ll, ess, fail = orc.weight_and_resample(likes, U=0.5 / 4)
+    # points 0.125, 0.375, 0.625, 0.875 against cumulative 0.1, 0.3, 0.6, 1.0
+    assert list(sel) == [1, 2, 3, 3]
+    assert ll == pytest.approx(math.log(1.0 / 4))
+    assert ess == pytest.approx(1.0 / (0.01 + 0.04 + 0.09 + 0.16))
+    assert fail == 0
+    assert w == pytest.approx([0.1, 0.2, 0.3, 0.4])
+
+
+def test_weight_failure_rule_known_answer():
+    orc = models.build_oracle('sir')   # one series: failure iff like <= LIKE_MIN
+    likes = [1e-17, 1e-17, 1e-17]
+    w, sel, ll, ess, fail = orc.weight_and_resample(likes, U=0.1)
+    assert fail == 1 and list(sel) == [0, 1, 2] and ess == 0.0
+    assert ll == pytest.approx(math.log(1e-17))
+    likes = [1e-17, 2e-17, 0.0]
+    w, sel, ll, ess, fail = orc.weight_and_resample(likes, U=0.1)
+    assert fail == 0 and list(sel) == [1, 1, 1]
+
+
+@pytest.mark.parametrize('J', [1, 7, 1000, 12345, 1 << 17])
+def test_systematic_closed_form_matches_sequential_additions(J):
+    orc = models.build_oracle('sir')
+    rng = np.random.default_rng(J)
+    inc = 1.0 / J
+    for U in [0.0, 5e-324, inc * 1e-9, np.nextafter(inc, 0.0)] + list(rng.uniform(0, inc, 20)):
+        np.testing.assert_array_equal(orc.systematic_points(U, J, table=True), orc.systematic_points(U, J))
+
+
+def test_oracle_threads_do_not_change_results():
+    orc = models.build_oracle('seir3')
+    p = models.make_problem('seir3', J=300, dt=1.0, precision=64, seed=9)
+    a = orc.smc(p, n_threads=1, ancestors=True)
+    b = orc.smc(p, n_threads=4, ancestors=True)
+    assert a.loglik == b.loglik
+    np.testing.assert_array_equal(a.ancestors, b.ancestors)
+
+
+def test_oracle_crn_is_deterministic_and_sensitive():
+    orc = models.build_oracle('sir_short')
+    p = models.make_problem('sir_short', J=200, dt=1.0, precision=64)
+    D = orc.draws_per_substep(0)
+    rng = np.random.default_rng(1)
+    z = rng.standard_normal(p.J * int(p.n_sub.sum()) * D)
+    u = rng.uniform(size=p.n_obs)
+    a = orc.smc(p, crn_normals=z, crn_uniforms=u)
+    b = orc.smc(p, crn_normals=z, crn_uniforms=u)
+    assert a.loglik == b.loglik
+    z2 = z.copy()
+    z2[0] += 1.0
+    assert orc.smc(p, crn_normals=z2, crn_uniforms=u).loglik != a.loglik
