@@ -42,6 +42,7 @@ def parse():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
     return ap.parse_args()
 
 
@@ -256,7 +257,7 @@ def main():
     # end to end through the one-shot C ABI call with host buffers
     from plomgpu.native import DescHolder
     e2e_times = []
-    for i in range(max(1, min(args.steps, 3))):
+    for i in range(args.e2e_runs):
         barrier()
         t0 = time.perf_counter()
         out = eng.smc(prob)
@@ -264,11 +265,11 @@ def main():
     h = DescHolder(prob)
     h2d = sum(a.nbytes for a in h.arrays.values())
     d2h = 8 * 2 * prob.n_obs + 16
-    e2e_s = statistics.median(e2e_times)
+    e2e_s = statistics.median(e2e_times) if e2e_times else float('nan')
     tt = torch.tensor([e2e_s], device='cuda')
     if dist is not None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = psteps * world / float(tt.item())
+    e2e_value = psteps * world / float(tt.item()) if e2e_times else None
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
