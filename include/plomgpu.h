@@ -154,6 +154,32 @@ void plomgpu_plan_destroy(plomgpu_plan *plan);
  * the device-side closed form (GPU) into out[J]. */
 int plomgpu_debug_systematic_points(double U, int J, double *out);
 
+/* Resamples one observation interval without allocating device memory.
+ *
+ * No counterpart in the reference.  For callers that cannot allocate: a
+ * plug-in inside a runtime whose caching allocator owns the GPU memory, or a
+ * latency-bounded serving loop in which cudaMalloc / cudaFree would
+ * synchronise the device.  Runs the weighting (failure rule, log-sum-exp
+ * normalisation, ESS), the cumulative weights and the systematic ancestor
+ * search of one interval (smc.c:27-112 semantics) on caller-owned device
+ * buffers:
+ *   log_weights  device, J values (float when precision == 32, double when 64)
+ *   u            uniform in [0, 1): the systematic offset is U = u / J
+ *   ancestors    device, J values written
+ *   out          device, 4 doubles written: log mean weight, ESS, all-fail
+ *                flag (1.0 when every particle failed: identity ancestors),
+ *                error flags (nonzero: a bounded wait ran out, result invalid)
+ *   stream       cudaStream_t the work is queued on (NULL: legacy stream)
+ * The work is asynchronous on `stream`; read `out` after synchronising it.
+ * Scratch is one fixed array of this library (about 2.1 MB, held on every
+ * GPU that loads the library until exit), so J is limited to 262144
+ * (PLOMGPU_EINVAL beyond).  Calls that overlap on the GPU, on any stream of
+ * the same device, race on that array and must be serialised by the caller.
+ * The first call on each device looks up the array's device address: make it
+ * before any stream capture on that device. */
+int plomgpu_resample_noalloc(const void *log_weights, int precision, int J, double like_min, double u,
+                             uint32_t *ancestors, double *out, void *stream);
+
 const char *plomgpu_last_error(void);
 
 #ifdef __cplusplus

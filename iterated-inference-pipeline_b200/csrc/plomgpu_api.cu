@@ -13,6 +13,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -628,3 +629,92 @@ int plomgpu_debug_systematic_points(double U, int J, double* out) {
 const char* plomgpu_last_error(void) { return g_err.c_str(); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Resampling without allocation.
+//
+// Some callers cannot allocate device memory: a plug-in hosted inside another
+// runtime whose caching allocator owns the GPU memory (a raw cudaMalloc there
+// bypasses the pool and can fail or stall once the pool holds the memory),
+// and latency-bounded loops such as a serving loop, where cudaMalloc and
+// cudaFree synchronise the device.  For them plomgpu_resample_noalloc runs the
+// weighting / cumulative-weight / ancestor kernels of one observation interval
+// on caller-owned inputs and outputs, with its scratch in the fixed array
+// below instead of allocated buffers.
+namespace {
+
+constexpr int kNoAllocMaxJ = 1 << 18;  // largest particle count the fixed scratch serves
+constexpr int kNoAllocTiles = (kNoAllocMaxJ + kTile - 1) / kTile;
+
+struct NoAllocScratch {
+  LseAcc part[kMaxWeightBlocks];
+  StepState st;
+  FilterAcc acc;
+  TileStatus tstat[kNoAllocTiles];
+  double C[kNoAllocMaxJ];
+};
+
+// Shared by every call on a device and held by every GPU that loads this
+// library until the process exits (about 2.1 MB).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {nullptr};
+
+__global__ void k_noalloc_out(const StepState* st, const FilterAcc* acc, double* out) {
+  out[2] = (double)st->all_fail;
+  out[3] = (double)acc->error;
+}
+
+template <class T>
+int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, double* out, cudaStream_t s,
+                NoAllocScratch* sc) {
+  const double thresh = pow(like_min, (double)M::N_TS);
+  int nblk = (J + kBtWeight * 4 - 1) / (kBtWeight * 4);
+  if (nblk > kMaxWeightBlocks) nblk = kMaxWeightBlocks;
+  if (nblk < 1) nblk = 1;
+  const int ntiles = (J + kTile - 1) / kTile;
+  // the accumulator and its tickets must start at zero; the previous call's
+  // contents are still there
+  k_reset_acc<<<1, 1, 0, s>>>(&sc->acc);
+  k_weight<T, kBtWeight><<<nblk, kBtWeight, 0, s>>>(lw, J, thresh, log(like_min), sc->part, &sc->st, &sc->acc,
+                                                   sc->tstat, ntiles, 0, u, nullptr, 0u, out, out + 1);
+  k_scan<T, kBtScan, kIptScan><<<ntiles, kBtScan, 0, s>>>(lw, J, thresh, &sc->st, sc->tstat, &sc->acc, sc->C);
+  k_search<kBtSearch><<<(J + kBtSearch - 1) / kBtSearch, kBtSearch, 0, s>>>(sc->C, J, &sc->st, anc, nullptr);
+  k_noalloc_out<<<1, 1, 0, s>>>(&sc->st, &sc->acc, out);
+  CK(cudaGetLastError());
+  return PLOMGPU_OK;
+}
+
+}  // namespace
+
+extern "C" int plomgpu_resample_noalloc(const void* log_weights, int precision, int J, double like_min, double u,
+                                        uint32_t* ancestors, double* out, void* stream) {
+  if (!log_weights || !ancestors || !out) return fail(PLOMGPU_EINVAL, "null pointer");
+  if (precision != 32 && precision != 64) return fail(PLOMGPU_EINVAL, "precision must be 32 or 64");
+  if (J < 1) return fail(PLOMGPU_EINVAL, "J must be >= 1");
+  if (J > kNoAllocMaxJ)
+    return fail(PLOMGPU_EINVAL, "J = " + std::to_string(J) + " exceeds the no-allocation limit of " +
+                                    std::to_string(kNoAllocMaxJ) + " particles");
+  if (!(like_min > 0.0)) return fail(PLOMGPU_EINVAL, "like_min must be > 0");
+  if (!(u >= 0.0 && u < 1.0)) return fail(PLOMGPU_EINVAL, "u must be in [0, 1)");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(PLOMGPU_EINVAL, "device index out of range");
+  void* base = nullptr;
+  {
+    // set-up, once per device, with that device current: the symbol's
+    // address on this device (the host-side name is not a device address)
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+      g_noalloc_ptr[dev] = p;
+    }
+    base = g_noalloc_ptr[dev];
+  }
+  NoAllocScratch* sc = reinterpret_cast<NoAllocScratch*>(base);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (precision == 64) return noalloc_run<double>((const double*)log_weights, J, like_min, u, ancestors, out, s, sc);
+  return noalloc_run<float>((const float*)log_weights, J, like_min, u, ancestors, out, s, sc);
+}

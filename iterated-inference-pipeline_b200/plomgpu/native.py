@@ -54,7 +54,7 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_create_ex', 'plomgpu_plan_propagate_time',
                'plomgpu_plan_update', 'plomgpu_plan_launch', 'plomgpu_plan_results', 'plomgpu_plan_stream',
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
-               'plomgpu_last_error']
+               'plomgpu_resample_noalloc', 'plomgpu_last_error']
 
 
 def _ptr(a, t):
@@ -142,6 +142,8 @@ def _declare(lib):
     lib.plomgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_plan_destroy.restype = None
     lib.plomgpu_debug_systematic_points.argtypes = [C.c_double, C.c_int, _dp]
+    lib.plomgpu_resample_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
     lib.plomgpu_last_error.restype = C.c_char_p
     return lib
 

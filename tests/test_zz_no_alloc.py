@@ -1,0 +1,85 @@
+"""plomgpu_resample_noalloc: the resampling step for callers that cannot
+allocate device memory (a plug-in whose host runtime owns the GPU memory
+through its own caching allocator, or a latency-bounded serving loop where
+cudaMalloc would synchronise the device).
+
+The entry point is checked against the regular entry point plomgpu_smc_run:
+one observation interval is filtered with common random numbers, the
+log-weights of its propagated particles are recomputed with the oracle, and
+the no-allocation call on those log-weights must give the same ancestors
+(bit-exact), log mean weight (1e-9) and ESS (1e-8), on two calls in a row
+and on a second, different problem (the fixed scratch keeps the previous
+call's contents).  This file is collected last on purpose.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+import models
+from plomgpu import native
+
+pytestmark = pytest.mark.gpu
+
+
+def _reference_interval(J, seed):
+    eng = models.engine('sir_short')
+    orc = models.build_oracle('sir_short')
+    p = models.make_problem('sir_short', J=J, dt=1.0, precision=64, seed=seed, nb_obs=1)
+    D = eng.draws_per_substep(0)
+    rng = np.random.Generator(np.random.Philox(seed))
+    z = rng.standard_normal(p.J * int(p.n_sub.sum()) * D)
+    u = rng.uniform(0.0, 1.0, size=p.n_obs)
+    g = eng.smc(p, crn_normals=z, crn_uniforms=u, ancestors=True, x_pred=True)
+    x = g.x_pred[0]
+    lw = np.array([orc.obs_loglik(p, x[:, j], 0) for j in range(J)])
+    return eng, g, lw, float(u[0])
+
+
+def _noalloc(eng, lw, u, like_min=1e-17):
+    import torch
+    J = len(lw)
+    d_lw = torch.tensor(lw, dtype=torch.float64, device='cuda')
+    d_anc = torch.full((J,), -1, dtype=torch.int32, device='cuda')
+    d_out = torch.full((4,), -7.0, dtype=torch.float64, device='cuda')
+    stream = torch.cuda.current_stream()
+    rc = eng.lib.plomgpu_resample_noalloc(ctypes.c_void_p(d_lw.data_ptr()), 64, J, like_min, u,
+                                          ctypes.c_void_p(d_anc.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
+                                          ctypes.c_void_p(stream.cuda_stream))
+    native.check(eng.lib, rc)
+    torch.cuda.synchronize()
+    return d_anc.cpu().numpy().astype(np.uint32), d_out.cpu().numpy()
+
+
+def _check(g, anc, out):
+    np.testing.assert_array_equal(anc, g.ancestors[0])
+    assert out[0] == pytest.approx(g.llike_n[0], rel=1e-9)
+    assert out[1] == pytest.approx(g.ess_n[0], rel=1e-8)
+    assert out[2] == 0.0
+    assert out[3] == 0.0
+
+
+def test_noalloc_matches_smc_run_twice_in_a_row():
+    eng, g, lw, u = _reference_interval(3000, seed=41)
+    anc1, out1 = _noalloc(eng, lw, u)
+    _check(g, anc1, out1)
+    anc2, out2 = _noalloc(eng, lw, u)
+    _check(g, anc2, out2)
+    np.testing.assert_array_equal(anc1, anc2)
+    assert np.array_equal(out1, out2)
+    # a different problem size right after: nothing of the previous call leaks
+    eng, g, lw, u = _reference_interval(4097, seed=42)
+    anc3, out3 = _noalloc(eng, lw, u)
+    _check(g, anc3, out3)
+
+
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    import torch
+    eng = models.engine('sir_short')
+    J = (1 << 18) + 1
+    d = torch.zeros(4, dtype=torch.float64, device='cuda')
+    rc = eng.lib.plomgpu_resample_noalloc(ctypes.c_void_p(d.data_ptr()), 64, J, 1e-17, 0.5,
+                                          ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()), None)
+    assert rc == 1
+    assert b'no-allocation limit' in eng.lib.plomgpu_last_error()
