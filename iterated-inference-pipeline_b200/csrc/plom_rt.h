@@ -38,6 +38,11 @@
 
 namespace plomrt {
 
+template <class T>
+struct V4 {
+  T a, b, c, d;
+};
+
 // ---------------------------------------------------------------- special functions
 template <class T> PLOM_HD T heaviside_(T x) { return (x < T(0)) ? T(0) : T(1); }
 template <class T> PLOM_HD T ramp_(T x) { return (x >= T(0)) ? x : T(0); }

@@ -194,8 +194,8 @@ int enqueue_filter(plomgpu_plan* p) {
 
   PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn);
   if (!kp) return fail(PLOMGPU_EINVAL, "common random numbers need precision 64");
-  const size_t smem = kSmem ? (size_t)M::S * kBtProp * sizeof(T) : 0;
-  if (smem > 0) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = propagate_smem_bytes<T, kSmem, kBtProp>();
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
   const int n_par = M::N_PAR_PROC * M::N_CAC;
   if (n_par > 0) {

@@ -56,9 +56,12 @@ struct ProcEnv {
   const int* dng_;
   const plomrt::BackTransform* dbt_;
   const T* dvol_;
-  __device__ __forceinline__ T par(int p, int cac) const { return __ldg(par_ + p * M::N_CAC + cac); }
+  __device__ __forceinline__ T par(int p, int cac) const { return par_[p * M::N_CAC + cac]; }
   __device__ __forceinline__ T cov(int k, int cac) const { return __ldg(cov_ + k * M::N_CAC + cac); }
-  __device__ __forceinline__ T coupling(int a, int b) const { return __ldg(coup_ + a * M::N_CAC + b); }
+  __device__ __forceinline__ T coupling(int a, int b) const { return coup_[a * M::N_CAC + b]; }
+  __device__ __forceinline__ plomrt::V4<T> coupling4(int a, int b) const {
+    return *reinterpret_cast<const plomrt::V4<T>*>(coup_ + a * M::N_CAC + b);
+  }
   __device__ __forceinline__ int drift_group(int i, int cac) const { return __ldg(dgroup_ + i * M::N_CAC + cac); }
   __device__ __forceinline__ int drift_ngroups(int i) const { return __ldg(dng_ + i); }
   __device__ __forceinline__ T drift_vol(int i, int g) const { return __ldg(dvol_ + i * M::N_CAC + g); }
@@ -77,6 +80,7 @@ struct ObsEnv {
 // ------------------------------------------------------------------ draw sources
 template <class T, int V>
 struct PhiloxDraws {
+  static constexpr int PER_BLOCK = plomrt::NormalGen<T>::per_block();
   plomrt::PhiloxKey key;
   uint32_t j, n, sub;
   template <int N>
@@ -93,6 +97,7 @@ struct PhiloxDraws {
 
 template <class T, int V>
 struct TableDraws {
+  static constexpr int PER_BLOCK = 1;
   const double* p;  // draws of this particle and substep
   template <int N>
   __device__ __forceinline__ void normals(int cac, T* out) const {
@@ -142,9 +147,29 @@ struct StepArgs {
 };
 
 // ------------------------------------------------------------------ propagate
+// shared-memory layout of k_propagate: coupling matrix, per-cac parameters
+// (both read by every thread with the same address), then the state
+// columns of the block's particles when the state does not fit registers
+constexpr int pad4(int n) { return (n + 3) & ~3; }
+constexpr int kSmemCoup = M::COUPLED ? pad4(M::N_CAC * M::N_CAC) : 0;
+constexpr int kSmemPar = pad4(M::N_PAR_PROC * M::N_CAC);
+
+template <class T, bool SMEM, int BT>
+constexpr size_t propagate_smem_bytes() {
+  return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) + (SMEM ? (size_t)M::S * BT * sizeof(T) : 0);
+}
+
 template <class T, int V, bool DRIFT, bool CRN, bool SMEM, int BT>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_coup = reinterpret_cast<T*>(smem_raw);
+  T* s_par = s_coup + kSmemCoup;
+  T* s_state = s_par + kSmemPar;
+  if constexpr (M::COUPLED) {
+    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = tb.coupling[i];
+  }
+  for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
+  __syncthreads();
   const int J = tb.J;
   const int j = blockIdx.x * BT + threadIdx.x;
   if (j >= J) return;
@@ -155,7 +180,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   typedef typename std::conditional<SMEM, SmemState<T, BT>, RegState<T, M::S>>::type Store;
   Store x;
   if constexpr (SMEM) {
-    x.b = reinterpret_cast<T*>(smem_raw) + threadIdx.x;
+    x.b = s_state + threadIdx.x;
   }
 #pragma unroll
   for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * J + src];
@@ -163,8 +188,8 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);  // reset_inc
 
   ProcEnv<T> e;
-  e.par_ = tb.par_cac;
-  e.coup_ = tb.coupling;
+  e.par_ = s_par;
+  e.coup_ = s_coup;
   e.dgroup_ = tb.drift_group;
   e.dng_ = tb.drift_ngroups;
   e.dbt_ = tb.drift_bt;

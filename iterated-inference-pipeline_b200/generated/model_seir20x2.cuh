@@ -22,99 +22,131 @@ struct Model {
     constexpr int tab[N_CAC][INC_PER_CAC] = {{0},{0},{1},{1},{2},{2},{3},{3},{4},{4},{5},{5},{6},{6},{7},{7},{8},{8},{9},{9},{10},{10},{11},{11},{12},{12},{13},{13},{14},{14},{15},{15},{16},{16},{17},{17},{18},{18},{19},{19}};
     return tab[cac][k];
   }
-  template <int V, bool DRIFT, class T, class X, class E, class D>
-  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {
-    (void)t;
-    constexpr int NW = draws_per_cac(V);
-    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-PLOM_UNROLL
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+  template <class T>
+  struct Pre {
     T yf_I[N_CAC];
-PLOM_UNROLL
-    for (int c2 = 0; c2 < N_CAC; ++c2) {
-      yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
+    int unused;
+  };
+  template <int V, bool DRIFT, class T, class X, class E>
+  PLOM_HD static void cac_body(X& x, const int cac, const T* nz, const T t, const T dt, const E& e,
+                               T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
+    (void)t; (void)nz; (void)pre;
+    const T xo_S = x[0*N_CAC+cac];
+    const T xo_E = x[1*N_CAC+cac];
+    const T xo_I = x[2*N_CAC+cac];
+    const T xo_R = x[3*N_CAC+cac];
+    T foi_I = T(0);
+    PLOM_UNROLL
+    for (int c2 = 0; c2 < N_CAC; c2 += 4) {
+      const plomrt::V4<T> w4 = e.coupling4(cac, c2);
+      foi_I += w4.a * pre.yf_I[c2];
+      foi_I += w4.b * pre.yf_I[c2 + 1];
+      foi_I += w4.c * pre.yf_I[c2 + 2];
+      foi_I += w4.d * pre.yf_I[c2 + 3];
     }
-    PLOM_PRAGMA_CAC
-    for (int cac = 0; cac < N_CAC; ++cac) {
-      const T xo_S = x[0*N_CAC+cac];
-      const T xo_E = x[1*N_CAC+cac];
-      const T xo_I = x[2*N_CAC+cac];
-      const T xo_R = x[3*N_CAC+cac];
-      T foi_I = T(0);
-PLOM_UNROLL
-      for (int c2 = 0; c2 < N_CAC; ++c2) foi_I += e.coupling(cac, c2) * yf_I[c2];
-      const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-      const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
-      const T r2 = e.par(2, cac);
-      const T r3 = e.par(1, cac);
-      const T r4 = e.par(5, cac);
-      T nz[NW > 0 ? NW : 1];
-      draws.template normals<NW>(cac, nz);
-      const T sqdt = sqrt(dt);
-      (void)sqdt;
-      int q = 0; (void)q;
-      const T dem_0 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_1 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_2 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_3 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_4 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_5 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_6 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T dem_7 = (V & 1) ? T(0) : sqdt*nz[q++];
-      const T wn_0 = (V & 2) ? T(0) : sqdt*nz[q++];
-      T incterm_0;
-      switch (V) {
-        case 0: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
-        case 1: incterm_0 = (+ (r3*xo_I))*dt; break;
-        case 2: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
-        case 3: incterm_0 = (+ (r3*xo_I))*dt; break;
-      }
-      T f_S;
-      switch (V) {
-        case 0: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0 - (r1*xo_S)*e.par(3, cac)*wn_0; break;
-        case 1: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - (r1*xo_S)*e.par(3, cac)*wn_0; break;
-        case 2: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0; break;
-        case 3: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt; break;
-      }
-      T f_E;
-      switch (V) {
-        case 0: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1 + (r1*xo_S)*e.par(3, cac)*wn_0; break;
-        case 1: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt + (r1*xo_S)*e.par(3, cac)*wn_0; break;
-        case 2: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1; break;
-        case 3: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt; break;
-      }
-      T f_I;
-      switch (V) {
-        case 0: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
-        case 1: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
-        case 2: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
-        case 3: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
-      }
-      T f_R;
-      switch (V) {
-        case 0: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
-        case 1: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
-        case 2: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
-        case 3: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
-      }
-PLOM_UNROLL
-      for (int k = 0; k < INC_PER_CAC; ++k) {
-        const int l = inc_link(cac, k);
-        if (l < 0) break;
-        const int o = l >> 10, w = l & 1023;
-PLOM_UNROLL
-        for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {
-          if (ww == w) {
-            if (o == 0) inc_acc[ww] += incterm_0;
-          }
+    const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
+    const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
+    const T r2 = e.par(2, cac);
+    const T r3 = e.par(1, cac);
+    const T r4 = e.par(5, cac);
+    const T sqdt = sqrt(dt);
+    (void)sqdt;
+    int q = 0; (void)q;
+    const T dem_0 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_1 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_2 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_3 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_4 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_5 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_6 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T dem_7 = (V & 1) ? T(0) : sqdt*nz[q++];
+    const T wn_0 = (V & 2) ? T(0) : sqdt*nz[q++];
+    T incterm_0;
+    switch (V) {
+      case 0: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
+      case 1: incterm_0 = (+ (r3*xo_I))*dt; break;
+      case 2: incterm_0 = (+ (r3*xo_I))*dt + sqrt(r3*xo_I)*dem_3; break;
+      case 3: incterm_0 = (+ (r3*xo_I))*dt; break;
+    }
+    T f_S;
+    switch (V) {
+      case 0: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0 - (r1*xo_S)*e.par(3, cac)*wn_0; break;
+      case 1: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - (r1*xo_S)*e.par(3, cac)*wn_0; break;
+      case 2: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt - sqrt(r1*xo_S)*dem_1 - sqrt(r4*xo_S)*dem_4 + sqrt(r0)*dem_0; break;
+      case 3: f_S = xo_S + (- (r1*xo_S) - (r4*xo_S) + (r0))*dt; break;
+    }
+    T f_E;
+    switch (V) {
+      case 0: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1 + (r1*xo_S)*e.par(3, cac)*wn_0; break;
+      case 1: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt + (r1*xo_S)*e.par(3, cac)*wn_0; break;
+      case 2: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt - sqrt(r2*xo_E)*dem_2 - sqrt(r4*xo_E)*dem_5 + sqrt(r1*xo_S)*dem_1; break;
+      case 3: f_E = xo_E + (- (r2*xo_E) - (r4*xo_E) + (r1*xo_S))*dt; break;
+    }
+    T f_I;
+    switch (V) {
+      case 0: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
+      case 1: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
+      case 2: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt - sqrt(r3*xo_I)*dem_3 - sqrt(r4*xo_I)*dem_6 + sqrt(r2*xo_E)*dem_2; break;
+      case 3: f_I = xo_I + (- (r3*xo_I) - (r4*xo_I) + (r2*xo_E))*dt; break;
+    }
+    T f_R;
+    switch (V) {
+      case 0: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
+      case 1: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
+      case 2: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt - sqrt(r4*xo_R)*dem_7 + sqrt(r3*xo_I)*dem_3; break;
+      case 3: f_R = xo_R + (- (r4*xo_R) + (r3*xo_I))*dt; break;
+    }
+    PLOM_UNROLL
+    for (int k = 0; k < INC_PER_CAC; ++k) {
+      const int l = inc_link(cac, k);
+      if (l < 0) break;
+      const int o = l >> 10, w = l & 1023;
+      PLOM_UNROLL
+      for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {
+        if (ww == w) {
+          if (o == 0) inc_acc[ww] += incterm_0;
         }
       }
-      x[0*N_CAC+cac] = (f_S < T(0)) ? T(0) : f_S;
-      x[1*N_CAC+cac] = (f_E < T(0)) ? T(0) : f_E;
-      x[2*N_CAC+cac] = (f_I < T(0)) ? T(0) : f_I;
-      x[3*N_CAC+cac] = (f_R < T(0)) ? T(0) : f_R;
     }
-PLOM_UNROLL
+    x[0*N_CAC+cac] = (f_S < T(0)) ? T(0) : f_S;
+    x[1*N_CAC+cac] = (f_E < T(0)) ? T(0) : f_E;
+    x[2*N_CAC+cac] = (f_I < T(0)) ? T(0) : f_I;
+    x[3*N_CAC+cac] = (f_R < T(0)) ? T(0) : f_R;
+  }
+  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)
+  static constexpr PLOM_HD int draw_group(int nw, int per_block) {
+    int g = 1;
+    while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;
+    return (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;
+  }
+  template <int V, bool DRIFT, class T, class X, class E, class D>
+  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {
+    constexpr int NW = draws_per_cac(V);
+    constexpr int G = draw_group(NW, D::PER_BLOCK);
+    constexpr int NMAIN = N_CAC - (N_CAC % G);
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+    PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    Pre<T> pre;
+    pre.unused = 0;
+    PLOM_UNROLL
+    for (int c2 = 0; c2 < N_CAC; ++c2) {
+      pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
+    }
+    PLOM_PRAGMA_CAC
+    for (int cac0 = 0; cac0 < NMAIN; cac0 += G) {
+      T nz[NW * G > 0 ? NW * G : 1];
+      draws.template normals<NW * G>(cac0, nz);
+      PLOM_UNROLL
+      for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);
+    }
+    PLOM_UNROLL
+    for (int cac = NMAIN; cac < N_CAC; ++cac) {
+      T nz[NW > 0 ? NW : 1];
+      draws.template normals<NW>(cac, nz);
+      cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);
+    }
+    PLOM_UNROLL
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {
       const T f = x[OFF_INC+w] + inc_acc[w];
       x[OFF_INC+w] = (f < T(0)) ? T(0) : f;

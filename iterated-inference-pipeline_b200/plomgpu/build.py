@@ -67,7 +67,10 @@ def _stamp(name, extra):
 
 def nvcc_command(name, S, out=None, verbose_ptxas=False):
     smem = 1 if S > SMEM_STATE_WORDS else 0
+    # single precision: flush denormals, hardware-rate sqrt and division (the
+    # FP32 path is judged statistically; FP64 arithmetic is unaffected)
     cmd = [NVCC] + ARCH + ['-lineinfo', '-O3', '-std=c++17', '--expt-relaxed-constexpr',
+                           '-ftz=true', '-prec-div=false', '-prec-sqrt=false',
                            '-Xcompiler', '-fPIC', '-shared',
                            '-DPLOM_MODEL_HEADER="model_%s.cuh"' % name, '-DPLOM_SMEM_STATE=%d' % smem,
                            '-I', CSRC, '-I', GEN, '-I', INCLUDE,

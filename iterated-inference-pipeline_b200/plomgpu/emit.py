@@ -322,88 +322,126 @@ class Emitter(object):
 
     def _emit_step(self, a, caches, ode, inc):
         m = self.m
-        nsv = len(m.par_sv)
-        a('  template <int V, bool DRIFT, class T, class X, class E, class D>')
-        a('  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {')
-        a('    (void)t;')
-        a('    constexpr int NW = draws_per_cac(V);')
-        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
-        a('PLOM_UNROLL')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
         foi_states = sorted(set(self._foi_states()))
+        # values computed once per substep from the previous state (coupling)
+        a('  template <class T>')
+        a('  struct Pre {')
         for s in foi_states:
-            si = m.par_sv.index(s)
             a('    T yf_%s[N_CAC];' % s)
-            a('PLOM_UNROLL')
-            a('    for (int c2 = 0; c2 < N_CAC; ++c2) {')
-            a('      yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s, si, self._npop_expr('c2')))
-            a('    }')
-        a('    PLOM_PRAGMA_CAC')
-        a('    for (int cac = 0; cac < N_CAC; ++cac) {')
+        a('    int unused;')
+        a('  };')
+        # one compartment-age class: rates, noises, equations, incidence
+        a('  template <int V, bool DRIFT, class T, class X, class E>')
+        a('  PLOM_HD static void cac_body(X& x, const int cac, const T* nz, const T t, const T dt, const E& e,')
+        a('                               T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
+        a('    (void)t; (void)nz; (void)pre;')
         for i, s in enumerate(m.par_sv):
-            a('      const T xo_%s = x[%d*N_CAC+cac];' % (s, i))
+            a('    const T xo_%s = x[%d*N_CAC+cac];' % (s, i))
         for k, p in enumerate(self.drift):
             pk = m.par_proc.index(p)
-            a('      T drift_%d;' % k)
-            a('      if (DRIFT) {')
-            a('        const int g = e.drift_group(%d, cac);' % k)
-            a('        T xw = T(0);')
-            a('        if constexpr (X::DYNAMIC) {')
-            a('          xw = x[OFF_DRIFT+%d*N_CAC+g];' % k)
-            a('        } else {')
-            a('          PLOM_UNROLL')
-            a('          for (int gg = 0; gg < N_CAC; ++gg) if (gg == g) xw = x[OFF_DRIFT+%d*N_CAC+gg];' % k)
-            a('        }')
-            a('        drift_%d = e.drift_value(%d, g, xw);' % (k, k))
+            a('    T drift_%d;' % k)
+            a('    if (DRIFT) {')
+            a('      const int g = e.drift_group(%d, cac);' % k)
+            a('      T xw = T(0);')
+            a('      if constexpr (X::DYNAMIC) {')
+            a('        xw = x[OFF_DRIFT+%d*N_CAC+g];' % k)
             a('      } else {')
-            a('        drift_%d = e.par(%d, cac);' % (k, pk))
+            a('        PLOM_UNROLL')
+            a('        for (int gg = 0; gg < N_CAC; ++gg) if (gg == g) xw = x[OFF_DRIFT+%d*N_CAC+gg];' % k)
             a('      }')
+            a('      drift_%d = e.drift_value(%d, g, xw);' % (k, k))
+            a('    } else {')
+            a('      drift_%d = e.par(%d, cac);' % (k, pk))
+            a('    }')
         for s in foi_states:
-            a('      T foi_%s = T(0);' % s)
-            a('PLOM_UNROLL')
-            a('      for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * yf_%s[c2];' % (s, s))
+            a('    T foi_%s = T(0);' % s)
+            if m.N_CAC % 4 == 0:
+                a('    PLOM_UNROLL')
+                a('    for (int c2 = 0; c2 < N_CAC; c2 += 4) {')
+                a('      const plomrt::V4<T> w4 = e.coupling4(cac, c2);')
+                a('      foi_%s += w4.a * pre.yf_%s[c2];' % (s, s))
+                a('      foi_%s += w4.b * pre.yf_%s[c2 + 1];' % (s, s))
+                a('      foi_%s += w4.c * pre.yf_%s[c2 + 2];' % (s, s))
+                a('      foi_%s += w4.d * pre.yf_%s[c2 + 3];' % (s, s))
+                a('    }')
+            else:
+                a('    PLOM_UNROLL')
+                a('    for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * pre.yf_%s[c2];' % (s, s))
         for k, c in enumerate(caches):
-            a('      const T r%d = %s;' % (k, c))
+            a('    const T r%d = %s;' % (k, c))
+        a('    const T sqdt = sqrt(dt);')
+        a('    (void)sqdt;')
+        a('    int q = 0; (void)q;')
+        for i in range(self.R):
+            a('    const T dem_%d = (V & 1) ? T(0) : sqdt*nz[q++];' % i)
+        for j in range(self.W):
+            a('    const T wn_%d = (V & 2) ? T(0) : sqdt*nz[q++];' % j)
+        for o, eq in enumerate(inc):
+            a('    T incterm_%d;' % o)
+            a('    switch (V) {')
+            for vname, v in VARIANTS.items():
+                a('      case %d: incterm_%d = %s; break;' % (v, o, self._rhs(eq, v)))
+            a('    }')
+        for i, s in enumerate(m.par_sv):
+            a('    T f_%s;' % s)
+            a('    switch (V) {')
+            for vname, v in VARIANTS.items():
+                a('      case %d: f_%s = xo_%s + %s; break;' % (v, s, s, self._rhs(ode[s], v)))
+            a('    }')
+        if inc:
+            a('    PLOM_UNROLL')
+            a('    for (int k = 0; k < INC_PER_CAC; ++k) {')
+            a('      const int l = inc_link(cac, k);')
+            a('      if (l < 0) break;')
+            a('      const int o = l >> 10, w = l & 1023;')
+            a('      PLOM_UNROLL')
+            a('      for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {')
+            a('        if (ww == w) {')
+            for o in range(len(inc)):
+                a('          if (o == %d) inc_acc[ww] += incterm_%d;' % (o, o))
+            a('        }')
+            a('      }')
+            a('    }')
+        for i, s in enumerate(m.par_sv):
+            a('    x[%d*N_CAC+cac] = (f_%s < T(0)) ? T(0) : f_%s;' % (i, s, s))
+        a('  }')
+        # one Euler-Maruyama substep of the whole particle
+        a('  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)')
+        a('  static constexpr PLOM_HD int draw_group(int nw, int per_block) {')
+        a('    int g = 1;')
+        a('    while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;')
+        a('    return (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;')
+        a('  }')
+        a('  template <int V, bool DRIFT, class T, class X, class E, class D>')
+        a('  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {')
+        a('    constexpr int NW = draws_per_cac(V);')
+        a('    constexpr int G = draw_group(NW, D::PER_BLOCK);')
+        a('    constexpr int NMAIN = N_CAC - (N_CAC % G);')
+        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
+        a('    PLOM_UNROLL')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        a('    Pre<T> pre;')
+        a('    pre.unused = 0;')
+        for s in foi_states:
+            si = m.par_sv.index(s)
+            a('    PLOM_UNROLL')
+            a('    for (int c2 = 0; c2 < N_CAC; ++c2) {')
+            a('      pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s, si, self._npop_expr('c2')))
+            a('    }')
+        a('    PLOM_PRAGMA_CAC')
+        a('    for (int cac0 = 0; cac0 < NMAIN; cac0 += G) {')
+        a('      T nz[NW * G > 0 ? NW * G : 1];')
+        a('      draws.template normals<NW * G>(cac0, nz);')
+        a('      PLOM_UNROLL')
+        a('      for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);')
+        a('    }')
+        a('    PLOM_UNROLL')
+        a('    for (int cac = NMAIN; cac < N_CAC; ++cac) {')
         a('      T nz[NW > 0 ? NW : 1];')
         a('      draws.template normals<NW>(cac, nz);')
-        a('      const T sqdt = sqrt(dt);')
-        a('      (void)sqdt;')
-        a('      int q = 0; (void)q;')
-        for i in range(self.R):
-            a('      const T dem_%d = (V & 1) ? T(0) : sqdt*nz[q++];' % i)
-        for j in range(self.W):
-            a('      const T wn_%d = (V & 2) ? T(0) : sqdt*nz[q++];' % j)
-        # incidence terms of this cac (one per incidence observation)
-        for o, eq in enumerate(inc):
-            a('      T incterm_%d;' % o)
-            a('      switch (V) {')
-            for vname, v in VARIANTS.items():
-                a('        case %d: incterm_%d = %s; break;' % (v, o, self._rhs(eq, v)))
-            a('      }')
-        for i, s in enumerate(m.par_sv):
-            a('      T f_%s;' % s)
-            a('      switch (V) {')
-            for vname, v in VARIANTS.items():
-                a('        case %d: f_%s = xo_%s + %s; break;' % (v, s, s, self._rhs(ode[s], v)))
-            a('      }')
-        if inc:
-            a('PLOM_UNROLL')
-            a('      for (int k = 0; k < INC_PER_CAC; ++k) {')
-            a('        const int l = inc_link(cac, k);')
-            a('        if (l < 0) break;')
-            a('        const int o = l >> 10, w = l & 1023;')
-            a('PLOM_UNROLL')
-            a('        for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {')
-            a('          if (ww == w) {')
-            for o in range(len(inc)):
-                a('            if (o == %d) inc_acc[ww] += incterm_%d;' % (o, o))
-            a('          }')
-            a('        }')
-            a('      }')
-        for i, s in enumerate(m.par_sv):
-            a('      x[%d*N_CAC+cac] = (f_%s < T(0)) ? T(0) : f_%s;' % (i, s, s))
+        a('      cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);')
         a('    }')
-        a('PLOM_UNROLL')
+        a('    PLOM_UNROLL')
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {')
         a('      const T f = x[OFF_INC+w] + inc_acc[w];')
         a('      x[OFF_INC+w] = (f < T(0)) ? T(0) : f;')

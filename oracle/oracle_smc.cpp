@@ -58,6 +58,10 @@ struct HostEnv {
   double par(int p, int cac) const { return par_[p * M::N_CAC + cac]; }
   double cov(int k, int cac) const { return cov_[k * M::N_CAC + cac]; }
   double coupling(int a, int b) const { return coup_[a * M::N_CAC + b]; }
+  plomrt::V4<double> coupling4(int a, int b) const {
+    const double* w = coup_ + a * M::N_CAC + b;
+    return plomrt::V4<double>{w[0], w[1], w[2], w[3]};
+  }
   int drift_group(int i, int cac) const { return dgroup_[i * M::N_CAC + cac]; }
   int drift_ngroups(int i) const { return dng_[i]; }
   double drift_vol(int i, int g) const { return dvol_[i * M::N_CAC + g]; }
@@ -77,6 +81,7 @@ struct HostObsEnv {
 
 template <int V>
 struct TableSource {
+  static constexpr int PER_BLOCK = 1;
   const double* p;
   template <int N>
   void normals(int cac, double* out) const {
@@ -87,6 +92,7 @@ struct TableSource {
 
 template <int V>
 struct PhiloxSource {
+  static constexpr int PER_BLOCK = plomrt::NormalGen<double>::per_block();
   plomrt::PhiloxKey key;
   uint32_t j, n, sub;
   template <int N>
