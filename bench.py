@@ -30,6 +30,8 @@ WORKLOADS = {
     # name: (model library, J, observation intervals, dt in days)
     'seir20x2': ('seir20x2', 100000, 520, 1.0),
     'sir': ('sir', 1000, 52, 1.0),
+    # 4096 SIR parameter sets, J in 256..16384, T in 52..520 weeks, one persistent launch
+    'sir_batch': ('sir', None, None, 1.0),
 }
 METRIC = 'particle-steps/s at matched loglik error'
 
@@ -201,10 +203,78 @@ def run_reference(args):
     return 0
 
 
+def run_batch(args):
+    """Batched filters (4096 SIR parameter sets) beside the plain single-filter path."""
+    import numpy as np
+    import torch
+    from plomgpu import workloads
+    from plomgpu.native import Engine, Batch, Plan
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    eng = Engine('sir')
+    bp = workloads.sir_batch(n_sets=4096, seed=2)
+    b = Batch(eng, bp, precision=32)
+    stream = torch.cuda.ExternalStream(b.stream)
+    for _ in range(args.warmup):
+        b.launch()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with Clocks(int(os.environ.get('LOCAL_RANK', '0'))) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            b.launch()
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    ll, nf, ess = b.results()
+    bt, grid = b.config
+    b.close()
+    value = bp.particle_steps / (ms / 1000.0)
+    # plain single-filter path on the config-0 filter (J = 1000, T = 52), graph replay
+    single = workload_problem('sir', precision=32, seed=5)
+    plan = Plan(eng, single)
+    s2 = torch.cuda.ExternalStream(plan.stream)
+    for _ in range(5):
+        plan.launch()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record(s2)
+    for _ in range(reps):
+        plan.launch()
+    e1.record(s2)
+    torch.cuda.synchronize()
+    ms_single = e0.elapsed_time(e1) / reps
+    plan.close()
+    single_value = single.J * single.n_obs / (ms_single / 1000.0)
+    # loglik error of the FP32 batch against FP64 on a sample of sets
+    sample = list(range(0, 4096, 256))
+    errs = []
+    for i in sample:
+        p64 = bp.single(i, precision=64)
+        errs.append(abs(eng.smc(p64).loglik - ll[i]))
+    line = {'metric': METRIC, 'value': value, 'unit': 'particle-steps/s', 'n_gpus': 1, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
+            'config': {'workload': 'sir_batch', 'filters': 4096, 'particle_steps': bp.particle_steps,
+                       'J_range': [256, 16384], 'T_range': [52, 520], 'block_threads': bt, 'grid': grid},
+            'plain_single_filter': {'value': single_value, 'ms_per_filter': ms_single, 'J': single.J,
+                                    'T': single.n_obs},
+            'batched_over_plain': value / single_value,
+            'loglik_abs_diff_fp32_vs_fp64_same_seed': {'mean': float(np.mean(errs)), 'max': float(np.max(errs)),
+                                                       'sets': len(sample)},
+            'clocks': clk.summary(), 'gpu_launches': args.steps}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == 'reference':
         return run_reference(args)
+    if args.workload == 'sir_batch':
+        return run_batch(args)
     import numpy as np
     import torch
     world = int(os.environ.get('WORLD_SIZE', '1'))

@@ -154,6 +154,57 @@ void plomgpu_plan_destroy(plomgpu_plan *plan);
  * the device-side closed form (GPU) into out[J]. */
 int plomgpu_debug_systematic_points(double U, int J, double *out);
 
+/* ------------------------------------------------------------------------
+ * Batched filters: many independent filters of one model (different
+ * parameters, particle counts, series lengths and data) in one persistent
+ * launch.  Serves the callers that evaluate many likelihoods at once (mif
+ * particles over parameter sets, concurrent pmcmc chains; C/mif/mif.c,
+ * C/pmcmc/pmcmc.c).  Filter i with seed[i] consumes exactly the draws of a
+ * single plomgpu_smc_run with seed = seed[i]. */
+typedef struct plomgpu_batch_desc {
+    int n_filters;
+    const int *J;              /* [n] particles of each filter */
+    const int *n_obs;          /* [n] intervals of each filter (<= max_obs) */
+    const long long *data_row; /* [n] first row of each filter in data */
+    const double *data;        /* [n_rows][n_ts], NaN = missing */
+    long long n_rows;
+    const double *par_cac;     /* [n][n_par_proc][n_cac] */
+    const double *par_ts;      /* [n][n_par_obs][n_ts] */
+    const double *x0;          /* [n][n_state] */
+    const uint64_t *seed;      /* [n] */
+    /* time grid and covariates of the longest filter, shared by all */
+    int max_obs;
+    const int *n_sub;          /* [max_obs] */
+    const double *t_sub;       /* [sum n_sub] */
+    const double *t_obs;       /* [max_obs] */
+    double dt;
+    const double *cov_cac;     /* [sum n_sub][n_cov_cac][n_cac] */
+    const double *cov_ts;      /* [max_obs][n_cov_ts][n_ts] */
+    const double *coupling;
+    const int *drift_group;
+    const int *drift_ngroups;
+    const plomgpu_back_transform *drift_bt;
+    const double *drift_vol;
+    int noises_off;
+    int filter;
+    double like_min;
+    int precision;             /* 32 or 64 */
+    int block_threads;         /* 0: autotuned among 128 / 256 / 512 */
+} plomgpu_batch_desc;
+
+typedef struct plomgpu_batch plomgpu_batch;
+
+/* Uploads the batch, sizes the per-CTA workspaces and (block_threads == 0)
+ * times the candidate block sizes on a sample of the batch. */
+int plomgpu_batch_create(const plomgpu_batch_desc *desc, plomgpu_batch **out);
+int plomgpu_batch_launch(plomgpu_batch *batch);
+int plomgpu_batch_results(plomgpu_batch *batch, double *loglik, int *n_all_fail, double *ess_min);
+void *plomgpu_batch_stream(plomgpu_batch *batch);
+int plomgpu_batch_config(plomgpu_batch *batch, int *block_threads, int *grid);
+void plomgpu_batch_destroy(plomgpu_batch *batch);
+/* One-shot: create, launch, results, destroy. */
+int plomgpu_batch_run(const plomgpu_batch_desc *desc, double *loglik, int *n_all_fail);
+
 /* Resamples one observation interval without allocating device memory.
  *
  * No counterpart in the reference.  For callers that cannot allocate: a

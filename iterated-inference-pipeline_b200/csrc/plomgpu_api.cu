@@ -718,3 +718,371 @@ extern "C" int plomgpu_resample_noalloc(const void* log_weights, int precision, 
   if (precision == 64) return noalloc_run<double>((const double*)log_weights, J, like_min, u, ancestors, out, s, sc);
   return noalloc_run<float>((const float*)log_weights, J, like_min, u, ancestors, out, s, sc);
 }
+
+// ---------------------------------------------------------------------------
+// Batched filters: many independent filters of one model in one persistent
+// launch (see smc_batch.cuh).
+#include "smc_batch.cuh"
+#include <algorithm>
+#include <numeric>
+
+struct plomgpu_batch {
+  int n = 0, max_obs = 0, max_J = 0, precision = 32, noises_off = 0, filter = 1;
+  int bt = 0, grid = 0, kernels = 1;
+  double dt = 1.0, like_min = 1e-17;
+  cudaStream_t stream = nullptr;
+  std::vector<BatchFilter> filters_h;
+  std::vector<int> order_h;
+  BatchFilter* filters = nullptr;
+  int* order = nullptr;
+  unsigned* queue = nullptr;
+  double *par_cac = nullptr, *par_ts = nullptr, *x0 = nullptr, *data = nullptr;
+  int *n_sub = nullptr, *sub0 = nullptr;
+  double *t_sub = nullptr, *t_obs = nullptr, *cov_ts = nullptr;
+  void *cov_cac = nullptr, *coupling = nullptr, *drift_vol = nullptr;
+  int *drift_group = nullptr, *drift_ngroups = nullptr;
+  plomrt::BackTransform* drift_bt = nullptr;
+  unsigned char* ws = nullptr;
+  size_t ws_stride = 0;
+  double* loglik = nullptr;
+  int* n_all_fail = nullptr;
+  double* ess_min = nullptr;
+  int* error = nullptr;
+};
+
+namespace {
+
+template <class T>
+using BatchKernel = void (*)(const BatchArgs<T>);
+
+template <class T, int BT>
+BatchKernel<T> pick_batch_bt(int v, bool drift) {
+  if constexpr (!kSmem) {
+    if (drift) {
+      if constexpr (M::N_DRIFT > 0) {
+        switch (v) {
+          case 0: return &k_batch<T, 0, true, BT>;
+          case 1: return &k_batch<T, 1, true, BT>;
+          case 2: return &k_batch<T, 2, true, BT>;
+          default: return &k_batch<T, 3, true, BT>;
+        }
+      }
+      return nullptr;
+    }
+    switch (v) {
+      case 0: return &k_batch<T, 0, false, BT>;
+      case 1: return &k_batch<T, 1, false, BT>;
+      case 2: return &k_batch<T, 2, false, BT>;
+      default: return &k_batch<T, 3, false, BT>;
+    }
+  }
+  return nullptr;
+}
+
+template <class T>
+BatchKernel<T> pick_batch(int bt, int noises_off) {
+  const int v = variant_of(noises_off);
+  const bool d = drift_on(noises_off);
+  if constexpr (std::is_same<T, double>::value) {
+    if (bt == 256) return pick_batch_bt<T, 256>(v, d);
+    return nullptr;
+  } else {
+    switch (bt) {
+      case 128: return pick_batch_bt<T, 128>(v, d);
+      case 256: return pick_batch_bt<T, 256>(v, d);
+      case 512: return pick_batch_bt<T, 512>(v, d);
+      default: return nullptr;
+    }
+  }
+}
+
+template <class T>
+BatchArgs<T> batch_args(plomgpu_batch* b, const BatchFilter* filters, int n, const int* order) {
+  BatchArgs<T> a;
+  a.filters = filters;
+  a.order = order;
+  a.n_filters = n;
+  a.queue = b->queue;
+  a.par_cac = b->par_cac;
+  a.par_ts = b->par_ts;
+  a.x0 = b->x0;
+  a.data = b->data;
+  a.n_sub = b->n_sub;
+  a.sub0 = b->sub0;
+  a.t_sub = b->t_sub;
+  a.t_obs = b->t_obs;
+  a.cov_cac = (const T*)b->cov_cac;
+  a.cov_ts = b->cov_ts;
+  a.coupling = (const T*)b->coupling;
+  a.drift_group = b->drift_group;
+  a.drift_ngroups = b->drift_ngroups;
+  a.drift_bt = b->drift_bt;
+  a.drift_vol = (const T*)b->drift_vol;
+  a.dt = b->dt;
+  a.like_min = b->like_min;
+  a.thresh = pow(b->like_min, (double)M::N_TS);
+  a.log_like_min = log(b->like_min);
+  a.filter_on = b->filter;
+  a.ws = b->ws;
+  a.ws_stride = b->ws_stride;
+  a.max_J = b->max_J;
+  a.loglik = b->loglik;
+  a.n_all_fail = b->n_all_fail;
+  a.ess_min = b->ess_min;
+  a.error = b->error;
+  return a;
+}
+
+template <class T>
+int batch_enqueue(plomgpu_batch* b, int bt, int grid, const BatchFilter* filters, int n, const int* order) {
+  BatchKernel<T> k = pick_batch<T>(bt, b->noises_off);
+  if (!k) return fail(PLOMGPU_EINVAL, "no batched kernel for this block size / precision / model");
+  CK(cudaMemsetAsync(b->queue, 0, sizeof(unsigned), b->stream));
+  CK(cudaMemsetAsync(b->error, 0, sizeof(int), b->stream));
+  k<<<grid, bt, 0, b->stream>>>(batch_args<T>(b, filters, n, order));
+  CK(cudaGetLastError());
+  return PLOMGPU_OK;
+}
+
+template <class T>
+int batch_occupancy(int bt, int noises_off, int* per_sm) {
+  BatchKernel<T> k = pick_batch<T>(bt, noises_off);
+  if (!k) return fail(PLOMGPU_EINVAL, "no batched kernel");
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, bt, 0));
+  return PLOMGPU_OK;
+}
+
+// Picks the block size (and the grid from the occupancy of that kernel) by
+// timing the candidates on a sample of the batch: the longest filters, cut
+// to a few intervals.
+template <class T>
+int batch_autotune(plomgpu_batch* b, int sms) {
+  std::vector<int> cands;
+  if (std::is_same<T, double>::value) cands = {256};
+  else cands = {128, 256, 512};
+  if (b->bt > 0) cands = {b->bt};
+  int best_bt = 0, best_grid = 0;
+  float best = 1e30f;
+  // sample: enough filters to fill the largest grid twice, 12 intervals each
+  std::vector<BatchFilter> sample;
+  for (int i = 0; i < b->n && (int)sample.size() < 2 * sms * 8; ++i) {
+    BatchFilter f = b->filters_h[b->order_h[i]];
+    f.n_obs = std::min(f.n_obs, 12);
+    sample.push_back(f);
+  }
+  std::vector<int> sorder(sample.size());
+  std::iota(sorder.begin(), sorder.end(), 0);
+  BatchFilter* d_sample = nullptr;
+  int* d_sorder = nullptr;
+  CK(cudaMalloc((void**)&d_sample, sample.size() * sizeof(BatchFilter)));
+  CK(cudaMalloc((void**)&d_sorder, sorder.size() * sizeof(int)));
+  CK(cudaMemcpy(d_sample, sample.data(), sample.size() * sizeof(BatchFilter), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_sorder, sorder.data(), sorder.size() * sizeof(int), cudaMemcpyHostToDevice));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = PLOMGPU_OK;
+  for (int bt : cands) {
+    int per_sm = 0;
+    if ((rc = batch_occupancy<T>(bt, b->noises_off, &per_sm))) break;
+    if (per_sm < 1) continue;
+    const int grid = sms * per_sm;
+    if ((size_t)grid * b->ws_stride > (size_t)b->grid * b->ws_stride) continue;  // workspace sized for b->grid
+    if ((rc = batch_enqueue<T>(b, bt, grid, d_sample, (int)sample.size(), d_sorder))) break;  // warm
+    CK(cudaEventRecord(e0, b->stream));
+    if ((rc = batch_enqueue<T>(b, bt, grid, d_sample, (int)sample.size(), d_sorder))) break;
+    CK(cudaEventRecord(e1, b->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      best_bt = bt;
+      best_grid = grid;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_sample);
+  cudaFree(d_sorder);
+  if (rc) return rc;
+  if (!best_bt) return fail(PLOMGPU_EINVAL, "no batched configuration fits");
+  b->bt = best_bt;
+  b->grid = best_grid;
+  return PLOMGPU_OK;
+}
+
+void batch_free(plomgpu_batch* b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  void* bufs[] = {b->filters, b->order, b->queue, b->par_cac, b->par_ts, b->x0, b->data, b->n_sub, b->sub0,
+                  b->t_sub, b->t_obs, b->cov_ts, b->cov_cac, b->coupling, b->drift_vol, b->drift_group,
+                  b->drift_ngroups, b->drift_bt, b->ws, b->loglik, b->n_all_fail, b->ess_min, b->error};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+template <class T>
+int batch_build(const plomgpu_batch_desc* d, plomgpu_batch* b) {
+  cudaStream_t s = b->stream;
+  int rc;
+  const int n = d->n_filters;
+  long long total_sub = 0;
+  std::vector<int> sub0(d->max_obs);
+  for (int i = 0; i < d->max_obs; ++i) {
+    sub0[i] = (int)total_sub;
+    total_sub += d->n_sub[i];
+  }
+  if ((rc = upload<BatchFilter>(b->filters_h.data(), (size_t)n, &b->filters, s))) return rc;
+  if ((rc = upload<int>(b->order_h.data(), (size_t)n, &b->order, s))) return rc;
+  CK(cudaMalloc((void**)&b->queue, sizeof(unsigned)));
+  CK(cudaMalloc((void**)&b->error, sizeof(int)));
+  if ((rc = upload<double>(d->par_cac, (size_t)n * M::N_PAR_PROC * M::N_CAC, &b->par_cac, s))) return rc;
+  if ((rc = upload<double>(d->par_ts, (size_t)n * M::N_PAR_OBS * M::N_TS, &b->par_ts, s))) return rc;
+  if ((rc = upload<double>(d->x0, (size_t)n * M::S, &b->x0, s))) return rc;
+  if ((rc = upload<double>(d->data, (size_t)d->n_rows * M::N_TS, &b->data, s))) return rc;
+  if ((rc = upload<int>(d->n_sub, (size_t)d->max_obs, &b->n_sub, s))) return rc;
+  if ((rc = upload<int>(sub0.data(), (size_t)d->max_obs, &b->sub0, s))) return rc;
+  if ((rc = upload<double>(d->t_sub, (size_t)total_sub, &b->t_sub, s))) return rc;
+  if ((rc = upload<double>(d->t_obs, (size_t)d->max_obs, &b->t_obs, s))) return rc;
+  if ((rc = upload_as<T>(d->cov_cac, (size_t)total_sub * M::N_COV_CAC * M::N_CAC, &b->cov_cac, s))) return rc;
+  if ((rc = upload<double>(d->cov_ts, (size_t)d->max_obs * M::N_COV_TS * M::N_TS, &b->cov_ts, s))) return rc;
+  if (M::COUPLED && (rc = upload_as<T>(d->coupling, (size_t)M::N_CAC * M::N_CAC, &b->coupling, s))) return rc;
+  if (drift_on(d->noises_off)) {
+    if ((rc = upload_as<T>(d->drift_vol, (size_t)M::N_DRIFT * M::N_CAC, &b->drift_vol, s))) return rc;
+    if ((rc = upload<int>(d->drift_group, (size_t)M::N_DRIFT * M::N_CAC, &b->drift_group, s))) return rc;
+    if ((rc = upload<int>(d->drift_ngroups, (size_t)M::N_DRIFT, &b->drift_ngroups, s))) return rc;
+    if ((rc = upload<plomrt::BackTransform>((const plomrt::BackTransform*)d->drift_bt, (size_t)M::N_DRIFT * M::N_CAC,
+                                            &b->drift_bt, s)))
+      return rc;
+  }
+  CK(cudaMalloc((void**)&b->loglik, (size_t)n * sizeof(double)));
+  CK(cudaMalloc((void**)&b->n_all_fail, (size_t)n * sizeof(int)));
+  CK(cudaMalloc((void**)&b->ess_min, (size_t)n * sizeof(double)));
+  // workspace for the largest grid any candidate block size can use
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int max_grid = 0;
+  for (int bt : {128, 256, 512}) {
+    if (std::is_same<T, double>::value && bt != 256) continue;
+    if (d->block_threads > 0 && bt != d->block_threads) continue;
+    int per_sm = 0;
+    if ((rc = batch_occupancy<T>(bt, d->noises_off, &per_sm))) return rc;
+    max_grid = std::max(max_grid, sms * per_sm);
+  }
+  if (max_grid < 1) return fail(PLOMGPU_EINVAL, "batched kernel does not fit on the device");
+  b->ws_stride = (batch_ws_bytes<T>(b->max_J) + 255) & ~(size_t)255;
+  b->grid = max_grid;
+  CK(cudaMalloc((void**)&b->ws, b->ws_stride * (size_t)max_grid));
+  CK(cudaStreamSynchronize(s));
+  b->bt = d->block_threads;
+  if ((rc = batch_autotune<T>(b, sms))) return rc;
+  return PLOMGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int plomgpu_batch_create(const plomgpu_batch_desc* d, plomgpu_batch** out) {
+  if (!out || !d) return fail(PLOMGPU_EINVAL, "null argument");
+  *out = nullptr;
+  if (kSmem) return fail(PLOMGPU_EINVAL, "batched filters need a model whose particle fits registers");
+  if (d->n_filters < 1) return fail(PLOMGPU_EINVAL, "n_filters must be >= 1");
+  if (d->precision != 32 && d->precision != 64) return fail(PLOMGPU_EINVAL, "precision must be 32 or 64");
+  if (!d->J || !d->n_obs || !d->data_row || !d->seed || !d->x0 || !d->n_sub || !d->t_obs)
+    return fail(PLOMGPU_EINVAL, "missing arrays");
+  if (M::COUPLED && !d->coupling) return fail(PLOMGPU_EINVAL, "coupled model needs a coupling matrix");
+  if (d->block_threads != 0 && d->block_threads != 128 && d->block_threads != 256 && d->block_threads != 512)
+    return fail(PLOMGPU_EINVAL, "block_threads must be 0 (autotune), 128, 256 or 512");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PLOMGPU_ENODEV, "no CUDA device");
+  plomgpu_batch* b = new plomgpu_batch();
+  b->n = d->n_filters;
+  b->max_obs = d->max_obs;
+  b->precision = d->precision;
+  b->noises_off = d->noises_off;
+  b->filter = d->filter;
+  b->dt = d->dt;
+  b->like_min = d->like_min;
+  b->filters_h.resize(b->n);
+  for (int i = 0; i < b->n; ++i) {
+    if (d->J[i] < 1 || d->n_obs[i] < 0 || d->n_obs[i] > d->max_obs) {
+      delete b;
+      return fail(PLOMGPU_EINVAL, "filter " + std::to_string(i) + ": bad J or n_obs");
+    }
+    if (d->data_row[i] < 0 || d->data_row[i] + d->n_obs[i] > d->n_rows) {
+      delete b;
+      return fail(PLOMGPU_EINVAL, "filter " + std::to_string(i) + ": data rows out of range");
+    }
+    b->filters_h[i] = BatchFilter{d->J[i], d->n_obs[i], d->data_row[i], d->seed[i]};
+    b->max_J = std::max(b->max_J, d->J[i]);
+  }
+  // longest filters first (list scheduling over the persistent CTAs)
+  b->order_h.resize(b->n);
+  std::iota(b->order_h.begin(), b->order_h.end(), 0);
+  std::stable_sort(b->order_h.begin(), b->order_h.end(), [&](int x, int y) {
+    return (long long)b->filters_h[x].J * b->filters_h[x].n_obs > (long long)b->filters_h[y].J * b->filters_h[y].n_obs;
+  });
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(PLOMGPU_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  int rc = (d->precision == 64) ? batch_build<double>(d, b) : batch_build<float>(d, b);
+  if (rc) {
+    std::string keep = g_err;
+    batch_free(b);
+    g_err = keep;
+    return rc;
+  }
+  *out = b;
+  return PLOMGPU_OK;
+}
+
+int plomgpu_batch_launch(plomgpu_batch* b) {
+  if (!b) return fail(PLOMGPU_EINVAL, "null batch");
+  return (b->precision == 64) ? batch_enqueue<double>(b, b->bt, b->grid, b->filters, b->n, b->order)
+                              : batch_enqueue<float>(b, b->bt, b->grid, b->filters, b->n, b->order);
+}
+
+int plomgpu_batch_results(plomgpu_batch* b, double* loglik, int* n_all_fail, double* ess_min) {
+  if (!b) return fail(PLOMGPU_EINVAL, "null batch");
+  int err = 0;
+  if (loglik) CK(cudaMemcpyAsync(loglik, b->loglik, (size_t)b->n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  if (n_all_fail)
+    CK(cudaMemcpyAsync(n_all_fail, b->n_all_fail, (size_t)b->n * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  if (ess_min) CK(cudaMemcpyAsync(ess_min, b->ess_min, (size_t)b->n * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaMemcpyAsync(&err, b->error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (err) return fail(PLOMGPU_ETIMEOUT, "systematic point table overflow");
+  return PLOMGPU_OK;
+}
+
+void* plomgpu_batch_stream(plomgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int plomgpu_batch_config(plomgpu_batch* b, int* block_threads, int* grid) {
+  if (!b) return fail(PLOMGPU_EINVAL, "null batch");
+  if (block_threads) *block_threads = b->bt;
+  if (grid) *grid = b->grid;
+  return PLOMGPU_OK;
+}
+
+void plomgpu_batch_destroy(plomgpu_batch* b) { batch_free(b); }
+
+int plomgpu_batch_run(const plomgpu_batch_desc* d, double* loglik, int* n_all_fail) {
+  plomgpu_batch* b = nullptr;
+  int rc = plomgpu_batch_create(d, &b);
+  if (rc) return rc;
+  rc = plomgpu_batch_launch(b);
+  if (!rc) rc = plomgpu_batch_results(b, loglik, n_all_fail, nullptr);
+  std::string keep = g_err;
+  batch_free(b);
+  g_err = keep;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,323 @@
+// Many independent particle filters in one persistent launch.
+//
+// Every CTA takes whole filters from a work queue (an atomic ticket over a
+// host-given order, longest first) and runs all of a filter's observation
+// intervals itself: the propagate loop over its particles, then a block-level
+// log-sum-exp reduction, cumulative-weight scan and ancestor search
+// (weight() / systematic_sampling() / resample_X(), model_builder/C/core/
+// smc.c:27-161), separated by __syncthreads.  The per-filter state lives in a
+// per-CTA workspace in HBM; the whole batch needs one launch, no host
+// round trip between intervals.
+//
+// The draws of filter f are keyed by its own seed (PhiloxKey(seed_f, 0)), so
+// a filter of the batch consumes exactly the draws of the single-filter path
+// (plomgpu_smc_run) with that seed.
+#pragma once
+
+#include "smc_engine.cuh"
+
+namespace plomgpu {
+
+struct BatchFilter {
+  int J;
+  int n_obs;
+  long long data_row;  // first data row of the filter
+  uint64_t seed;
+};
+
+template <class T>
+struct BatchArgs {
+  const BatchFilter* filters;
+  const int* order;         // processing order of the filters
+  int n_filters;
+  unsigned* queue;          // work ticket (reset by the host before each launch)
+  const double* par_cac;    // [n][N_PAR_PROC][N_CAC]
+  const double* par_ts;     // [n][N_PAR_OBS][N_TS]
+  const double* x0;         // [n][S]
+  const double* data;       // concatenated rows [*][N_TS]
+  // time grid shared by all filters (of the longest one)
+  const int* n_sub;         // [max_obs]
+  const int* sub0;          // [max_obs]
+  const double* t_sub;
+  const double* t_obs;
+  const T* cov_cac;         // [sub][N_COV_CAC][N_CAC]
+  const double* cov_ts;     // [max_obs][N_COV_TS][N_TS]
+  const T* coupling;
+  const int* drift_group;
+  const int* drift_ngroups;
+  const plomrt::BackTransform* drift_bt;
+  const T* drift_vol;
+  double dt, like_min, thresh, log_like_min;
+  int filter_on;
+  // per-CTA workspace
+  unsigned char* ws;
+  size_t ws_stride;
+  int max_J;
+  // outputs
+  double* loglik;
+  int* n_all_fail;
+  double* ess_min;
+  int* error;
+};
+
+template <class T>
+struct BatchWs {
+  T* X[2];
+  T* lw;
+  double* C;
+  uint32_t* anc;
+};
+
+template <class T>
+__host__ __device__ inline size_t batch_ws_bytes(int max_J) {
+  const size_t mj = (size_t)((max_J + 31) & ~31);
+  return 2 * (size_t)M::S * mj * sizeof(T) + mj * sizeof(T) + mj * sizeof(double) + mj * sizeof(uint32_t) + 256;
+}
+
+template <class T>
+__device__ inline BatchWs<T> batch_ws(unsigned char* base, int max_J) {
+  const size_t mj = (size_t)((max_J + 31) & ~31);
+  BatchWs<T> w;
+  unsigned char* p = base;
+  w.C = reinterpret_cast<double*>(p);
+  p += mj * sizeof(double);
+  w.X[0] = reinterpret_cast<T*>(p);
+  p += (size_t)M::S * mj * sizeof(T);
+  w.X[1] = reinterpret_cast<T*>(p);
+  p += (size_t)M::S * mj * sizeof(T);
+  w.lw = reinterpret_cast<T*>(p);
+  p += mj * sizeof(T);
+  w.anc = reinterpret_cast<uint32_t*>(p);
+  return w;
+}
+
+// block-wide helpers (fixed order: deterministic for a fixed block size)
+template <int BT>
+__device__ inline LseAcc block_lse(LseAcc a, LseAcc* sh) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = a;
+  __syncthreads();
+  if (warp == 0) {
+    a = (lane < BT / 32) ? sh[lane] : LseAcc{-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+    if (lane == 0) sh[0] = a;
+  }
+  __syncthreads();
+  a = sh[0];
+  __syncthreads();
+  return a;
+}
+
+// exclusive scan of one double per thread; returns the exclusive prefix, total in *tot
+template <int BT>
+__device__ inline double block_exscan(double v, double* sh, double* tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double o = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += o;
+  }
+  if (lane == 31) sh[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    double w = (lane < BT / 32) ? sh[lane] : 0.0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += o;
+    }
+    if (lane < BT / 32) sh[lane] = w;
+  }
+  __syncthreads();
+  const double excl = (warp > 0 ? sh[warp - 1] : 0.0) + (x - v);
+  *tot = sh[BT / 32 - 1];
+  __syncthreads();
+  return excl;
+}
+
+template <class T, int V, bool DRIFT, int BT>
+__global__ void __launch_bounds__(BT) k_batch(const BatchArgs<T> a) {
+  __shared__ LseAcc sh_lse[BT / 32];
+  __shared__ double sh_scan[BT / 32];
+  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  __shared__ int s_f, s_ns, s_fail;
+  __shared__ double s_m, s_s1;
+  __shared__ __align__(16) T s_coup[kSmemCoup > 0 ? kSmemCoup : 4];
+  __shared__ __align__(16) T s_par[kSmemPar > 0 ? kSmemPar : 4];
+
+  if constexpr (M::COUPLED) {
+    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = a.coupling[i];
+  }
+  const BatchWs<T> ws = batch_ws<T>(a.ws + blockIdx.x * a.ws_stride, a.max_J);
+  const size_t ld = (size_t)((a.max_J + 31) & ~31);
+
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const unsigned t = atomicAdd(a.queue, 1u);
+      s_f = (t < (unsigned)a.n_filters) ? a.order[t] : -1;
+    }
+    __syncthreads();
+    const int f = s_f;
+    if (f < 0) break;
+    const BatchFilter fl = a.filters[f];
+    const int J = fl.J;
+    for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT)
+      s_par[i] = (T)a.par_cac[(size_t)f * M::N_PAR_PROC * M::N_CAC + i];
+    const double* x0 = a.x0 + (size_t)f * M::S;
+    for (int j = threadIdx.x; j < J; j += BT) {
+#pragma unroll
+      for (int w = 0; w < M::OFF_INC; ++w) ws.X[0][(size_t)w * ld + j] = (T)x0[w];
+    }
+    __syncthreads();
+    ProcEnv<T> e;
+    e.par_ = s_par;
+    e.coup_ = s_coup;
+    e.dgroup_ = a.drift_group;
+    e.dng_ = a.drift_ngroups;
+    e.dbt_ = a.drift_bt;
+    e.dvol_ = a.drift_vol;
+    ObsEnv oe;
+    oe.par_ts_ = a.par_ts + (size_t)f * M::N_PAR_OBS * M::N_TS;
+    const plomrt::PhiloxKey key = plomrt::make_key(fl.seed, 0u);
+    const T dt = (T)a.dt;
+    double loglik = 0.0, ess_min = INFINITY;
+    int n_all_fail = 0;
+    int cur = 0;
+    bool resampled = false;
+    for (int n = 0; n < fl.n_obs; ++n) {
+      const double* y = a.data + (size_t)(fl.data_row + n) * M::N_TS;
+      bool any = false;
+#pragma unroll
+      for (int ts = 0; ts < M::N_TS; ++ts) any |= !isnan(__ldg(y + ts));
+      const bool weigh = a.filter_on && any;
+      oe.cov_ts_ = a.cov_ts + (size_t)n * M::N_COV_TS * M::N_TS;
+      const int K = __ldg(a.n_sub + n), sub0 = __ldg(a.sub0 + n);
+      const double t_obs = __ldg(a.t_obs + n);
+      const T* Xp = ws.X[cur];
+      T* Xn = ws.X[cur ^ 1];
+      LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
+      for (int j = threadIdx.x; j < J; j += BT) {
+        const uint32_t src = resampled ? ws.anc[j] : (uint32_t)j;
+        RegState<T, M::S> x;
+#pragma unroll
+        for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * ld + src];
+#pragma unroll
+        for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);
+        for (int k = 0; k < K; ++k) {
+          const int sub = sub0 + k;
+          e.cov_ = a.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
+          const T t = (T)__ldg(a.t_sub + sub);
+          PhiloxDraws<T, V> d;
+          d.key = key;
+          d.j = (uint32_t)j;
+          d.n = (uint32_t)n;
+          d.sub = (uint32_t)k;
+          M::template step<V, DRIFT, T>(x, t, dt, e, d);
+        }
+#pragma unroll
+        for (int w = 0; w < M::OFF_INC; ++w) Xn[(size_t)w * ld + j] = x[w];
+        if (weigh) {
+          double obs[M::N_TS];
+          M::template proj2obs<T>(x, obs);
+          double ll = 0.0;
+#pragma unroll
+          for (int ts = 0; ts < M::N_TS; ++ts) {
+            const double yy = __ldg(y + ts);
+            if (isnan(yy)) continue;
+            const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
+            const double var = M::obs_var(obs[ts], ts, t_obs, oe);
+            ll += log(plomrt::disc_normal_like(yy, mu, var, a.like_min));
+          }
+          const T l = (T)ll;
+          ws.lw[j] = l;
+          if (weight_fails(l, a.thresh)) {
+            acc.nfail += 1;
+          } else {
+            LseAcc b = {(double)l, 1.0, 1.0, 0};
+            acc = lse_merge(acc, b);
+          }
+        }
+      }
+      cur ^= 1;
+      if (!weigh) {
+        resampled = false;
+        __syncthreads();
+        continue;
+      }
+      acc = block_lse<BT>(acc, sh_lse);  // (syncs: Xn / lw visible to the block)
+      if (threadIdx.x == 0) {
+        const int all_fail = (acc.nfail == J);
+        double llike, ess;
+        if (all_fail) {
+          llike = a.log_like_min * (double)M::N_TS;
+          ess = 0.0;
+          n_all_fail += 1;
+        } else {
+          llike = acc.m + log(acc.s1 / (double)J);
+          ess = (acc.s1 * acc.s1) / acc.s2;
+        }
+        loglik += llike;
+        ess_min = fmin(ess_min, ess);
+        s_fail = all_fail;
+        s_m = acc.m;
+        s_s1 = acc.s1;
+        const double inc = 1.0 / (double)J;
+        const double U = inc * plomrt::resample_uniform(key, (uint32_t)n);
+        int ns = plomrt::systematic_table(U, inc, J, seg, plomrt::SYS_MAX_SEG);
+        if (ns < 0) {
+          atomicOr(a.error, (int)ERR_SYS_TABLE);
+          ns = 0;
+        }
+        s_ns = ns;
+      }
+      __syncthreads();
+      if (s_fail || s_ns == 0) {
+        for (int j = threadIdx.x; j < J; j += BT) ws.anc[j] = (uint32_t)j;
+      } else {
+        // cumulative normalised weights: each thread a contiguous chunk
+        const int P = (J + BT - 1) / BT;
+        const int i0 = threadIdx.x * P;
+        const int i1 = min(J, i0 + P);
+        const double m = s_m, s1 = s_s1;
+        double run = 0.0;
+        for (int i = i0; i < i1; ++i) {
+          const T l = ws.lw[i];
+          run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+        }
+        double tot;
+        const double pre = block_exscan<BT>(run, sh_scan, &tot);
+        run = pre;
+        for (int i = i0; i < i1; ++i) {
+          const T l = ws.lw[i];
+          run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+          ws.C[i] = run;
+        }
+        __syncthreads();
+        const int ns = s_ns;
+        for (int j = threadIdx.x; j < J; j += BT) {
+          const double ran = plomrt::systematic_point(seg, ns, j);
+          int lo = 0, hi = J - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ran > ws.C[mid]) lo = mid + 1; else hi = mid;
+          }
+          ws.anc[j] = (uint32_t)lo;
+        }
+      }
+      resampled = true;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      a.loglik[f] = loglik;
+      a.n_all_fail[f] = n_all_fail;
+      if (a.ess_min) a.ess_min[f] = ess_min;
+    }
+  }
+}
+
+}  // namespace plomgpu

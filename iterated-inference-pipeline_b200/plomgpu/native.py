@@ -45,6 +45,15 @@ class SmcDesc(C.Structure):
                 ('crn_normals', _dp), ('crn_uniforms', _dp)]
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [('n_filters', C.c_int), ('J', _ip), ('n_obs', _ip), ('data_row', _P(C.c_longlong)),
+                ('data', _dp), ('n_rows', C.c_longlong), ('par_cac', _dp), ('par_ts', _dp), ('x0', _dp),
+                ('seed', _P(C.c_uint64)), ('max_obs', C.c_int), ('n_sub', _ip), ('t_sub', _dp), ('t_obs', _dp),
+                ('dt', C.c_double), ('cov_cac', _dp), ('cov_ts', _dp), ('coupling', _dp), ('drift_group', _ip),
+                ('drift_ngroups', _ip), ('drift_bt', _P(BackTransform)), ('drift_vol', _dp), ('noises_off', C.c_int),
+                ('filter', C.c_int), ('like_min', C.c_double), ('precision', C.c_int), ('block_threads', C.c_int)]
+
+
 class SmcResult(C.Structure):
     _fields_ = [('loglik', C.c_double), ('n_all_fail', C.c_int), ('status', C.c_int),
                 ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp)]
@@ -54,7 +63,9 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_create_ex', 'plomgpu_plan_propagate_time',
                'plomgpu_plan_update', 'plomgpu_plan_launch', 'plomgpu_plan_results', 'plomgpu_plan_stream',
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
-               'plomgpu_resample_noalloc', 'plomgpu_last_error']
+               'plomgpu_resample_noalloc', 'plomgpu_last_error', 'plomgpu_batch_create', 'plomgpu_batch_launch',
+               'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
+               'plomgpu_batch_run']
 
 
 def _ptr(a, t):
@@ -145,6 +156,15 @@ def _declare(lib):
     lib.plomgpu_resample_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
     lib.plomgpu_last_error.restype = C.c_char_p
+    lib.plomgpu_batch_create.argtypes = [_P(BatchDesc), _P(C.c_void_p)]
+    lib.plomgpu_batch_launch.argtypes = [C.c_void_p]
+    lib.plomgpu_batch_results.argtypes = [C.c_void_p, _dp, _ip, _dp]
+    lib.plomgpu_batch_stream.argtypes = [C.c_void_p]
+    lib.plomgpu_batch_stream.restype = C.c_void_p
+    lib.plomgpu_batch_config.argtypes = [C.c_void_p, _ip, _ip]
+    lib.plomgpu_batch_destroy.argtypes = [C.c_void_p]
+    lib.plomgpu_batch_destroy.restype = None
+    lib.plomgpu_batch_run.argtypes = [_P(BatchDesc), _dp, _ip]
     return lib
 
 
@@ -240,6 +260,90 @@ class Plan(object):
     def close(self):
         if self.p:
             self.lib.plomgpu_plan_destroy(self.p)
+            self.p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch(object):
+    """Many filters of one model in one persistent launch (plomgpu_batch_*)."""
+
+    def __init__(self, engine, bp, precision=32, block_threads=0):
+        self.engine = engine
+        self.lib = engine.lib
+        self.bp = bp
+        self.keep = {}
+
+        def k(name, a, dt):
+            arr = np.ascontiguousarray(a, dtype=dt)
+            self.keep[name] = arr
+            return arr
+
+        base = bp.base
+        J = k('J', bp.J, np.int32)
+        n_obs = k('n_obs', bp.n_obs, np.int32)
+        rows = k('rows', bp.data_row, np.int64)
+        data = k('data', bp.data, np.float64)
+        par_cac = k('par_cac', bp.par_cac, np.float64)
+        par_ts = k('par_ts', bp.par_ts, np.float64)
+        x0 = k('x0', bp.x0, np.float64)
+        seed = k('seed', bp.seed, np.uint64)
+        n_sub = k('n_sub', base.n_sub, np.int32)
+        t_sub = k('t_sub', base.t_sub, np.float64)
+        t_obs = k('t_obs', base.t_obs, np.float64)
+        cov_cac = k('cov_cac', base.cov_cac if base.cov_cac.size else np.zeros(1), np.float64)
+        cov_ts = k('cov_ts', base.cov_ts if base.cov_ts.size else np.zeros(1), np.float64)
+        coup = k('coup', base.coupling, np.float64) if base.coupling is not None else None
+        dg = k('dg', base.drift_group, np.int32)
+        dng = k('dng', base.drift_ngroups, np.int32)
+        dvol = k('dvol', base.drift_vol, np.float64)
+        nd, ncac = len(base.drift_bt), len(base.drift_bt[0])
+        bts = (BackTransform * (nd * ncac))()
+        for i in range(nd):
+            for c in range(ncac):
+                f, s_, dur, a_, b_, mult = base.drift_bt[i][c]
+                bts[i * ncac + c] = BackTransform(int(f), int(s_), int(dur), 0, float(a_), float(b_), float(mult))
+        self.keep['bts'] = bts
+        self.desc = BatchDesc(
+            n_filters=len(bp.J), J=_ptr(J, _ip), n_obs=_ptr(n_obs, _ip), data_row=rows.ctypes.data_as(_P(C.c_longlong)),
+            data=_ptr(data, _dp), n_rows=data.shape[0], par_cac=_ptr(par_cac, _dp), par_ts=_ptr(par_ts, _dp),
+            x0=_ptr(x0, _dp), seed=seed.ctypes.data_as(_P(C.c_uint64)), max_obs=base.n_obs, n_sub=_ptr(n_sub, _ip),
+            t_sub=_ptr(t_sub, _dp), t_obs=_ptr(t_obs, _dp), dt=base.dt, cov_cac=_ptr(cov_cac, _dp),
+            cov_ts=_ptr(cov_ts, _dp), coupling=_ptr(coup, _dp), drift_group=_ptr(dg, _ip),
+            drift_ngroups=_ptr(dng, _ip), drift_bt=C.cast(bts, _P(BackTransform)), drift_vol=_ptr(dvol, _dp),
+            noises_off=base.noises_off, filter=1 if base.filter else 0, like_min=base.like_min,
+            precision=precision, block_threads=block_threads)
+        self.p = C.c_void_p()
+        check(self.lib, self.lib.plomgpu_batch_create(C.byref(self.desc), C.byref(self.p)))
+
+    def launch(self):
+        check(self.lib, self.lib.plomgpu_batch_launch(self.p))
+
+    def results(self):
+        n = len(self.bp.J)
+        ll = np.zeros(n)
+        nf = np.zeros(n, dtype=np.int32)
+        ess = np.zeros(n)
+        check(self.lib, self.lib.plomgpu_batch_results(self.p, _ptr(ll, _dp), _ptr(nf, _ip), _ptr(ess, _dp)))
+        return ll, nf, ess
+
+    @property
+    def stream(self):
+        return self.lib.plomgpu_batch_stream(self.p)
+
+    @property
+    def config(self):
+        bt, grid = C.c_int(), C.c_int()
+        check(self.lib, self.lib.plomgpu_batch_config(self.p, C.byref(bt), C.byref(grid)))
+        return bt.value, grid.value
+
+    def close(self):
+        if self.p:
+            self.lib.plomgpu_batch_destroy(self.p)
             self.p = C.c_void_p()
 
     def __del__(self):

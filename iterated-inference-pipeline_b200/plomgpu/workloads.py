@@ -17,6 +17,7 @@ noise, numpy Philox generator seeded per workload).  The simulator evaluates
 the same rate expressions through sympy.
 """
 
+import copy
 import datetime
 import math
 
@@ -304,3 +305,123 @@ def load(name, n_obs=None):
     if name == 'seir20x2':
         return with_data(seir20x2(n_obs=n_obs or 520), seed=0)
     raise KeyError(name)
+
+
+# ---------------------------------------------------------------- batches of parameter sets
+def simulate_paths(problem, par_cac, x0, rng):
+    """Euler-Maruyama paths of many parameter sets at once.
+
+    par_cac: [n][N_PAR_PROC][N_CAC], x0: [n][S]; returns incidence [n][n_obs][words].
+    """
+    m = problem.model
+    names, funcs = _rate_functions(m)
+    n = par_cac.shape[0]
+    nsv = len(m.par_sv)
+    X = np.array([x0[i][:nsv * m.N_CAC].reshape(nsv, m.N_CAC) for i in range(n)]).transpose(1, 0, 2)  # [sv][n][cac]
+    par = dict((p, par_cac[:, k, :]) for k, p in enumerate(m.par_proc))
+    cov_names = [p for p in m.par_fixed if p not in m.par_fixed_obs]
+    W = problem.coupling
+    univ = (UNIVERSE, m.remainder)
+    words = []
+    for o in range(m.N_OBS_INC):
+        info = m.obs2ts[o]
+        for u in range(info['n_ts_unique']):
+            words.append((o, [c * m.N_AC + a for (c, a) in info['cac'][u]]))
+    inc_reac = []
+    for defs in m.obs_var_def:
+        if isinstance(defs[0], dict):
+            inc_reac.append([i for i, r in enumerate(m.proc_model) for d in defs
+                             if r['from'] == d['from'] and r['to'] == d['to'] and r['rate'] == d['rate']])
+    dt = problem.dt
+    out = np.zeros((n, problem.n_obs, len(words)))
+    sub = 0
+    for k_obs in range(problem.n_obs):
+        inc = np.zeros((n, len(words)))
+        for _k in range(int(problem.n_sub[k_obs])):
+            t = problem.t_sub[sub]
+            cov = problem.cov_cac[sub]
+            sub += 1
+            env = {'t': t}
+            for i, s in enumerate(m.par_sv):
+                env[s] = X[i]
+            env.update(par)
+            for kk, p in enumerate(cov_names):
+                env[p] = np.broadcast_to(cov[kk], (n, m.N_CAC))
+            npop = X.sum(axis=0) if m.remainder is None else env['N']
+            foi = {}
+            for i, s in enumerate(m.par_sv):
+                foi[s] = (X[i] / npop) @ W.T if W is not None else np.zeros((n, m.N_CAC))
+            args = [env.get(nm, 0.0) for nm in names] + [foi[s] for s in m.par_sv]
+            flows = []
+            for ri, r in enumerate(m.proc_model):
+                rate = np.broadcast_to(np.asarray(funcs[ri](*args), dtype=float), (n, m.N_CAC))
+                base = rate if r['from'] in univ else rate * X[m.par_sv.index(r['from'])]
+                base = np.maximum(base, 0.0)
+                f = base * dt + np.sqrt(base * dt) * rng.standard_normal((n, m.N_CAC))
+                if 'white_noise' in r:
+                    sd = par[r['white_noise']['sd']]
+                    f = f + base * sd * math.sqrt(dt) * rng.standard_normal((n, m.N_CAC))
+                flows.append(f)
+            newX = X.copy()
+            for ri, r in enumerate(m.proc_model):
+                if r['from'] not in univ:
+                    newX[m.par_sv.index(r['from'])] -= flows[ri]
+                if r['to'] not in univ:
+                    newX[m.par_sv.index(r['to'])] += flows[ri]
+            for w, (o, cacs) in enumerate(words):
+                inc[:, w] = np.maximum(inc[:, w] + sum(flows[ri][:, cacs].sum(axis=1) for ri in inc_reac[o]), 0.0)
+            X = np.maximum(newX, 0.0)
+        out[:, k_obs] = inc
+    return out
+
+
+def sir_batch(n_sets=4096, seed=2, J_range=(256, 16384), T_range=(52, 520), sd=0.1):
+    """cfg2: parameter sets of the SIR workload around its values (relative sd 0.1),
+    uneven particle counts and series lengths, data simulated under each set.
+
+    Returns (base Problem with the longest time grid, thetas, J, T, data, seeds)."""
+    from .batch import BatchProblem
+    rng = np.random.Generator(np.random.Philox(seed))
+    files = sir(n_obs=T_range[1])
+    ctx, process, link, theta0 = files
+    base_model = PlomModel(ctx, process, link)
+    base = Problem(base_model, base_model.settings(), theta0, J=1, dt=1.0)
+    thetas = []
+    keys = ['r0', 'v', 'sto', 'mu_b', 'mu_d', 'rep', 'phi']
+    for i in range(n_sets):
+        th = copy.deepcopy(theta0)
+        for k in keys:
+            p = th['parameter'][k]
+            v = p['guess'] * (1.0 + sd * rng.standard_normal())
+            if k == 'rep':
+                v = min(max(v, 0.05), 0.95)
+            v = max(v, 1e-3 * p['guess'])
+            p['guess'] = p['min'] = p['max'] = v
+        r0 = th['parameter']['r0']['guess']
+        S0, I0 = 1.0 / r0, 1e-4
+        for s, val in (('S', S0), ('I', I0), ('R', 1.0 - S0 - I0)):
+            q = th['parameter'][s]
+            q['guess'] = q['min'] = q['max'] = val
+        thetas.append(th)
+    J = rng.integers(J_range[0], J_range[1] + 1, size=n_sets)
+    T = rng.integers(T_range[0], T_range[1] + 1, size=n_sets)
+    from .theta import Parameters
+    pc = np.array([Parameters(base_model, th).par_cac() for th in thetas])
+    pt = np.array([Parameters(base_model, th).par_ts() for th in thetas])
+    x0 = np.array([Parameters(base_model, th).x0(base.pop_size_t0) for th in thetas])
+    inc = simulate_paths(base, pc, x0, rng)
+    m = base_model
+    data = []
+    for i in range(n_sets):
+        y = np.zeros((int(T[i]), m.N_TS))
+        rep = pt[i][m.par_obs.index('rep')]
+        phi = pt[i][m.par_obs.index('phi')]
+        for n in range(int(T[i])):
+            for ts in range(m.N_TS):
+                x = inc[i, n, 0]
+                mu = rep[ts] * x
+                var = rep[ts] * (1.0 - rep[ts]) * x + (rep[ts] * phi[ts] * x) ** 2
+                y[n, ts] = float(max(round(mu + math.sqrt(max(var, 0.0)) * rng.standard_normal()), 0.0))
+        data.append(y)
+    seeds = np.arange(n_sets, dtype=np.uint64) * 7919 + 17
+    return BatchProblem(base, thetas, J, T, data, seeds)
