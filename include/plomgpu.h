@@ -89,6 +89,7 @@ typedef struct plomgpu_smc_desc {
     double like_min;          /* LIKE_MIN (smc -l), default 1e-17 */
     uint64_t seed;            /* Philox key; ignored with CRN draws */
     int precision;            /* 32: FP32 state and log-weights; 64: FP64 everywhere */
+                              /* (with CRN draws in precision 32 the injected normals are rounded to FP32) */
     /* Common random numbers (optional): when crn_normals is set, every normal
      * is read from it: [n][j][k][d] for interval n, particle j, substep k and
      * draw d < plomgpu_draws_per_substep(noises_off) in the reference's draw

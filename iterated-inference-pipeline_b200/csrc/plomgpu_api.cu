@@ -164,10 +164,7 @@ template <class T>
 PropKernel<T> pick_prop(int noises_off, bool crn) {
   const int v = variant_of(noises_off);
   const bool d = drift_on(noises_off);
-  if (crn) {
-    if constexpr (std::is_same<T, double>::value) return pick_v<T, true>(v, d);
-    return nullptr;
-  }
+  if (crn) return pick_v<T, true>(v, d);
   return pick_v<T, false>(v, d);
 }
 
@@ -193,7 +190,7 @@ int enqueue_filter(plomgpu_plan* p) {
   tb.J = J;
 
   PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn);
-  if (!kp) return fail(PLOMGPU_EINVAL, "common random numbers need precision 64");
+  if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
   const size_t smem = propagate_smem_bytes<T, kSmem, kBtProp>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
@@ -282,7 +279,6 @@ int check_desc(const plomgpu_smc_desc* d) {
   if (M::COUPLED && !d->coupling) return fail(PLOMGPU_EINVAL, "coupled model needs a coupling matrix");
   if (drift_on(d->noises_off) && (!d->drift_group || !d->drift_ngroups || !d->drift_bt || !d->drift_vol))
     return fail(PLOMGPU_EINVAL, "drift tables missing");
-  if (d->crn_normals && d->precision != 64) return fail(PLOMGPU_EINVAL, "common random numbers need precision 64");
   if (d->crn_normals && !d->crn_uniforms) return fail(PLOMGPU_EINVAL, "crn_uniforms missing");
   if (!(d->dt > 0.0)) return fail(PLOMGPU_EINVAL, "dt must be > 0");
   if (!(d->like_min > 0.0)) return fail(PLOMGPU_EINVAL, "like_min must be > 0");
