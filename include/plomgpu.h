@@ -156,6 +156,44 @@ void plomgpu_plan_destroy(plomgpu_plan *plan);
 int plomgpu_debug_systematic_points(double U, int J, double *out);
 
 /* ------------------------------------------------------------------------
+ * Iterated filtering (mif, model_builder/C/mif/mif.c:21-247): R independent
+ * runs of J particles, each particle carrying its own transformed
+ * parameters theta[q], q < n_theta (<= 16).  Per observation interval the
+ * particles are propagated with their back-transformed parameters, weighted,
+ * the weighted mean and prediction variance of every component are recorded
+ * (mean_var_theta_theoretical_mif, C/mif/methods.c:133-192), and the
+ * parameters are resampled with the particles and perturbed by a Gaussian
+ * random walk on the estimated components (resample_and_mut_theta_mif,
+ * methods.c:261-367).  The theta-hat update between iterations is left to
+ * the host (update_theta_best_*, methods.c:394-467).  Fitted parameters take
+ * one value for all populations / series (one group). */
+typedef struct plomgpu_mif_desc {
+    int n_runs;
+    int n_theta;
+    const int *proc_slot;   /* [n_par_proc] component of each process parameter, -1: from par_cac */
+    const int *obs_slot;    /* [n_par_obs] component of each observation parameter, -1: from par_ts */
+    const plomgpu_back_transform *theta_bt; /* [n_theta] transformed -> natural scale */
+    const int *estimated;   /* [n_theta] 1: perturbed by the random walk */
+} plomgpu_mif_desc;
+
+typedef struct plomgpu_plan plomgpu_mif;
+
+/* base: the filter problem (data, grid, covariates, fixed parameters, x0,
+ * J particles per run); captures one iteration as a CUDA graph. */
+int plomgpu_mif_create(const plomgpu_smc_desc *base, const plomgpu_mif_desc *mif, plomgpu_mif **out);
+/* One iteration of all runs.  theta_hat [n_runs][n_theta] (transformed
+ * scale); sd_init [n_theta] sd of the initial proposal around theta_hat;
+ * sd_mut [n_obs][n_theta] random-walk sd applied after the resampling of
+ * interval n; vt_add [n_obs][n_theta] theoretical variance added to the
+ * prediction variance of interval n.  Outputs: loglik [n_runs],
+ * n_all_fail [n_runs], bart / vt [n_runs][n_obs][n_theta] (rows of intervals
+ * without data are not written). */
+int plomgpu_mif_iteration(plomgpu_mif *mif, const double *theta_hat, const double *sd_init, const double *sd_mut,
+                          const double *vt_add, uint64_t seed, double *loglik, int *n_all_fail, double *bart,
+                          double *vt);
+void plomgpu_mif_destroy(plomgpu_mif *mif);
+
+/* ------------------------------------------------------------------------
  * Batched filters: many independent filters of one model (different
  * parameters, particle counts, series lengths and data) in one persistent
  * launch.  Serves the callers that evaluate many likelihoods at once (mif

@@ -180,7 +180,7 @@ PLOM_HD void box_muller_f(float u1, float u2, float* z0, float* z1) {
 // with key = (seed low ^ filter * golden, seed high).  Draw blocks of one
 // substep: (substep * (N_CAC + 1) + cac) * blocks + b; slot cac = N_CAC holds
 // the drift draws.
-enum { STREAM_PROCESS = 0, STREAM_RESAMPLE = 1 };
+enum { STREAM_PROCESS = 0, STREAM_RESAMPLE = 1, STREAM_MUTATE = 2, STREAM_INIT = 3 };
 
 struct PhiloxKey {
   uint32_t k0, k1;
@@ -199,10 +199,11 @@ template <class T> struct NormalGen;
 template <> struct NormalGen<float> {
   // 4 normals per Philox block
   template <int N>
-  PLOM_HD static void fill(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk0, float* out) {
+  PLOM_HD static void fill(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk0, float* out,
+                           uint32_t tag = STREAM_PROCESS) {
 #pragma unroll
     for (int b = 0; b < (N + 3) / 4; ++b) {
-      U4 c = {j, n, blk0 + (uint32_t)b, (uint32_t)STREAM_PROCESS};
+      U4 c = {j, n, blk0 + (uint32_t)b, tag};
       const U4 r = philox4x32_10(c, k.k0, k.k1);
       float z0, z1, z2, z3;
       box_muller_f(u01f_radius(r.x), u01f(r.y), &z0, &z1);
@@ -219,10 +220,11 @@ template <> struct NormalGen<float> {
 template <> struct NormalGen<double> {
   // 2 normals per Philox block (53-bit uniforms)
   template <int N>
-  PLOM_HD static void fill(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk0, double* out) {
+  PLOM_HD static void fill(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk0, double* out,
+                           uint32_t tag = STREAM_PROCESS) {
 #pragma unroll
     for (int b = 0; b < (N + 1) / 2; ++b) {
-      U4 c = {j, n, blk0 + (uint32_t)b, (uint32_t)STREAM_PROCESS};
+      U4 c = {j, n, blk0 + (uint32_t)b, tag};
       const U4 r = philox4x32_10(c, k.k0, k.k1);
       double z0, z1;
       box_muller_d(u01d(r.x, r.y), u01d(r.z, r.w), &z0, &z1);

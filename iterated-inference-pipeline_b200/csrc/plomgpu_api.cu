@@ -104,6 +104,22 @@ struct plomgpu_plan {
   // optional timing events around every propagate launch (event record nodes of the graph)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // [2 * n_obs]: before / after propagate n
+  // lock-stepped runs and iterated filtering (per-particle parameters)
+  int R = 1;
+  bool mif = false;
+  int Q = 0;
+  unsigned est_mask = 0;
+  void* theta[2] = {nullptr, nullptr};  // T [Q][R*J]
+  double* theta_hat = nullptr;          // [R][Q]
+  double* sd_init = nullptr;            // [Q]
+  double* sd_mut = nullptr;             // [n_obs][Q]
+  double* vt_add = nullptr;             // [n_obs][Q]
+  double* bart = nullptr;               // [R][n_obs][Q]
+  double* vt = nullptr;                 // [R][n_obs][Q]
+  plomrt::BackTransform* theta_bt = nullptr;
+  int* proc_slot = nullptr;
+  int* obs_slot = nullptr;
+  std::vector<FilterAcc> acc_runs_h;
 };
 
 namespace {
@@ -135,37 +151,41 @@ int upload(const U* h, size_t n, U** d, cudaStream_t s) {
 template <class T>
 using PropKernel = void (*)(const Tables<T>, const StepArgs);
 
-template <class T, int V, bool DRIFT, bool CRN>
+template <class T, int V, bool DRIFT, bool CRN, bool MIF>
 PropKernel<T> pick4() {
-  return &k_propagate<T, V, DRIFT, CRN, kSmem, kBtProp>;
+  return &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp>;
 }
 
-template <class T, bool CRN>
+template <class T, bool CRN, bool MIF>
 PropKernel<T> pick_v(int v, bool drift) {
   if (drift) {
     if constexpr (M::N_DRIFT > 0) {
       switch (v) {
-        case 0: return pick4<T, 0, true, CRN>();
-        case 1: return pick4<T, 1, true, CRN>();
-        case 2: return pick4<T, 2, true, CRN>();
-        default: return pick4<T, 3, true, CRN>();
+        case 0: return pick4<T, 0, true, CRN, MIF>();
+        case 1: return pick4<T, 1, true, CRN, MIF>();
+        case 2: return pick4<T, 2, true, CRN, MIF>();
+        default: return pick4<T, 3, true, CRN, MIF>();
       }
     }
   }
   switch (v) {
-    case 0: return pick4<T, 0, false, CRN>();
-    case 1: return pick4<T, 1, false, CRN>();
-    case 2: return pick4<T, 2, false, CRN>();
-    default: return pick4<T, 3, false, CRN>();
+    case 0: return pick4<T, 0, false, CRN, MIF>();
+    case 1: return pick4<T, 1, false, CRN, MIF>();
+    case 2: return pick4<T, 2, false, CRN, MIF>();
+    default: return pick4<T, 3, false, CRN, MIF>();
   }
 }
 
 template <class T>
-PropKernel<T> pick_prop(int noises_off, bool crn) {
+PropKernel<T> pick_prop(int noises_off, bool crn, bool mif) {
   const int v = variant_of(noises_off);
   const bool d = drift_on(noises_off);
-  if (crn) return pick_v<T, true>(v, d);
-  return pick_v<T, false>(v, d);
+  if (mif) {
+    if (crn) return nullptr;
+    return pick_v<T, false, true>(v, d);
+  }
+  if (crn) return pick_v<T, true, false>(v, d);
+  return pick_v<T, false, false>(v, d);
 }
 
 template <class T>
@@ -188,8 +208,16 @@ int enqueue_filter(plomgpu_plan* p) {
   tb.seed = p->seed;
   tb.filter_id = 0;
   tb.J = J;
+  tb.R = p->R;
+  tb.Q = p->Q;
+  tb.est_mask = p->est_mask;
+  tb.theta_bt = p->theta_bt;
+  tb.proc_slot = p->proc_slot;
+  tb.obs_slot = p->obs_slot;
+  const int R = p->R;
+  const size_t RJ = (size_t)R * J;
 
-  PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn);
+  PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif);
   if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
   const size_t smem = propagate_smem_bytes<T, kSmem, kBtProp>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -199,19 +227,26 @@ int enqueue_filter(plomgpu_plan* p) {
     k_convert<T><<<(n_par + 255) / 256, 256, 0, s>>>(p->par_cac_d, (T*)p->par_cac, n_par);
     ++kernels;
   }
-  k_reset_acc<<<1, 1, 0, s>>>(p->acc);
+  k_reset_acc<<<1, 128, 0, s>>>(p->acc, R);
   ++kernels;
   {
-    const size_t total = (size_t)M::OFF_INC * J;
+    const size_t total = (size_t)M::OFF_INC * RJ;
     const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
-    k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, J, (T*)p->X[0]);
+    k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, (int)RJ, (T*)p->X[0]);
+    ++kernels;
+  }
+  int th_cur = 0;
+  if (p->mif) {
+    const int g = (int)((RJ + 255) / 256 < 4096 ? (RJ + 255) / 256 : 4096);
+    k_mif_init<T><<<g, 256, 0, s>>>(p->theta_hat, p->sd_init, p->Q, p->est_mask, R, J, p->seed, 0u,
+                                    (T*)p->theta[0]);
     ++kernels;
   }
   const int D = p->crn ? draws_per_substep(p->noises_off) : 0;
   size_t crn_off = 0;
   int cur = 0;           // generation holding the particles before interval n
   int anc_cur = -1;      // ancestors to apply when loading (index into p->anc), -1 = identity
-  const int gprop = (J + kBtProp - 1) / kBtProp;
+  const int gprop = (int)((RJ + kBtProp - 1) / kBtProp);
   for (int n = 0; n < p->n_obs; ++n) {
     StepArgs a;
     a.n = n;
@@ -227,23 +262,34 @@ int enqueue_filter(plomgpu_plan* p) {
     a.lw = p->lw;
     a.crn = p->crn ? p->crn_tab + crn_off : nullptr;
     a.crn_d = D;
-    a.x_hist = p->x_hist ? p->x_hist + (size_t)n * M::S * J : nullptr;
+    a.x_hist = p->x_hist ? p->x_hist + (size_t)n * M::S * RJ : nullptr;
     a.write_inc = (p->x_final != nullptr && n == p->n_obs - 1) ? 1 : 0;
-    crn_off += (size_t)J * p->n_sub[n] * D;
+    a.theta_prev = p->mif ? p->theta[th_cur] : nullptr;
+    a.theta_next = p->mif ? p->theta[th_cur ^ 1] : nullptr;
+    // the random walk applies where the previous interval resampled (C/mif/mif.c:190-191)
+    a.sd_mut = (p->mif && n > 0 && p->weigh[n - 1]) ? p->sd_mut + (size_t)(n - 1) * p->Q : nullptr;
+    crn_off += RJ * p->n_sub[n] * D;
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
     kp<<<gprop, kBtProp, smem, s>>>(tb, a);
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n + 1], s, cudaEventRecordExternal));
     ++kernels;
     cur ^= 1;
+    if (p->mif) th_cur ^= 1;
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
       const double Uc = p->crn ? p->crn_u[n] : -1.0;
-      k_weight<T, kBtWeight><<<p->nblk_weight, kBtWeight, 0, s>>>(
+      k_weight<T, kBtWeight><<<dim3(p->nblk_weight, R), kBtWeight, 0, s>>>(
           (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->st, p->acc, p->tstat, p->ntiles, n, Uc,
-          p->seed, 0u, p->llike, p->ess);
-      k_scan<T, kBtScan, kIptScan><<<p->ntiles, kBtScan, 0, s>>>((const T*)p->lw, J, p->thresh, p->st, p->tstat,
-                                                                  p->acc, p->C);
-      k_search<kBtSearch><<<(J + kBtSearch - 1) / kBtSearch, kBtSearch, 0, s>>>(
+          p->seed, 0u, p->llike, p->ess, p->n_obs);
+      if (p->mif) {
+        k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
+                                                            p->thresh, p->st, p->theta_hat, p->vt_add, p->Q, n,
+                                                            p->n_obs, p->bart, p->vt);
+        ++kernels;
+      }
+      k_scan<T, kBtScan, kIptScan><<<dim3(p->ntiles, R), kBtScan, 0, s>>>((const T*)p->lw, J, p->thresh, p->st,
+                                                                         p->tstat, p->acc, p->C);
+      k_search<kBtSearch><<<dim3((J + kBtSearch - 1) / kBtSearch, R), kBtSearch, 0, s>>>(
           p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
       kernels += 3;
       anc_cur = nxt;
@@ -310,22 +356,27 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   const int J = d->J;
   p->tsize = sizeof(T);
   int rc;
-  CK(cudaMalloc(&p->X[0], (size_t)M::S * J * sizeof(T)));
-  CK(cudaMalloc(&p->X[1], (size_t)M::S * J * sizeof(T)));
-  CK(cudaMalloc(&p->lw, (size_t)J * sizeof(T)));
-  CK(cudaMalloc((void**)&p->C, (size_t)J * sizeof(double)));
-  CK(cudaMalloc((void**)&p->anc[0], (size_t)J * sizeof(uint32_t)));
-  CK(cudaMalloc((void**)&p->anc[1], (size_t)J * sizeof(uint32_t)));
+  const size_t RJ = (size_t)p->R * J;
+  CK(cudaMalloc(&p->X[0], (size_t)M::S * RJ * sizeof(T)));
+  CK(cudaMalloc(&p->X[1], (size_t)M::S * RJ * sizeof(T)));
+  CK(cudaMalloc(&p->lw, RJ * sizeof(T)));
+  CK(cudaMalloc((void**)&p->C, RJ * sizeof(double)));
+  CK(cudaMalloc((void**)&p->anc[0], RJ * sizeof(uint32_t)));
+  CK(cudaMalloc((void**)&p->anc[1], RJ * sizeof(uint32_t)));
+  if (p->mif) {
+    CK(cudaMalloc(&p->theta[0], (size_t)p->Q * RJ * sizeof(T)));
+    CK(cudaMalloc(&p->theta[1], (size_t)p->Q * RJ * sizeof(T)));
+  }
   p->nblk_weight = (J + kBtWeight * 4 - 1) / (kBtWeight * 4);
   if (p->nblk_weight > kMaxWeightBlocks) p->nblk_weight = kMaxWeightBlocks;
   if (p->nblk_weight < 1) p->nblk_weight = 1;
   p->ntiles = (J + kTile - 1) / kTile;
-  CK(cudaMalloc((void**)&p->part, (size_t)p->nblk_weight * sizeof(LseAcc)));
-  CK(cudaMalloc((void**)&p->st, sizeof(StepState)));
-  CK(cudaMalloc((void**)&p->acc, sizeof(FilterAcc)));
-  CK(cudaMemsetAsync(p->acc, 0, sizeof(FilterAcc), s));
-  CK(cudaMalloc((void**)&p->tstat, (size_t)p->ntiles * sizeof(TileStatus)));
-  CK(cudaMemsetAsync(p->tstat, 0, (size_t)p->ntiles * sizeof(TileStatus), s));
+  CK(cudaMalloc((void**)&p->part, (size_t)p->R * p->nblk_weight * sizeof(LseAcc)));
+  CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
+  CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
+  CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
+  CK(cudaMalloc((void**)&p->tstat, (size_t)p->R * p->ntiles * sizeof(TileStatus)));
+  CK(cudaMemsetAsync(p->tstat, 0, (size_t)p->R * p->ntiles * sizeof(TileStatus), s));
   CK(cudaMallocHost((void**)&p->acc_h, sizeof(FilterAcc)));
 
   const size_t n_par = (size_t)M::N_PAR_PROC * M::N_CAC;
@@ -363,10 +414,26 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
     if ((rc = upload<double>(d->crn_normals, nd, &p->crn_tab, s))) return rc;
   }
   if (p->want_llike) {
-    CK(cudaMalloc((void**)&p->llike, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double)));
-    CK(cudaMalloc((void**)&p->ess, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double)));
-    CK(cudaMemsetAsync(p->llike, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double), s));
-    CK(cudaMemsetAsync(p->ess, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * sizeof(double), s));
+    const size_t no = (size_t)p->R * (d->n_obs > 0 ? d->n_obs : 1);
+    CK(cudaMalloc((void**)&p->llike, no * sizeof(double)));
+    CK(cudaMalloc((void**)&p->ess, no * sizeof(double)));
+    CK(cudaMemsetAsync(p->llike, 0, no * sizeof(double), s));
+    CK(cudaMemsetAsync(p->ess, 0, no * sizeof(double), s));
+  }
+  if (p->mif) {
+    const size_t nq = (size_t)(d->n_obs > 0 ? d->n_obs : 1) * p->Q;
+    CK(cudaMalloc((void**)&p->theta_hat, (size_t)p->R * p->Q * sizeof(double)));
+    CK(cudaMalloc((void**)&p->sd_init, (size_t)p->Q * sizeof(double)));
+    CK(cudaMalloc((void**)&p->sd_mut, nq * sizeof(double)));
+    CK(cudaMalloc((void**)&p->vt_add, nq * sizeof(double)));
+    CK(cudaMalloc((void**)&p->bart, (size_t)p->R * nq * sizeof(double)));
+    CK(cudaMalloc((void**)&p->vt, (size_t)p->R * nq * sizeof(double)));
+    CK(cudaMemsetAsync(p->theta_hat, 0, (size_t)p->R * p->Q * sizeof(double), s));
+    CK(cudaMemsetAsync(p->sd_init, 0, (size_t)p->Q * sizeof(double), s));
+    CK(cudaMemsetAsync(p->sd_mut, 0, nq * sizeof(double), s));
+    CK(cudaMemsetAsync(p->vt_add, 0, nq * sizeof(double), s));
+    CK(cudaMemsetAsync(p->bart, 0, (size_t)p->R * nq * sizeof(double), s));
+    CK(cudaMemsetAsync(p->vt, 0, (size_t)p->R * nq * sizeof(double), s));
   }
   if (p->want_anc) CK(cudaMalloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
   if (p->want_xpred) CK(cudaMalloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
@@ -399,7 +466,9 @@ void plan_free(plomgpu_plan* p) {
   void* bufs[] = {p->X[0], p->X[1], p->lw, p->C, p->anc[0], p->anc[1], p->part, p->st, p->acc, p->tstat,
                   p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
-                  p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final};
+                  p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
+                  p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
+                  p->obs_slot};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (p->acc_h) cudaFreeHost(p->acc_h);
@@ -410,7 +479,7 @@ void plan_free(plomgpu_plan* p) {
 }
 
 int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bool want_xpred, bool want_final,
-                bool timing = false) {
+                bool timing = false, const plomgpu_mif_desc* mif = nullptr) {
   *out = nullptr;
   int rc = check_desc(d);
   if (rc) return rc;
@@ -426,6 +495,14 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->want_anc = want_anc;
   p->want_xpred = want_xpred;
   p->timing = timing;
+  if (mif) {
+    p->R = mif->n_runs;
+    p->mif = true;
+    p->Q = mif->n_theta;
+    p->est_mask = 0u;
+    for (int q = 0; q < mif->n_theta; ++q)
+      if (mif->estimated[q]) p->est_mask |= 1u << q;
+  }
   p->dt = d->dt;
   p->like_min = d->like_min;
   p->thresh = pow(d->like_min, (double)M::N_TS);
@@ -455,6 +532,18 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
     if (e != cudaSuccess) {
       plan_free(p);
       return fail(PLOMGPU_ENOMEM, "x_final allocation failed");
+    }
+  }
+  if (mif) {
+    int rc2;
+    if ((rc2 = upload<plomrt::BackTransform>((const plomrt::BackTransform*)mif->theta_bt, (size_t)mif->n_theta,
+                                             &p->theta_bt, p->stream)) ||
+        (rc2 = upload<int>(mif->proc_slot, (size_t)(M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 0), &p->proc_slot, p->stream)) ||
+        (rc2 = upload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream))) {
+      std::string keep = g_err;
+      plan_free(p);
+      g_err = keep;
+      return rc2;
     }
   }
   rc = (d->precision == 64) ? plan_build<double>(d, p) : plan_build<float>(d, p);
@@ -627,6 +716,59 @@ const char* plomgpu_last_error(void) { return g_err.c_str(); }
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// Iterated filtering: R runs of J particles with per-particle parameters,
+// advanced in lock step by one captured graph per iteration.
+extern "C" int plomgpu_mif_create(const plomgpu_smc_desc* base, const plomgpu_mif_desc* m, plomgpu_mif** out) {
+  if (!out || !base || !m) return fail(PLOMGPU_EINVAL, "null argument");
+  *out = nullptr;
+  if (m->n_runs < 1) return fail(PLOMGPU_EINVAL, "n_runs must be >= 1");
+  if (m->n_theta < 1 || m->n_theta > kMaxTheta)
+    return fail(PLOMGPU_EINVAL, "n_theta must be in [1, " + std::to_string(kMaxTheta) + "]");
+  if (!m->theta_bt || !m->estimated || (M::N_PAR_PROC > 0 && !m->proc_slot) || (M::N_PAR_OBS > 0 && !m->obs_slot))
+    return fail(PLOMGPU_EINVAL, "missing arrays");
+  for (int k = 0; k < M::N_PAR_PROC; ++k)
+    if (m->proc_slot[k] < -1 || m->proc_slot[k] >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad proc_slot");
+  for (int k = 0; k < M::N_PAR_OBS; ++k)
+    if (m->obs_slot[k] < -1 || m->obs_slot[k] >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad obs_slot");
+  if (base->crn_normals) return fail(PLOMGPU_EINVAL, "iterated filtering draws its own numbers");
+  if ((long long)m->n_runs * base->J > (1LL << 31) - 1) return fail(PLOMGPU_EINVAL, "n_runs * J too large");
+  return plan_create(base, out, false, false, false, false, m);
+}
+
+extern "C" int plomgpu_mif_iteration(plomgpu_mif* p, const double* theta_hat, const double* sd_init,
+                                     const double* sd_mut, const double* vt_add, uint64_t seed, double* loglik,
+                                     int* n_all_fail, double* bart, double* vt) {
+  if (!p || !p->mif) return fail(PLOMGPU_EINVAL, "not an iterated-filtering plan");
+  if (!theta_hat || !sd_init || !sd_mut || !vt_add) return fail(PLOMGPU_EINVAL, "null input");
+  const size_t nq = (size_t)p->n_obs * p->Q;
+  cudaStream_t s = p->stream;
+  CK(cudaMemcpyAsync(p->theta_hat, theta_hat, (size_t)p->R * p->Q * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(p->sd_init, sd_init, (size_t)p->Q * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (nq) {
+    CK(cudaMemcpyAsync(p->sd_mut, sd_mut, nq * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(p->vt_add, vt_add, nq * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemcpyAsync(p->seed, &seed, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGraphLaunch(p->exec, s));
+  p->acc_runs_h.resize(p->R);
+  CK(cudaMemcpyAsync(p->acc_runs_h.data(), p->acc, (size_t)p->R * sizeof(FilterAcc), cudaMemcpyDeviceToHost, s));
+  if (bart && nq) CK(cudaMemcpyAsync(bart, p->bart, (size_t)p->R * nq * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (vt && nq) CK(cudaMemcpyAsync(vt, p->vt, (size_t)p->R * nq * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  int err = 0;
+  for (int r = 0; r < p->R; ++r) {
+    if (loglik) loglik[r] = p->acc_runs_h[r].loglik;
+    if (n_all_fail) n_all_fail[r] = p->acc_runs_h[r].n_all_fail;
+    err |= p->acc_runs_h[r].error;
+  }
+  if (err) return fail(PLOMGPU_ETIMEOUT, "a bounded device wait ran out");
+  return PLOMGPU_OK;
+}
+
+extern "C" void plomgpu_mif_destroy(plomgpu_mif* p) { plan_free(p); }
+
+// ---------------------------------------------------------------------------
 // Resampling without allocation.
 //
 // Some callers cannot allocate device memory: a plug-in hosted inside another
@@ -674,7 +816,7 @@ int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, do
   // contents are still there
   k_reset_acc<<<1, 1, 0, s>>>(&sc->acc);
   k_weight<T, kBtWeight><<<nblk, kBtWeight, 0, s>>>(lw, J, thresh, log(like_min), sc->part, &sc->st, &sc->acc,
-                                                   sc->tstat, ntiles, 0, u, nullptr, 0u, out, out + 1);
+                                                   sc->tstat, ntiles, 0, u, nullptr, 0u, out, out + 1, 0);
   k_scan<T, kBtScan, kIptScan><<<ntiles, kBtScan, 0, s>>>(lw, J, thresh, &sc->st, sc->tstat, &sc->acc, sc->C);
   k_search<kBtSearch><<<(J + kBtSearch - 1) / kBtSearch, kBtSearch, 0, s>>>(sc->C, J, &sc->st, anc, nullptr);
   k_noalloc_out<<<1, 1, 0, s>>>(&sc->st, &sc->acc, out);

@@ -124,9 +124,18 @@ struct Tables {
   double dt;
   double like_min;
   const uint64_t* seed;      // device copy of the Philox seed (updatable without re-capture)
-  uint32_t filter_id;
-  int J;
+  uint32_t filter_id;        // Philox key of run r uses filter_id + r
+  int J;                     // particles per run
+  int R;                     // runs advanced in lock step (1 for a plain filter)
+  // per-particle parameters (iterated filtering); unused when the kernel has MIF = false
+  int Q;                                 // theta components (<= kMaxTheta)
+  unsigned est_mask;                     // components perturbed by the random walk
+  const plomrt::BackTransform* theta_bt; // [Q] transformed -> natural
+  const int* proc_slot;                  // [N_PAR_PROC] component of each process parameter, -1: table
+  const int* obs_slot;                   // [N_PAR_OBS] component of each observation parameter, -1: table
 };
+
+constexpr int kMaxTheta = 16;
 
 struct StepArgs {
   int n;                  // interval index
@@ -144,6 +153,27 @@ struct StepArgs {
   int crn_d;              // D
   double* x_hist;         // optional [S][J] double copy of the propagated particles
   int write_inc;          // 1: also store the incidence words in X_next
+  const void* theta_prev; // [Q][R*J] (T) per-particle transformed parameters, MIF only
+  void* theta_next;       // [Q][R*J] (T)
+  const double* sd_mut;   // [Q] random-walk sd applied when gathering from ancestors, NULL: none
+};
+
+// environments with per-particle parameters (iterated filtering)
+template <class T>
+struct MifProcEnv : ProcEnv<T> {
+  T parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
+  unsigned uni;
+  __device__ __forceinline__ T par(int p, int cac) const {
+    return ((uni >> p) & 1u) ? parp[p] : this->par_[p * M::N_CAC + cac];
+  }
+};
+
+struct MifObsEnv : ObsEnv {
+  double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
+  unsigned uni;
+  __device__ __forceinline__ double par_ts(int p, int ts) const {
+    return ((uni >> p) & 1u) ? obsp[p] : __ldg(par_ts_ + p * M::N_TS + ts);
+  }
 };
 
 // ------------------------------------------------------------------ propagate
@@ -159,7 +189,7 @@ constexpr size_t propagate_smem_bytes() {
   return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) + (SMEM ? (size_t)M::S * BT * sizeof(T) : 0);
 }
 
-template <class T, int V, bool DRIFT, bool CRN, bool SMEM, int BT>
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_coup = reinterpret_cast<T*>(smem_raw);
@@ -171,9 +201,12 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
   __syncthreads();
   const int J = tb.J;
-  const int j = blockIdx.x * BT + threadIdx.x;
-  if (j >= J) return;
-  const uint32_t src = a.anc ? __ldg(a.anc + j) : (uint32_t)j;
+  const size_t RJ = (size_t)tb.R * J;
+  const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;  // particle of all runs
+  if (g >= RJ) return;
+  const int r = (int)(g / J);
+  const int j = (int)(g - (size_t)r * J);                  // slot within its run
+  const size_t src = (size_t)r * J + (a.anc ? __ldg(a.anc + g) : (uint32_t)j);
   const T* __restrict__ Xp = (const T*)a.X_prev;
   T* __restrict__ Xn = (T*)a.X_next;
 
@@ -183,11 +216,12 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     x.b = s_state + threadIdx.x;
   }
 #pragma unroll
-  for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * J + src];
+  for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * RJ + src];
 #pragma unroll
   for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);  // reset_inc
 
-  ProcEnv<T> e;
+  typedef typename std::conditional<MIF, MifProcEnv<T>, ProcEnv<T>>::type PEnv;
+  PEnv e;
   e.par_ = s_par;
   e.coup_ = s_coup;
   e.dgroup_ = tb.drift_group;
@@ -195,7 +229,58 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   e.dbt_ = tb.drift_bt;
   e.dvol_ = tb.drift_vol;
   const T dt = (T)tb.dt;
-  const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id);
+  const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id + (uint32_t)r);
+
+  typedef typename std::conditional<MIF, MifObsEnv, ObsEnv>::type OEnv;
+  OEnv oe;
+  oe.par_ts_ = tb.par_ts;
+  oe.cov_ts_ = a.cov_ts;
+  if constexpr (MIF) {
+    // gather this particle's parameters from its ancestor, perturb them
+    // (resample_and_mut_theta_mif, model_builder/C/mif/methods.c:261-367), keep
+    // them for the next interval and back-transform them
+    // (back_transform_theta2par per particle, C/mif/mif.c:142-144)
+    const T* __restrict__ thp = (const T*)a.theta_prev;
+    T* __restrict__ thn = (T*)a.theta_next;
+    double nat[kMaxTheta];
+#pragma unroll
+    for (int q = 0; q < kMaxTheta; ++q) {
+      nat[q] = 0.0;
+      if (q < tb.Q) {
+        T v = thp[(size_t)q * RJ + src];
+        if (a.sd_mut && ((tb.est_mask >> q) & 1u)) {
+          T z[1];
+          plomrt::NormalGen<T>::template fill<1>(key, (uint32_t)j, (uint32_t)a.n, (uint32_t)q, z,
+                                                 (uint32_t)plomrt::STREAM_MUTATE);
+          v += (T)__ldg(a.sd_mut + q) * z[0];
+        }
+        thn[(size_t)q * RJ + g] = v;
+        nat[q] = (double)plomrt::back_transform<T>(v, tb.theta_bt[q]);
+      }
+    }
+    e.uni = 0u;
+#pragma unroll
+    for (int k = 0; k < M::N_PAR_PROC; ++k) {
+      const int slot = __ldg(tb.proc_slot + k);
+      T v = T(0);
+#pragma unroll
+      for (int q = 0; q < kMaxTheta; ++q)
+        if (q == slot) v = (T)nat[q];
+      e.parp[k] = v;
+      if (slot >= 0) e.uni |= 1u << k;
+    }
+    oe.uni = 0u;
+#pragma unroll
+    for (int k = 0; k < M::N_PAR_OBS; ++k) {
+      const int slot = __ldg(tb.obs_slot + k);
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < kMaxTheta; ++q)
+        if (q == slot) v = nat[q];
+      oe.obsp[k] = v;
+      if (slot >= 0) oe.uni |= 1u << k;
+    }
+  }
 
   for (int k = 0; k < a.n_sub; ++k) {
     const int sub = a.sub0 + k;
@@ -203,7 +288,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     const T t = (T)__ldg(tb.t_sub + sub);
     if constexpr (CRN) {
       TableDraws<T, V> d;
-      d.p = a.crn + ((size_t)j * a.n_sub + k) * a.crn_d;
+      d.p = a.crn + ((size_t)g * a.n_sub + k) * a.crn_d;
       M::template step<V, DRIFT, T>(x, t, dt, e, d);
     } else {
       PhiloxDraws<T, V> d;
@@ -217,19 +302,16 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
 
 #pragma unroll
   for (int w = 0; w < M::S; ++w) {
-    if (w < M::OFF_INC || a.write_inc) Xn[(size_t)w * J + j] = x[w];
+    if (w < M::OFF_INC || a.write_inc) Xn[(size_t)w * RJ + g] = x[w];
   }
   if (a.x_hist) {
 #pragma unroll
-    for (int w = 0; w < M::S; ++w) a.x_hist[(size_t)w * J + j] = (double)x[w];
+    for (int w = 0; w < M::S; ++w) a.x_hist[(size_t)w * RJ + g] = (double)x[w];
   }
 
   if (a.weigh) {
     double obs[M::N_TS];
     M::template proj2obs<T>(x, obs);
-    ObsEnv oe;
-    oe.par_ts_ = tb.par_ts;
-    oe.cov_ts_ = a.cov_ts;
     double ll = 0.0;
 #pragma unroll
     for (int ts = 0; ts < M::N_TS; ++ts) {
@@ -239,7 +321,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
       ll += log(plomrt::disc_normal_like(y, mu, var, tb.like_min));
     }
-    ((T*)a.lw)[j] = (T)ll;
+    ((T*)a.lw)[g] = (T)ll;
   }
 }
 
@@ -311,9 +393,20 @@ template <class T, int BT>
 __global__ void __launch_bounds__(BT) k_weight(const T* __restrict__ lw, int J, double thresh, double log_like_min,
                                                LseAcc* part, StepState* st, FilterAcc* acc, TileStatus* tstat,
                                                int ntiles, int n, double U_crn, const uint64_t* seed, uint32_t filter_id,
-                                               double* llike_out, double* ess_out) {
+                                               double* llike_out, double* ess_out, int out_stride) {
   __shared__ LseAcc sh[BT / 32];
   __shared__ bool last;
+  {  // run r of the lock-stepped runs
+    const int r = blockIdx.y;
+    lw += (size_t)r * J;
+    part += (size_t)r * gridDim.x;
+    st += r;
+    acc += r;
+    tstat += (size_t)r * ntiles;
+    if (llike_out) llike_out += (size_t)r * out_stride;
+    if (ess_out) ess_out += (size_t)r * out_stride;
+    filter_id += (uint32_t)r;
+  }
   LseAcc a = {-INFINITY, 0.0, 0.0, 0};
   for (int i = blockIdx.x * BT + threadIdx.x; i < J; i += gridDim.x * BT) {
     const T l = lw[i];
@@ -404,6 +497,14 @@ template <class T, int BT, int IPT>
 __global__ void __launch_bounds__(BT) k_scan(const T* __restrict__ lw, int J, double thresh, const StepState* st,
                                              TileStatus* tstat, FilterAcc* acc, double* __restrict__ C) {
   constexpr int TILE = BT * IPT;
+  {
+    const int r = blockIdx.y;
+    lw += (size_t)r * J;
+    st += r;
+    acc += r;
+    tstat += (size_t)r * gridDim.x;
+    C += (size_t)r * J;
+  }
   __shared__ double sv[TILE];
   __shared__ double swarp[BT / 32];
   __shared__ int s_tile;
@@ -495,6 +596,13 @@ __global__ void __launch_bounds__(BT) k_search(const double* __restrict__ C, int
                                                uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
   __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
   __shared__ int s_ns, s_fail;
+  {
+    const int r = blockIdx.y;
+    C += (size_t)r * J;
+    st += r;
+    anc += (size_t)r * J;
+    if (anc_hist) anc_hist += (size_t)r * J;
+  }
   if (threadIdx.x == 0) {
     s_ns = st->nseg;
     s_fail = st->all_fail;
@@ -547,12 +655,99 @@ __global__ void k_identity(uint32_t* __restrict__ out, int J) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J; j += gridDim.x * blockDim.x) out[j] = (uint32_t)j;
 }
 
-__global__ void k_reset_acc(FilterAcc* acc) {
-  acc->loglik = 0.0;
-  acc->n_all_fail = 0;
-  acc->error = 0;
-  acc->ticket = 0u;
-  acc->tile_ticket = 0u;
+__global__ void k_reset_acc(FilterAcc* acc, int R = 1) {
+  for (int r = threadIdx.x; r < R; r += blockDim.x) {
+    acc[r].loglik = 0.0;
+    acc[r].n_all_fail = 0;
+    acc[r].error = 0;
+    acc[r].ticket = 0u;
+    acc[r].tile_ticket = 0u;
+  }
+}
+
+// ------------------------------------------------------------------ iterated filtering
+// Initial parameters of every particle of every run: theta_hat of the run plus a
+// Gaussian proposal on the estimated components (propose_safe_theta_and_load_X0
+// with ran_proposal, model_builder/C/mif/mif.c:119-121, C/core/proposal.c:40-62).
+template <class T>
+__global__ void k_mif_init(const double* __restrict__ theta_hat, const double* __restrict__ sd_init, int Q,
+                           unsigned est_mask, int R, int J, const uint64_t* seed, uint32_t filter_id,
+                           T* __restrict__ theta) {
+  const size_t RJ = (size_t)R * J;
+  for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < RJ; g += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(g / J);
+    const int j = (int)(g - (size_t)r * J);
+    const plomrt::PhiloxKey key = plomrt::make_key(*seed, filter_id + (uint32_t)r);
+    for (int q = 0; q < Q; ++q) {
+      double v = theta_hat[(size_t)r * Q + q];
+      if ((est_mask >> q) & 1u) {
+        T z[1];
+        plomrt::NormalGen<T>::template fill<1>(key, (uint32_t)j, 0u, (uint32_t)q, z, (uint32_t)plomrt::STREAM_INIT);
+        v += sd_init[q] * (double)z[0];
+      }
+      theta[(size_t)q * RJ + g] = (T)v;
+    }
+  }
+}
+
+// Filtered mean (weighted) and prediction variance (unweighted, plus the
+// theoretical variance of the perturbation) of every component, per run
+// (mean_var_theta_theoretical_mif, model_builder/C/mif/methods.c:133-192).
+// Grid (Q, R); the sums are shifted by theta_hat for a stable variance.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT) k_mif_moments(const T* __restrict__ lw, const T* __restrict__ theta, int J, int R,
+                                                    double thresh, const StepState* st,
+                                                    const double* __restrict__ theta_hat, const double* __restrict__ vt_add,
+                                                    int Q, int n, int n_obs, double* bart, double* vt) {
+  const int q = blockIdx.x, r = blockIdx.y;
+  const size_t RJ = (size_t)R * J;
+  const StepState* s = st + r;
+  const double m = s->m, s1 = s->s1;
+  const int all_fail = s->all_fail;
+  const double c = theta_hat[(size_t)r * Q + q];
+  double sw = 0.0, sd = 0.0, sd2 = 0.0;
+  for (int j = threadIdx.x; j < J; j += BT) {
+    const size_t g = (size_t)r * J + j;
+    const double th = (double)theta[(size_t)q * RJ + g];
+    double w;
+    if (all_fail) {
+      w = 1.0 / (double)J;
+    } else {
+      const T l = lw[g];
+      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+    }
+    sw += w * th;
+    const double d = th - c;
+    sd += d;
+    sd2 += d * d;
+  }
+  __shared__ double sh[3][BT / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    sw += __shfl_xor_sync(0xffffffffu, sw, off);
+    sd += __shfl_xor_sync(0xffffffffu, sd, off);
+    sd2 += __shfl_xor_sync(0xffffffffu, sd2, off);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[0][warp] = sw;
+    sh[1][warp] = sd;
+    sh[2][warp] = sd2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, c2 = 0.0;
+    for (int w = 0; w < BT / 32; ++w) {
+      a += sh[0][w];
+      b += sh[1][w];
+      c2 += sh[2][w];
+    }
+    double var = (J > 1) ? (c2 - b * b / (double)J) / ((double)J - 1.0) : 0.0;
+    if (!(var >= 0.0) || isinf(var)) var = 0.0;
+    const size_t o = ((size_t)r * n_obs + n) * Q + q;
+    bart[o] = a;
+    vt[o] = var + vt_add[(size_t)n * Q + q];
+  }
 }
 
 __global__ void k_sys_points(double U, int J, double* out, int* err) {

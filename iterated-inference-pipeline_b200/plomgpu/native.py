@@ -54,6 +54,11 @@ class BatchDesc(C.Structure):
                 ('filter', C.c_int), ('like_min', C.c_double), ('precision', C.c_int), ('block_threads', C.c_int)]
 
 
+class MifDesc(C.Structure):
+    _fields_ = [('n_runs', C.c_int), ('n_theta', C.c_int), ('proc_slot', _ip), ('obs_slot', _ip),
+                ('theta_bt', _P(BackTransform)), ('estimated', _ip)]
+
+
 class SmcResult(C.Structure):
     _fields_ = [('loglik', C.c_double), ('n_all_fail', C.c_int), ('status', C.c_int),
                 ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp)]
@@ -65,7 +70,7 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
                'plomgpu_resample_noalloc', 'plomgpu_last_error', 'plomgpu_batch_create', 'plomgpu_batch_launch',
                'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
-               'plomgpu_batch_run']
+               'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy']
 
 
 def _ptr(a, t):
@@ -165,6 +170,10 @@ def _declare(lib):
     lib.plomgpu_batch_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_batch_destroy.restype = None
     lib.plomgpu_batch_run.argtypes = [_P(BatchDesc), _dp, _ip]
+    lib.plomgpu_mif_create.argtypes = [_P(SmcDesc), _P(MifDesc), _P(C.c_void_p)]
+    lib.plomgpu_mif_iteration.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_uint64, _dp, _ip, _dp, _dp]
+    lib.plomgpu_mif_destroy.argtypes = [C.c_void_p]
+    lib.plomgpu_mif_destroy.restype = None
     return lib
 
 
@@ -344,6 +353,61 @@ class Batch(object):
     def close(self):
         if self.p:
             self.lib.plomgpu_batch_destroy(self.p)
+            self.p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MifDescHolder(object):
+    """plomgpu_mif_desc of n_runs runs over the components ``components``:
+    list of (kind, index, back_transform tuple, estimated) with kind 'proc' or 'obs'."""
+
+    def __init__(self, n_runs, components, n_par_proc, n_par_obs):
+        self.R = int(n_runs)
+        self.Q = len(components)
+        self.proc_slot = np.full(max(n_par_proc, 1), -1, dtype=np.int32)
+        self.obs_slot = np.full(max(n_par_obs, 1), -1, dtype=np.int32)
+        self.bts = (BackTransform * max(self.Q, 1))()
+        self.estimated = np.zeros(max(self.Q, 1), dtype=np.int32)
+        for q, (kind, idx, bt, est) in enumerate(components):
+            (self.proc_slot if kind == 'proc' else self.obs_slot)[idx] = q
+            f, s_, dur, a_, b_, mult = bt
+            self.bts[q] = BackTransform(int(f), int(s_), int(dur), 0, float(a_), float(b_), float(mult))
+            self.estimated[q] = 1 if est else 0
+        self.desc = MifDesc(self.R, self.Q, _ptr(self.proc_slot, _ip), _ptr(self.obs_slot, _ip),
+                            C.cast(self.bts, _P(BackTransform)), _ptr(self.estimated, _ip))
+
+
+class MifPlan(object):
+    """plomgpu_mif_*: lock-stepped iterated-filtering runs on the GPU."""
+
+    def __init__(self, engine, problem, mif_holder, precision=None):
+        self.engine = engine
+        self.lib = engine.lib
+        self.h = DescHolder(problem, precision=precision)
+        self.m = mif_holder
+        self.problem = problem
+        self.p = C.c_void_p()
+        check(self.lib, self.lib.plomgpu_mif_create(C.byref(self.h.desc), C.byref(self.m.desc), C.byref(self.p)))
+
+    def iteration(self, theta_hat, sd_init, sd_mut, vt_add, seed):
+        R, Q, T = self.m.R, self.m.Q, self.problem.n_obs
+        ll = np.zeros(R)
+        nf = np.zeros(R, dtype=np.int32)
+        bart = np.zeros((R, T, Q))
+        vt = np.zeros((R, T, Q))
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (theta_hat, sd_init, sd_mut, vt_add)]
+        check(self.lib, self.lib.plomgpu_mif_iteration(self.p, *(x.ctypes.data_as(_dp) for x in a), C.c_uint64(seed),
+                                                       _ptr(ll, _dp), _ptr(nf, _ip), _ptr(bart, _dp), _ptr(vt, _dp)))
+        return ll, nf, bart, vt
+
+    def close(self):
+        if self.p:
+            self.lib.plomgpu_mif_destroy(self.p)
             self.p = C.c_void_p()
 
     def __del__(self):

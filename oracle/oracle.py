@@ -40,6 +40,8 @@ class Oracle(object):
         L.oracle_like.restype = C.c_double
         L.oracle_weight_and_resample.argtypes = [_dp, C.c_int, C.c_double, C.c_double, _dp, _dp,
                                                  C.POINTER(C.c_uint32)]
+        L.oracle_mif_iteration.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.MifDesc), _dp, _dp, _dp, _dp,
+                                           _dp, C.POINTER(C.c_int), _dp, _dp]
         L.oracle_proj2obs.argtypes = [_dp, _dp]
         L.oracle_proj2obs.restype = None
         self.info = native.ModelInfo()
@@ -65,6 +67,23 @@ class Oracle(object):
         fail = self.lib.oracle_weight_and_resample(w.ctypes.data_as(_dp), len(w), like_min, U, C.byref(ll),
                                                    C.byref(ess), sel.ctypes.data_as(C.POINTER(C.c_uint32)))
         return w, sel, ll.value, ess.value, fail
+
+    def mif_iteration(self, problem, mif_desc_holder, theta_hat, sd_init, sd_mut, vt_add, seed):
+        """One iterated-filtering iteration of every run (FP64, Philox draws of the GPU's FP64 mode)."""
+        import copy as _copy
+        p = _copy.copy(problem)
+        p.seed = seed
+        h = native.DescHolder(p, precision=64)
+        R, Q, T = mif_desc_holder.R, mif_desc_holder.Q, problem.n_obs
+        ll = np.zeros(R)
+        nf = np.zeros(R, dtype=np.int32)
+        bart = np.zeros((R, T, Q))
+        vt = np.zeros((R, T, Q))
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (theta_hat, sd_init, sd_mut, vt_add)]
+        self.lib.oracle_mif_iteration(C.byref(h.desc), C.byref(mif_desc_holder.desc), *(x.ctypes.data_as(_dp) for x in a),
+                                      ll.ctypes.data_as(_dp), nf.ctypes.data_as(C.POINTER(C.c_int)),
+                                      bart.ctypes.data_as(_dp), vt.ctypes.data_as(_dp))
+        return ll, nf, bart, vt
 
     def systematic_points(self, U, J, table=False):
         out = np.zeros(J)

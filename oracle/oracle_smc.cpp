@@ -353,6 +353,185 @@ int oracle_weight_and_resample(double* w, int J, double like_min, double U, doub
   return n_all_fail;
 }
 
+// ---------------------------------------------------------------------------
+// One iteration of iterated filtering for R runs (the body of the m loop of
+// mif(), model_builder/C/mif/mif.c:115-200, with diagonal proposals):
+// per-particle parameters proposed around theta_hat (ran_proposal), per
+// interval back-transformed (back_transform_theta2par), particles propagated
+// and weighted, weighted mean / prediction variance of every component
+// (mean_var_theta_theoretical_mif, C/mif/methods.c:133-192), systematic
+// resampling, parameters resampled and perturbed (resample_and_mut_theta_mif,
+// methods.c:261-367), particles resampled.  Draws: Philox with the counter
+// layout of the GPU's FP64 mode.
+}  // extern "C"
+
+namespace {
+
+struct HostMifEnv : HostEnv {
+  double parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
+  unsigned uni;
+  double par(int p, int cac) const { return ((uni >> p) & 1u) ? parp[p] : par_[p * M::N_CAC + cac]; }
+};
+
+struct HostMifObsEnv : HostObsEnv {
+  double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
+  unsigned uni;
+  double par_ts(int p, int ts) const { return ((uni >> p) & 1u) ? obsp[p] : par_ts_[p * M::N_TS + ts]; }
+};
+
+template <int V, bool DRIFT>
+void mif_propagate(double* x, const plomgpu_smc_desc* d, const HostMifEnv& e0, int n, int j, int sub0, uint32_t run) {
+  HostMifEnv e = e0;
+  HostState xs;
+  xs.b = x;
+  for (int k = 0; k < d->n_sub[n]; ++k) {
+    const int sub = sub0 + k;
+    e.cov_ = d->cov_cac ? d->cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC : nullptr;
+    PhiloxSource<V> src;
+    src.key = plomrt::make_key(d->seed, run);
+    src.j = (uint32_t)j;
+    src.n = (uint32_t)n;
+    src.sub = (uint32_t)k;
+    M::step<V, DRIFT, double>(xs, d->t_sub[sub], d->dt, e, src);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, const double* theta_hat,
+                         const double* sd_init, const double* sd_mut, const double* vt_add, double* loglik,
+                         int* n_all_fail_out, double* bart, double* vt) {
+  const int J = d->J, S = M::S, Q = mf->n_theta, R = mf->n_runs;
+  const int v = d->noises_off & 3;
+  const bool drift = M::N_DRIFT > 0 && !(d->noises_off & PLOMGPU_NO_DRIFT);
+  typedef void (*MP)(double*, const plomgpu_smc_desc*, const HostMifEnv&, int, int, int, uint32_t);
+  MP prop;
+  if (drift) prop = v == 0 ? &mif_propagate<0, true> : v == 1 ? &mif_propagate<1, true> : v == 2 ? &mif_propagate<2, true> : &mif_propagate<3, true>;
+  else prop = v == 0 ? &mif_propagate<0, false> : v == 1 ? &mif_propagate<1, false> : v == 2 ? &mif_propagate<2, false> : &mif_propagate<3, false>;
+  for (int r = 0; r < R; ++r) {
+    const plomrt::PhiloxKey key = plomrt::make_key(d->seed, (uint32_t)r);
+    std::vector<double> X((size_t)J * S), Xn((size_t)J * S), th((size_t)J * Q), thn((size_t)J * Q), w(J);
+    std::vector<uint32_t> select(J);
+    for (int j = 0; j < J; ++j) {
+      for (int s = 0; s < S; ++s) X[(size_t)j * S + s] = (s < M::OFF_INC) ? d->x0[s] : 0.0;
+      for (int q = 0; q < Q; ++q) {
+        double t = theta_hat[(size_t)r * Q + q];
+        if (mf->estimated[q]) {
+          double z[1];
+          plomrt::NormalGen<double>::fill<1>(key, (uint32_t)j, 0u, (uint32_t)q, z, (uint32_t)plomrt::STREAM_INIT);
+          t += sd_init[q] * z[0];
+        }
+        th[(size_t)j * Q + q] = t;
+      }
+    }
+    double Llike = 0.0;
+    int n_all_fail = 0;
+    int sub0 = 0;
+    for (int n = 0; n < d->n_obs; ++n) {
+      const double* y = d->data + (size_t)n * M::N_TS;
+      int n_nonan = 0;
+      for (int ts = 0; ts < M::N_TS; ++ts)
+        if (!isnan(y[ts])) ++n_nonan;
+#pragma omp parallel for schedule(static)
+      for (int j = 0; j < J; ++j) {
+        HostMifEnv e;
+        e.par_ = d->par_cac;
+        e.coup_ = d->coupling;
+        e.dgroup_ = d->drift_group;
+        e.dng_ = d->drift_ngroups;
+        e.dbt_ = d->drift_bt;
+        e.dvol_ = d->drift_vol;
+        e.uni = 0u;
+        HostMifObsEnv oe;
+        oe.par_ts_ = d->par_ts;
+        oe.cov_ts_ = d->cov_ts ? d->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS : nullptr;
+        oe.uni = 0u;
+        double nat[32];
+        for (int q = 0; q < Q; ++q) {
+          plomrt::BackTransform bt;
+          memcpy(&bt, &mf->theta_bt[q], sizeof(bt));
+          nat[q] = plomrt::back_transform<double>(th[(size_t)j * Q + q], bt);
+        }
+        for (int k = 0; k < M::N_PAR_PROC; ++k) {
+          e.parp[k] = mf->proc_slot[k] >= 0 ? nat[mf->proc_slot[k]] : 0.0;
+          if (mf->proc_slot[k] >= 0) e.uni |= 1u << k;
+        }
+        for (int k = 0; k < M::N_PAR_OBS; ++k) {
+          oe.obsp[k] = mf->obs_slot[k] >= 0 ? nat[mf->obs_slot[k]] : 0.0;
+          if (mf->obs_slot[k] >= 0) oe.uni |= 1u << k;
+        }
+        double* x = &Xn[(size_t)j * S];
+        memcpy(x, &X[(size_t)j * S], sizeof(double) * S);
+        for (int s = M::OFF_INC; s < S; ++s) x[s] = 0.0;
+        prop(x, d, e, n, j, sub0, (uint32_t)r);
+        if (n_nonan) {
+          double obs[M::N_TS];
+          HostState xs;
+          xs.b = x;
+          M::proj2obs<double>(xs, obs);
+          double ll = 0.0;
+          for (int ts = 0; ts < M::N_TS; ++ts) {
+            if (isnan(y[ts])) continue;
+            const double mu = M::obs_mean(obs[ts], ts, d->t_obs[n], oe);
+            const double var = M::obs_var(obs[ts], ts, d->t_obs[n], oe);
+            ll += log(plomrt::disc_normal_like(y[ts], mu, var, d->like_min));
+          }
+          w[j] = exp(ll);
+        }
+      }
+      sub0 += d->n_sub[n];
+      const bool weigh = d->filter && n_nonan > 0;
+      if (weigh) {
+        double llike_n = 0.0, ess = 0.0;
+        const int ok = weight(w, J, d->like_min, &llike_n, &ess, &Llike, &n_all_fail, select.data());
+        // moments of the parameters used in this interval (weights normalised)
+        for (int q = 0; q < Q; ++q) {
+          double bt = 0.0, kn = 0.0, avg = 0.0, M2 = 0.0;
+          for (int j = 0; j < J; ++j) {
+            const double t = th[(size_t)j * Q + q];
+            kn += 1.0;
+            const double delta = t - avg;
+            avg += delta / kn;
+            M2 += delta * (t - avg);
+            bt += w[j] * t;
+          }
+          double var = M2 / (kn - 1.0);
+          if (!(var >= 0.0) || isinf(var)) var = 0.0;
+          const size_t o = ((size_t)r * d->n_obs + n) * Q + q;
+          bart[o] = bt;
+          vt[o] = var + vt_add[(size_t)n * Q + q];
+        }
+        if (ok) {
+          const double u = plomrt::resample_uniform(key, (uint32_t)n);
+          systematic_sampling(w, J, (1.0 / (double)J) * u, select.data());
+        }
+        for (int j = 0; j < J; ++j) {
+          const size_t s = (size_t)select[j];
+          for (int k = 0; k < S; ++k) X[(size_t)j * S + k] = Xn[s * S + k];
+          for (int q = 0; q < Q; ++q) {
+            double t = th[s * Q + q];
+            if (mf->estimated[q]) {
+              double z[1];
+              plomrt::NormalGen<double>::fill<1>(key, (uint32_t)j, (uint32_t)(n + 1), (uint32_t)q, z,
+                                                 (uint32_t)plomrt::STREAM_MUTATE);
+              t += sd_mut[(size_t)n * Q + q] * z[0];
+            }
+            thn[(size_t)j * Q + q] = t;
+          }
+        }
+        th.swap(thn);
+      } else {
+        X.swap(Xn);
+      }
+    }
+    loglik[r] = Llike;
+    n_all_fail_out[r] = n_all_fail;
+  }
+  return 0;
+}
+
 // Systematic points exactly as the reference walks them (ran += inc).
 void oracle_systematic_points_sequential(double U, int J, double* out) {
   const double inc = 1.0 / (double)J;
