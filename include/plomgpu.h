@@ -244,6 +244,45 @@ void plomgpu_batch_destroy(plomgpu_batch *batch);
 /* One-shot: create, launch, results, destroy. */
 int plomgpu_batch_run(const plomgpu_batch_desc *desc, double *loglik, int *n_all_fail);
 
+/* ------------------------------------------------------------------------
+ * Likelihood server for concurrent callers (pmcmc chains, C/pmcmc/pmcmc.c:
+ * 186-266): requests (parameters, initial state, seed, J) on one data set
+ * are queued, admitted while their HBM footprint fits the memory budget,
+ * and run concurrently.  Models whose particle fits registers run on a
+ * device-resident loop (a persistent kernel taking requests from a ring in
+ * mapped host memory, one CTA per request, continuous batching); larger
+ * models run on a pool of captured plans, one stream each.  A result does
+ * not depend on what else runs: each request is computed by the same
+ * deterministic kernels alone or in the mix.  Thread-safe. */
+typedef struct plomgpu_server_opts {
+    int max_J;              /* largest particle count of a request */
+    double memory_budget;   /* bytes of HBM the requests may hold (0: 150e9) */
+    int ring_slots;         /* requests in flight on the device loop (0: 1024) */
+    int plan_pool;          /* concurrent plans for models served per plan (0: 8) */
+    int precision;          /* 32 or 64 */
+} plomgpu_server_opts;
+
+typedef struct plomgpu_server_stats {
+    long long pending, in_flight, completed, launches, peak_in_flight;
+    double bytes_in_use, peak_bytes;
+    int persistent_loop;    /* 1: device-resident loop, 0: plan pool */
+} plomgpu_server_stats;
+
+typedef struct plomgpu_server plomgpu_server;
+
+/* base: the shared data set, time grid, covariates and default parameters
+ * (base->J is ignored). */
+int plomgpu_server_create(const plomgpu_smc_desc *base, const plomgpu_server_opts *opts, plomgpu_server **out);
+/* par_cac / par_ts / x0 may be NULL to use the base values. */
+int plomgpu_server_submit(plomgpu_server *server, int J, const double *par_cac, const double *par_ts,
+                          const double *x0, uint64_t seed, long long *ticket);
+int plomgpu_server_poll(plomgpu_server *server, long long ticket, int *done, double *loglik, int *n_all_fail,
+                        double *latency_s);
+int plomgpu_server_wait(plomgpu_server *server, long long ticket, double timeout_s, double *loglik,
+                        int *n_all_fail, double *latency_s);
+int plomgpu_server_get_stats(plomgpu_server *server, plomgpu_server_stats *stats);
+void plomgpu_server_destroy(plomgpu_server *server);
+
 /* Resamples one observation interval without allocating device memory.
  *
  * No counterpart in the reference.  For callers that cannot allocate: a

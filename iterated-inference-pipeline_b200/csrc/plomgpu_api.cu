@@ -1224,3 +1224,260 @@ int plomgpu_batch_run(const plomgpu_batch_desc* d, double* loglik, int* n_all_fa
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Likelihood server (see serve_host.cuh / smc_serve.cuh).
+#include "serve_host.cuh"
+
+namespace {
+
+template <class T>
+int server_build(plomgpu_server* sv, int dev) {
+  cudaStream_t s = sv->stream;
+  int rc;
+  const plomgpu_smc_desc& d = sv->base;
+  std::vector<int> sub0(d.n_obs);
+  long long tot = 0;
+  for (int n = 0; n < d.n_obs; ++n) {
+    sub0[n] = (int)tot;
+    tot += d.n_sub[n];
+  }
+  if ((rc = upload<int>(d.n_sub, (size_t)d.n_obs, &sv->d_n_sub, s))) return rc;
+  if ((rc = upload<int>(sub0.data(), sub0.size(), &sv->d_sub0, s))) return rc;
+  if ((rc = upload<double>(d.t_sub, (size_t)tot, &sv->d_t_sub, s))) return rc;
+  if ((rc = upload<double>(d.t_obs, (size_t)d.n_obs, &sv->d_t_obs, s))) return rc;
+  if ((rc = upload<double>(d.data, (size_t)d.n_obs * M::N_TS, &sv->d_data, s))) return rc;
+  if ((rc = upload_as<T>(d.cov_cac, (size_t)tot * M::N_COV_CAC * M::N_CAC, &sv->d_cov_cac, s))) return rc;
+  if ((rc = upload<double>(d.cov_ts, (size_t)d.n_obs * M::N_COV_TS * M::N_TS, &sv->d_cov_ts, s))) return rc;
+  if (M::COUPLED && (rc = upload_as<T>(d.coupling, (size_t)M::N_CAC * M::N_CAC, &sv->d_coupling, s))) return rc;
+  if (drift_on(d.noises_off)) {
+    if ((rc = upload_as<T>(d.drift_vol, (size_t)M::N_DRIFT * M::N_CAC, &sv->d_drift_vol, s))) return rc;
+    if ((rc = upload<int>(d.drift_group, (size_t)M::N_DRIFT * M::N_CAC, &sv->d_drift_group, s))) return rc;
+    if ((rc = upload<int>(d.drift_ngroups, (size_t)M::N_DRIFT, &sv->d_drift_ngroups, s))) return rc;
+    if ((rc = upload<plomrt::BackTransform>((const plomrt::BackTransform*)d.drift_bt, (size_t)M::N_DRIFT * M::N_CAC,
+                                            &sv->d_drift_bt, s)))
+      return rc;
+  }
+  CK(cudaMalloc((void**)&sv->d_error, sizeof(int)));
+  CK(cudaMemsetAsync(sv->d_error, 0, sizeof(int), s));
+  CK(cudaHostAlloc((void**)&sv->slots_h, (size_t)sv->ring * sizeof(ServeSlot), cudaHostAllocMapped | cudaHostAllocPortable));
+  CK(cudaHostAlloc((void**)&sv->ctl_h, sizeof(ServeCtl), cudaHostAllocMapped | cudaHostAllocPortable));
+  CK(cudaHostAlloc((void**)&sv->map_h, (size_t)sv->ring * sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+  memset(sv->slots_h, 0, (size_t)sv->ring * sizeof(ServeSlot));
+  memset(sv->ctl_h, 0, sizeof(ServeCtl));
+  memset(sv->map_h, 0, (size_t)sv->ring * sizeof(int));
+  CK(cudaHostGetDevicePointer((void**)&sv->slots_d, sv->slots_h, 0));
+  CK(cudaHostGetDevicePointer((void**)&sv->ctl_d, sv->ctl_h, 0));
+  CK(cudaHostGetDevicePointer((void**)&sv->map_d, sv->map_h, 0));
+  CK(cudaMalloc((void**)&sv->d_head, sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(sv->d_head, 0, sizeof(unsigned long long), s));
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  size_t pool = std::min(sv->budget, (size_t)sv->ring * serve_ws_bytes(sv, sv->max_J));
+  pool = std::min(pool, (size_t)(0.8 * (double)free_b));
+  if (pool < serve_ws_bytes(sv, sv->max_J)) return fail(PLOMGPU_ENOMEM, "memory budget below one request");
+  CK(cudaMalloc((void**)&sv->d_pool, pool));
+  sv->pool.init(pool);
+  int sms = 0, per_sm = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ServeKernel<T> k = pick_serve<T>(d.noises_off);
+  if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, sv->bt, 0));
+  sv->grid = sms * std::max(per_sm, 1);
+  CK(cudaStreamSynchronize(s));
+  return PLOMGPU_OK;
+}
+
+void server_free(plomgpu_server* sv) {
+  if (!sv) return;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->stop = true;
+  }
+  sv->cv.notify_all();
+  if (sv->worker.joinable()) sv->worker.join();
+  if (sv->ctl_h) __atomic_store_n(&sv->ctl_h->stop, 1, __ATOMIC_RELEASE);
+  if (sv->stream) cudaStreamSynchronize(sv->stream);
+  for (auto& pp : sv->plans) {
+    if (pp.plan) plan_free(pp.plan);
+    if (pp.done_ev) cudaEventDestroy(pp.done_ev);
+  }
+  void* bufs[] = {sv->d_n_sub, sv->d_sub0, sv->d_t_sub, sv->d_t_obs, sv->d_cov_ts, sv->d_data, sv->d_cov_cac,
+                  sv->d_coupling, sv->d_drift_vol, sv->d_drift_group, sv->d_drift_ngroups, sv->d_drift_bt,
+                  sv->d_error, sv->d_head, sv->d_pool};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (sv->slots_h) cudaFreeHost(sv->slots_h);
+  if (sv->ctl_h) cudaFreeHost(sv->ctl_h);
+  if (sv->map_h) cudaFreeHost(sv->map_h);
+  if (sv->kernel_ev) cudaEventDestroy(sv->kernel_ev);
+  if (sv->stream) cudaStreamDestroy(sv->stream);
+  delete sv;
+}
+
+}  // namespace
+
+extern "C" {
+
+int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* o, plomgpu_server** out) {
+  if (!d || !o || !out) return fail(PLOMGPU_EINVAL, "null argument");
+  *out = nullptr;
+  if (o->max_J < 1) return fail(PLOMGPU_EINVAL, "max_J must be >= 1");
+  plomgpu_smc_desc chk = *d;
+  chk.J = o->max_J;
+  chk.crn_normals = nullptr;
+  chk.crn_uniforms = nullptr;
+  chk.precision = o->precision;
+  int rc = check_desc(&chk);
+  if (rc) return rc;
+  int dev = 0, ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PLOMGPU_ENODEV, "no CUDA device");
+  CK(cudaGetDevice(&dev));
+  plomgpu_server* sv = new plomgpu_server();
+  sv->precision = o->precision;
+  sv->max_J = o->max_J;
+  sv->ring = o->ring_slots > 0 ? o->ring_slots : 1024;
+  sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 8;
+  sv->budget = o->memory_budget > 0 ? (size_t)o->memory_budget : (size_t)150e9;
+  // keep host copies of the shared problem
+  const int n = d->n_obs;
+  long long tot = 0;
+  for (int i = 0; i < n; ++i) tot += d->n_sub[i];
+  sv->n_sub_h.assign(d->n_sub, d->n_sub + n);
+  sv->t_sub_h.assign(d->t_sub, d->t_sub + tot);
+  sv->t_obs_h.assign(d->t_obs, d->t_obs + n);
+  sv->data_h.assign(d->data, d->data + (size_t)n * M::N_TS);
+  if (d->cov_cac) sv->cov_cac_h.assign(d->cov_cac, d->cov_cac + (size_t)tot * M::N_COV_CAC * M::N_CAC);
+  if (d->cov_ts) sv->cov_ts_h.assign(d->cov_ts, d->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS);
+  if (d->coupling) sv->coupling_h.assign(d->coupling, d->coupling + (size_t)M::N_CAC * M::N_CAC);
+  if (drift_on(d->noises_off)) {
+    sv->drift_vol_h.assign(d->drift_vol, d->drift_vol + (size_t)M::N_DRIFT * M::N_CAC);
+    sv->drift_group_h.assign(d->drift_group, d->drift_group + (size_t)M::N_DRIFT * M::N_CAC);
+    sv->drift_ngroups_h.assign(d->drift_ngroups, d->drift_ngroups + M::N_DRIFT);
+    sv->drift_bt_h.assign(d->drift_bt, d->drift_bt + (size_t)M::N_DRIFT * M::N_CAC);
+  }
+  sv->par_cac_h.assign(d->par_cac, d->par_cac + (size_t)M::N_PAR_PROC * M::N_CAC);
+  sv->par_ts_h.assign(d->par_ts, d->par_ts + (size_t)M::N_PAR_OBS * M::N_TS);
+  sv->x0_h.assign(d->x0, d->x0 + M::S);
+  sv->base = *d;
+  sv->base.precision = o->precision;
+  sv->base.crn_normals = nullptr;
+  sv->base.crn_uniforms = nullptr;
+  sv->base.n_sub = sv->n_sub_h.data();
+  sv->base.t_sub = sv->t_sub_h.data();
+  sv->base.t_obs = sv->t_obs_h.data();
+  sv->base.data = sv->data_h.data();
+  sv->base.cov_cac = sv->cov_cac_h.empty() ? nullptr : sv->cov_cac_h.data();
+  sv->base.cov_ts = sv->cov_ts_h.empty() ? nullptr : sv->cov_ts_h.data();
+  sv->base.coupling = sv->coupling_h.empty() ? nullptr : sv->coupling_h.data();
+  sv->base.drift_vol = sv->drift_vol_h.empty() ? nullptr : sv->drift_vol_h.data();
+  sv->base.drift_group = sv->drift_group_h.empty() ? nullptr : sv->drift_group_h.data();
+  sv->base.drift_ngroups = sv->drift_ngroups_h.empty() ? nullptr : sv->drift_ngroups_h.data();
+  sv->base.drift_bt = sv->drift_bt_h.empty() ? nullptr : sv->drift_bt_h.data();
+  sv->base.par_cac = sv->par_cac_h.data();
+  sv->base.par_ts = sv->par_ts_h.data();
+  sv->base.x0 = sv->x0_h.data();
+  cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->kernel_ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    server_free(sv);
+    return fail(PLOMGPU_ECUDA, std::string("stream/event: ") + cudaGetErrorString(e));
+  }
+  if (sv->persistent) {
+    rc = (o->precision == 64) ? server_build<double>(sv, dev) : server_build<float>(sv, dev);
+    if (rc) {
+      std::string keep = g_err;
+      server_free(sv);
+      g_err = keep;
+      return rc;
+    }
+    sv->slot_ticket.assign(sv->ring, -1);
+    sv->slot_off.assign(sv->ring, 0);
+    sv->slot_bytes.assign(sv->ring, 0);
+    sv->slot_t.assign(sv->ring, Clock::now());
+    for (int i = 0; i < sv->ring; ++i) sv->free_slots.push_back(i);
+  }
+  sv->worker = std::thread([sv, dev]() {
+    cudaSetDevice(dev);
+    serve_loop(sv);
+  });
+  *out = sv;
+  return PLOMGPU_OK;
+}
+
+int plomgpu_server_submit(plomgpu_server* sv, int J, const double* par_cac, const double* par_ts, const double* x0,
+                          uint64_t seed, long long* ticket) {
+  if (!sv || !ticket) return fail(PLOMGPU_EINVAL, "null argument");
+  if (J < 1 || J > sv->max_J) return fail(PLOMGPU_EINVAL, "J out of range [1, max_J]");
+  ServeRequest rq;
+  rq.J = J;
+  rq.seed = seed;
+  rq.par_cac.assign(par_cac ? par_cac : sv->par_cac_h.data(),
+                    (par_cac ? par_cac : sv->par_cac_h.data()) + (size_t)M::N_PAR_PROC * M::N_CAC);
+  rq.par_ts.assign(par_ts ? par_ts : sv->par_ts_h.data(),
+                   (par_ts ? par_ts : sv->par_ts_h.data()) + (size_t)M::N_PAR_OBS * M::N_TS);
+  rq.x0.assign(x0 ? x0 : sv->x0_h.data(), (x0 ? x0 : sv->x0_h.data()) + M::S);
+  rq.t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    rq.ticket = sv->next_ticket++;
+    *ticket = rq.ticket;
+    sv->results[rq.ticket] = ServeResult();
+    sv->pending.push_back(std::move(rq));
+  }
+  sv->cv.notify_all();
+  return PLOMGPU_OK;
+}
+
+int plomgpu_server_poll(plomgpu_server* sv, long long ticket, int* done, double* loglik, int* n_all_fail,
+                        double* latency_s) {
+  if (!sv || !done) return fail(PLOMGPU_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  auto it = sv->results.find(ticket);
+  if (it == sv->results.end()) return fail(PLOMGPU_EINVAL, "unknown ticket");
+  *done = it->second.done ? 1 : 0;
+  if (it->second.done) {
+    if (loglik) *loglik = it->second.loglik;
+    if (n_all_fail) *n_all_fail = it->second.n_all_fail;
+    if (latency_s) *latency_s = it->second.latency_s;
+    if (it->second.status) return fail(it->second.status, "request failed");
+  }
+  return PLOMGPU_OK;
+}
+
+int plomgpu_server_wait(plomgpu_server* sv, long long ticket, double timeout_s, double* loglik, int* n_all_fail,
+                        double* latency_s) {
+  if (!sv) return fail(PLOMGPU_EINVAL, "null argument");
+  std::unique_lock<std::mutex> lock(sv->mu);
+  auto it = sv->results.find(ticket);
+  if (it == sv->results.end()) return fail(PLOMGPU_EINVAL, "unknown ticket");
+  const auto until = Clock::now() + std::chrono::duration<double>(timeout_s);
+  while (!sv->results[ticket].done) {
+    if (sv->cv_done.wait_until(lock, until) == std::cv_status::timeout && !sv->results[ticket].done)
+      return fail(PLOMGPU_ETIMEOUT, "request not finished before the timeout");
+  }
+  const ServeResult& r = sv->results[ticket];
+  if (loglik) *loglik = r.loglik;
+  if (n_all_fail) *n_all_fail = r.n_all_fail;
+  if (latency_s) *latency_s = r.latency_s;
+  if (r.status) return fail(r.status, "request failed");
+  return PLOMGPU_OK;
+}
+
+int plomgpu_server_get_stats(plomgpu_server* sv, plomgpu_server_stats* st) {
+  if (!sv || !st) return fail(PLOMGPU_EINVAL, "null argument");
+  std::lock_guard<std::mutex> lock(sv->mu);
+  st->pending = (long long)sv->pending.size();
+  st->in_flight = sv->in_flight;
+  st->completed = sv->completed;
+  st->launches = sv->launches;
+  st->peak_in_flight = sv->peak_in_flight;
+  st->bytes_in_use = (double)(sv->pool.used + sv->plan_bytes_total);
+  st->peak_bytes = (double)(sv->pool.peak + sv->plan_bytes_total);
+  st->persistent_loop = sv->persistent ? 1 : 0;
+  return PLOMGPU_OK;
+}
+
+void plomgpu_server_destroy(plomgpu_server* sv) { server_free(sv); }
+
+}  // extern "C"

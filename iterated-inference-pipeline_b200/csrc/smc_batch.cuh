@@ -139,184 +139,215 @@ __device__ inline double block_exscan(double v, double* sh, double* tot) {
   return excl;
 }
 
+// Shared memory of one CTA running whole filters.
+template <class T, int BT>
+struct CtaShared {
+  LseAcc lse[BT / 32];
+  double scan[BT / 32];
+  plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  int f, ns, fail;
+  double m, s1;
+  __align__(16) T coup[kSmemCoup > 0 ? kSmemCoup : 4];
+  __align__(16) T par[kSmemPar > 0 ? kSmemPar : 4];
+  double par_ts[M::N_PAR_OBS * M::N_TS > 0 ? M::N_PAR_OBS * M::N_TS : 1];
+};
+
+// One filter on the calling CTA: every interval of `job` (propagate, block
+// log-sum-exp, chunked FP64 scan, ancestor search).  All threads of the CTA
+// call it; outputs are written by thread 0.
+struct FilterJob {
+  int J;
+  int n_obs;
+  uint64_t seed;
+  const double* data;     // first row of the filter's data
+  const double* par_cac;  // [N_PAR_PROC][N_CAC]
+  const double* par_ts;   // [N_PAR_OBS][N_TS]
+  const double* x0;       // [S]
+};
+
+template <class T, int V, bool DRIFT, int BT>
+__device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const FilterJob& job, const BatchWs<T>& ws,
+                           const size_t ld, double* out_ll, int* out_nf, double* out_ess) {
+  const int J = job.J;
+  for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) sh.par[i] = (T)job.par_cac[i];
+  for (int i = threadIdx.x; i < M::N_PAR_OBS * M::N_TS; i += BT) sh.par_ts[i] = job.par_ts[i];
+  for (int j = threadIdx.x; j < J; j += BT) {
+#pragma unroll
+    for (int w = 0; w < M::OFF_INC; ++w) ws.X[0][(size_t)w * ld + j] = (T)job.x0[w];
+  }
+  __syncthreads();
+  ProcEnv<T> e;
+  e.par_ = sh.par;
+  e.coup_ = sh.coup;
+  e.dgroup_ = a.drift_group;
+  e.dng_ = a.drift_ngroups;
+  e.dbt_ = a.drift_bt;
+  e.dvol_ = a.drift_vol;
+  ObsEnv oe;
+  oe.par_ts_ = sh.par_ts;
+  const plomrt::PhiloxKey key = plomrt::make_key(job.seed, 0u);
+  const T dt = (T)a.dt;
+  double loglik = 0.0, ess_min = INFINITY;
+  int n_all_fail = 0;
+  int cur = 0;
+  bool resampled = false;
+  for (int n = 0; n < job.n_obs; ++n) {
+    const double* y = job.data + (size_t)n * M::N_TS;
+    bool any = false;
+#pragma unroll
+    for (int ts = 0; ts < M::N_TS; ++ts) any |= !isnan(y[ts]);
+    const bool weigh = a.filter_on && any;
+    oe.cov_ts_ = a.cov_ts + (size_t)n * M::N_COV_TS * M::N_TS;
+    const int K = __ldg(a.n_sub + n), sub0 = __ldg(a.sub0 + n);
+    const double t_obs = __ldg(a.t_obs + n);
+    const T* Xp = ws.X[cur];
+    T* Xn = ws.X[cur ^ 1];
+    LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
+    for (int j = threadIdx.x; j < J; j += BT) {
+      const uint32_t src = resampled ? ws.anc[j] : (uint32_t)j;
+      RegState<T, M::S> x;
+#pragma unroll
+      for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * ld + src];
+#pragma unroll
+      for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);
+      for (int k = 0; k < K; ++k) {
+        const int sub = sub0 + k;
+        e.cov_ = a.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
+        const T t = (T)__ldg(a.t_sub + sub);
+        PhiloxDraws<T, V> d;
+        d.key = key;
+        d.j = (uint32_t)j;
+        d.n = (uint32_t)n;
+        d.sub = (uint32_t)k;
+        M::template step<V, DRIFT, T>(x, t, dt, e, d);
+      }
+#pragma unroll
+      for (int w = 0; w < M::OFF_INC; ++w) Xn[(size_t)w * ld + j] = x[w];
+      if (weigh) {
+        double obs[M::N_TS];
+        M::template proj2obs<T>(x, obs);
+        double ll = 0.0;
+#pragma unroll
+        for (int ts = 0; ts < M::N_TS; ++ts) {
+          const double yy = y[ts];
+          if (isnan(yy)) continue;
+          const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
+          const double var = M::obs_var(obs[ts], ts, t_obs, oe);
+          ll += log(plomrt::disc_normal_like(yy, mu, var, a.like_min));
+        }
+        const T l = (T)ll;
+        ws.lw[j] = l;
+        if (weight_fails(l, a.thresh)) {
+          acc.nfail += 1;
+        } else {
+          LseAcc b = {(double)l, 1.0, 1.0, 0};
+          acc = lse_merge(acc, b);
+        }
+      }
+    }
+    cur ^= 1;
+    if (!weigh) {
+      resampled = false;
+      __syncthreads();
+      continue;
+    }
+    acc = block_lse<BT>(acc, sh.lse);  // (syncs: Xn / lw visible to the block)
+    if (threadIdx.x == 0) {
+      const int all_fail = (acc.nfail == J);
+      double llike, ess;
+      if (all_fail) {
+        llike = a.log_like_min * (double)M::N_TS;
+        ess = 0.0;
+        n_all_fail += 1;
+      } else {
+        llike = acc.m + log(acc.s1 / (double)J);
+        ess = (acc.s1 * acc.s1) / acc.s2;
+      }
+      loglik += llike;
+      ess_min = fmin(ess_min, ess);
+      sh.fail = all_fail;
+      sh.m = acc.m;
+      sh.s1 = acc.s1;
+      const double inc = 1.0 / (double)J;
+      const double U = inc * plomrt::resample_uniform(key, (uint32_t)n);
+      int ns = plomrt::systematic_table(U, inc, J, sh.seg, plomrt::SYS_MAX_SEG);
+      if (ns < 0) {
+        atomicOr(a.error, (int)ERR_SYS_TABLE);
+        ns = 0;
+      }
+      sh.ns = ns;
+    }
+    __syncthreads();
+    if (sh.fail || sh.ns == 0) {
+      for (int j = threadIdx.x; j < J; j += BT) ws.anc[j] = (uint32_t)j;
+    } else {
+      // cumulative normalised weights: each thread a contiguous chunk
+      const int P = (J + BT - 1) / BT;
+      const int i0 = threadIdx.x * P;
+      const int i1 = min(J, i0 + P);
+      const double m = sh.m, s1 = sh.s1;
+      double run = 0.0;
+      for (int i = i0; i < i1; ++i) {
+        const T l = ws.lw[i];
+        run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+      }
+      double tot;
+      const double pre = block_exscan<BT>(run, sh.scan, &tot);
+      run = pre;
+      for (int i = i0; i < i1; ++i) {
+        const T l = ws.lw[i];
+        run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+        ws.C[i] = run;
+      }
+      __syncthreads();
+      const int ns = sh.ns;
+      for (int j = threadIdx.x; j < J; j += BT) {
+        const double ran = plomrt::systematic_point(sh.seg, ns, j);
+        int lo = 0, hi = J - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (ran > ws.C[mid]) lo = mid + 1; else hi = mid;
+        }
+        ws.anc[j] = (uint32_t)lo;
+      }
+    }
+    resampled = true;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *out_ll = loglik;
+    *out_nf = n_all_fail;
+    if (out_ess) *out_ess = ess_min;
+  }
+}
+
 template <class T, int V, bool DRIFT, int BT>
 __global__ void __launch_bounds__(BT) k_batch(const BatchArgs<T> a) {
-  __shared__ LseAcc sh_lse[BT / 32];
-  __shared__ double sh_scan[BT / 32];
-  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  __shared__ int s_f, s_ns, s_fail;
-  __shared__ double s_m, s_s1;
-  __shared__ __align__(16) T s_coup[kSmemCoup > 0 ? kSmemCoup : 4];
-  __shared__ __align__(16) T s_par[kSmemPar > 0 ? kSmemPar : 4];
-
+  __shared__ CtaShared<T, BT> sh;
   if constexpr (M::COUPLED) {
-    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = a.coupling[i];
+    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) sh.coup[i] = a.coupling[i];
   }
   const BatchWs<T> ws = batch_ws<T>(a.ws + blockIdx.x * a.ws_stride, a.max_J);
   const size_t ld = (size_t)((a.max_J + 31) & ~31);
-
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) {
       const unsigned t = atomicAdd(a.queue, 1u);
-      s_f = (t < (unsigned)a.n_filters) ? a.order[t] : -1;
+      sh.f = (t < (unsigned)a.n_filters) ? a.order[t] : -1;
     }
     __syncthreads();
-    const int f = s_f;
+    const int f = sh.f;
     if (f < 0) break;
     const BatchFilter fl = a.filters[f];
-    const int J = fl.J;
-    for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT)
-      s_par[i] = (T)a.par_cac[(size_t)f * M::N_PAR_PROC * M::N_CAC + i];
-    const double* x0 = a.x0 + (size_t)f * M::S;
-    for (int j = threadIdx.x; j < J; j += BT) {
-#pragma unroll
-      for (int w = 0; w < M::OFF_INC; ++w) ws.X[0][(size_t)w * ld + j] = (T)x0[w];
-    }
-    __syncthreads();
-    ProcEnv<T> e;
-    e.par_ = s_par;
-    e.coup_ = s_coup;
-    e.dgroup_ = a.drift_group;
-    e.dng_ = a.drift_ngroups;
-    e.dbt_ = a.drift_bt;
-    e.dvol_ = a.drift_vol;
-    ObsEnv oe;
-    oe.par_ts_ = a.par_ts + (size_t)f * M::N_PAR_OBS * M::N_TS;
-    const plomrt::PhiloxKey key = plomrt::make_key(fl.seed, 0u);
-    const T dt = (T)a.dt;
-    double loglik = 0.0, ess_min = INFINITY;
-    int n_all_fail = 0;
-    int cur = 0;
-    bool resampled = false;
-    for (int n = 0; n < fl.n_obs; ++n) {
-      const double* y = a.data + (size_t)(fl.data_row + n) * M::N_TS;
-      bool any = false;
-#pragma unroll
-      for (int ts = 0; ts < M::N_TS; ++ts) any |= !isnan(__ldg(y + ts));
-      const bool weigh = a.filter_on && any;
-      oe.cov_ts_ = a.cov_ts + (size_t)n * M::N_COV_TS * M::N_TS;
-      const int K = __ldg(a.n_sub + n), sub0 = __ldg(a.sub0 + n);
-      const double t_obs = __ldg(a.t_obs + n);
-      const T* Xp = ws.X[cur];
-      T* Xn = ws.X[cur ^ 1];
-      LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
-      for (int j = threadIdx.x; j < J; j += BT) {
-        const uint32_t src = resampled ? ws.anc[j] : (uint32_t)j;
-        RegState<T, M::S> x;
-#pragma unroll
-        for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * ld + src];
-#pragma unroll
-        for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);
-        for (int k = 0; k < K; ++k) {
-          const int sub = sub0 + k;
-          e.cov_ = a.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
-          const T t = (T)__ldg(a.t_sub + sub);
-          PhiloxDraws<T, V> d;
-          d.key = key;
-          d.j = (uint32_t)j;
-          d.n = (uint32_t)n;
-          d.sub = (uint32_t)k;
-          M::template step<V, DRIFT, T>(x, t, dt, e, d);
-        }
-#pragma unroll
-        for (int w = 0; w < M::OFF_INC; ++w) Xn[(size_t)w * ld + j] = x[w];
-        if (weigh) {
-          double obs[M::N_TS];
-          M::template proj2obs<T>(x, obs);
-          double ll = 0.0;
-#pragma unroll
-          for (int ts = 0; ts < M::N_TS; ++ts) {
-            const double yy = __ldg(y + ts);
-            if (isnan(yy)) continue;
-            const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
-            const double var = M::obs_var(obs[ts], ts, t_obs, oe);
-            ll += log(plomrt::disc_normal_like(yy, mu, var, a.like_min));
-          }
-          const T l = (T)ll;
-          ws.lw[j] = l;
-          if (weight_fails(l, a.thresh)) {
-            acc.nfail += 1;
-          } else {
-            LseAcc b = {(double)l, 1.0, 1.0, 0};
-            acc = lse_merge(acc, b);
-          }
-        }
-      }
-      cur ^= 1;
-      if (!weigh) {
-        resampled = false;
-        __syncthreads();
-        continue;
-      }
-      acc = block_lse<BT>(acc, sh_lse);  // (syncs: Xn / lw visible to the block)
-      if (threadIdx.x == 0) {
-        const int all_fail = (acc.nfail == J);
-        double llike, ess;
-        if (all_fail) {
-          llike = a.log_like_min * (double)M::N_TS;
-          ess = 0.0;
-          n_all_fail += 1;
-        } else {
-          llike = acc.m + log(acc.s1 / (double)J);
-          ess = (acc.s1 * acc.s1) / acc.s2;
-        }
-        loglik += llike;
-        ess_min = fmin(ess_min, ess);
-        s_fail = all_fail;
-        s_m = acc.m;
-        s_s1 = acc.s1;
-        const double inc = 1.0 / (double)J;
-        const double U = inc * plomrt::resample_uniform(key, (uint32_t)n);
-        int ns = plomrt::systematic_table(U, inc, J, seg, plomrt::SYS_MAX_SEG);
-        if (ns < 0) {
-          atomicOr(a.error, (int)ERR_SYS_TABLE);
-          ns = 0;
-        }
-        s_ns = ns;
-      }
-      __syncthreads();
-      if (s_fail || s_ns == 0) {
-        for (int j = threadIdx.x; j < J; j += BT) ws.anc[j] = (uint32_t)j;
-      } else {
-        // cumulative normalised weights: each thread a contiguous chunk
-        const int P = (J + BT - 1) / BT;
-        const int i0 = threadIdx.x * P;
-        const int i1 = min(J, i0 + P);
-        const double m = s_m, s1 = s_s1;
-        double run = 0.0;
-        for (int i = i0; i < i1; ++i) {
-          const T l = ws.lw[i];
-          run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
-        }
-        double tot;
-        const double pre = block_exscan<BT>(run, sh_scan, &tot);
-        run = pre;
-        for (int i = i0; i < i1; ++i) {
-          const T l = ws.lw[i];
-          run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
-          ws.C[i] = run;
-        }
-        __syncthreads();
-        const int ns = s_ns;
-        for (int j = threadIdx.x; j < J; j += BT) {
-          const double ran = plomrt::systematic_point(seg, ns, j);
-          int lo = 0, hi = J - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (ran > ws.C[mid]) lo = mid + 1; else hi = mid;
-          }
-          ws.anc[j] = (uint32_t)lo;
-        }
-      }
-      resampled = true;
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      a.loglik[f] = loglik;
-      a.n_all_fail[f] = n_all_fail;
-      if (a.ess_min) a.ess_min[f] = ess_min;
-    }
+    FilterJob job;
+    job.J = fl.J;
+    job.n_obs = fl.n_obs;
+    job.seed = fl.seed;
+    job.data = a.data + (size_t)fl.data_row * M::N_TS;
+    job.par_cac = a.par_cac + (size_t)f * M::N_PAR_PROC * M::N_CAC;
+    job.par_ts = a.par_ts + (size_t)f * M::N_PAR_OBS * M::N_TS;
+    job.x0 = a.x0 + (size_t)f * M::S;
+    cta_filter<T, V, DRIFT, BT>(sh, a, job, ws, ld, a.loglik + f, a.n_all_fail + f, a.ess_min ? a.ess_min + f : nullptr);
   }
 }
 

@@ -73,7 +73,7 @@ struct ProcEnv {
 struct ObsEnv {
   const double* par_ts_;
   const double* cov_ts_;
-  __device__ __forceinline__ double par_ts(int p, int ts) const { return __ldg(par_ts_ + p * M::N_TS + ts); }
+  __device__ __forceinline__ double par_ts(int p, int ts) const { return par_ts_[p * M::N_TS + ts]; }
   __device__ __forceinline__ double cov_ts(int k, int ts) const { return __ldg(cov_ts_ + k * M::N_TS + ts); }
 };
 
@@ -172,7 +172,7 @@ struct MifObsEnv : ObsEnv {
   double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
   unsigned uni;
   __device__ __forceinline__ double par_ts(int p, int ts) const {
-    return ((uni >> p) & 1u) ? obsp[p] : __ldg(par_ts_ + p * M::N_TS + ts);
+    return ((uni >> p) & 1u) ? obsp[p] : par_ts_[p * M::N_TS + ts];
   }
 };
 

@@ -59,6 +59,17 @@ class MifDesc(C.Structure):
                 ('theta_bt', _P(BackTransform)), ('estimated', _ip)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [('max_J', C.c_int), ('memory_budget', C.c_double), ('ring_slots', C.c_int), ('plan_pool', C.c_int),
+                ('precision', C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [('pending', C.c_longlong), ('in_flight', C.c_longlong), ('completed', C.c_longlong),
+                ('launches', C.c_longlong), ('peak_in_flight', C.c_longlong), ('bytes_in_use', C.c_double),
+                ('peak_bytes', C.c_double), ('persistent_loop', C.c_int)]
+
+
 class SmcResult(C.Structure):
     _fields_ = [('loglik', C.c_double), ('n_all_fail', C.c_int), ('status', C.c_int),
                 ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp)]
@@ -70,7 +81,9 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
                'plomgpu_resample_noalloc', 'plomgpu_last_error', 'plomgpu_batch_create', 'plomgpu_batch_launch',
                'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
-               'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy']
+               'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
+               'plomgpu_server_create', 'plomgpu_server_submit', 'plomgpu_server_poll', 'plomgpu_server_wait',
+               'plomgpu_server_get_stats', 'plomgpu_server_destroy']
 
 
 def _ptr(a, t):
@@ -174,6 +187,13 @@ def _declare(lib):
     lib.plomgpu_mif_iteration.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_uint64, _dp, _ip, _dp, _dp]
     lib.plomgpu_mif_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_mif_destroy.restype = None
+    lib.plomgpu_server_create.argtypes = [_P(SmcDesc), _P(ServerOpts), _P(C.c_void_p)]
+    lib.plomgpu_server_submit.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, C.c_uint64, _P(C.c_longlong)]
+    lib.plomgpu_server_poll.argtypes = [C.c_void_p, C.c_longlong, _ip, _dp, _ip, _dp]
+    lib.plomgpu_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, _dp, _ip, _dp]
+    lib.plomgpu_server_get_stats.argtypes = [C.c_void_p, _P(ServerStats)]
+    lib.plomgpu_server_destroy.argtypes = [C.c_void_p]
+    lib.plomgpu_server_destroy.restype = None
     return lib
 
 
@@ -408,6 +428,53 @@ class MifPlan(object):
     def close(self):
         if self.p:
             self.lib.plomgpu_mif_destroy(self.p)
+            self.p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server(object):
+    """plomgpu_server_*: concurrent likelihood requests on one data set."""
+
+    def __init__(self, engine, problem, max_J, memory_budget=0.0, ring_slots=0, plan_pool=0, precision=32):
+        self.engine = engine
+        self.lib = engine.lib
+        self.h = DescHolder(problem, precision=precision)
+        self.opts = ServerOpts(int(max_J), float(memory_budget), int(ring_slots), int(plan_pool), int(precision))
+        self.p = C.c_void_p()
+        check(self.lib, self.lib.plomgpu_server_create(C.byref(self.h.desc), C.byref(self.opts), C.byref(self.p)))
+
+    def submit(self, J, par_cac=None, par_ts=None, x0=None, seed=0):
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (par_cac, par_ts, x0)]
+        t = C.c_longlong()
+        check(self.lib, self.lib.plomgpu_server_submit(self.p, int(J), *(None if a is None else a.ctypes.data_as(_dp)
+                                                                          for a in keep), C.c_uint64(seed),
+                                                       C.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        done, ll, nf, lat = C.c_int(), C.c_double(), C.c_int(), C.c_double()
+        check(self.lib, self.lib.plomgpu_server_poll(self.p, ticket, C.byref(done), C.byref(ll), C.byref(nf),
+                                                     C.byref(lat)))
+        return (ll.value, nf.value, lat.value) if done.value else None
+
+    def wait(self, ticket, timeout=60.0):
+        ll, nf, lat = C.c_double(), C.c_int(), C.c_double()
+        check(self.lib, self.lib.plomgpu_server_wait(self.p, ticket, timeout, C.byref(ll), C.byref(nf), C.byref(lat)))
+        return ll.value, nf.value, lat.value
+
+    def stats(self):
+        st = ServerStats()
+        check(self.lib, self.lib.plomgpu_server_get_stats(self.p, C.byref(st)))
+        return dict((f, getattr(st, f)) for f, _ in ServerStats._fields_)
+
+    def close(self):
+        if self.p:
+            self.lib.plomgpu_server_destroy(self.p)
             self.p = C.c_void_p()
 
     def __del__(self):
