@@ -34,6 +34,8 @@ WORKLOADS = {
     'sir_batch': ('sir', None, None, 1.0),
     # 64 iterated-filtering runs of the SEIR 20x2 model, J = 20000 each (per-iteration timing)
     'mif_seir': ('seir20x2', 20000, 520, 1.0),
+    # 32 pMCMC chains (16 SIR J=2000, 16 SEIR 20x2 J=20000), Poisson arrivals at 2000 req/s
+    'serve': (None, None, None, 1.0),
 }
 METRIC = 'particle-steps/s at matched loglik error'
 
@@ -324,8 +326,106 @@ def run_mif(args):
     return 0
 
 
+def run_serve(args, window_s=0.25, rate=2000.0):
+    """Served pMCMC likelihoods: asynchronous random-walk chains submit requests as
+    Poisson arrivals; results feed Metropolis-Hastings accept / reject."""
+    import numpy as np
+    import torch
+    from plomgpu.native import Engine, Server
+    torch.cuda.set_device(int(os.environ.get('LOCAL_RANK', '0')))
+    classes = {
+        'sir': {'lib': 'sir', 'J': 2000, 'prob': workload_problem('sir', precision=32, seed=1, J=2000)},
+        'seir': {'lib': 'seir20x2', 'J': 20000, 'prob': workload_problem('seir20x2', precision=32, seed=1, J=20000)},
+    }
+    for c in classes.values():
+        c['eng'] = Engine(c['lib'])
+        c['server'] = Server(c['eng'], c['prob'], max_J=c['J'], memory_budget=150e9 / 2, plan_pool=8, precision=32)
+    rng = np.random.Generator(np.random.Philox(12))
+    chains = []
+    for i in range(32):
+        cl = 'sir' if i < 16 else 'seir'
+        p = classes[cl]['prob']
+        chains.append({'cls': cl, 'theta': p.par_cac.copy(), 'll': -np.inf, 'accepted': 0, 'done': 0})
+    # warm up both servers (kernels, plans)
+    for c in classes.values():
+        c['server'].wait(c['server'].submit(c['J'], seed=1))
+    gaps = rng.exponential(1.0 / rate, size=int(rate * window_s * 3))
+    arrivals = np.cumsum(gaps)
+    arrivals = arrivals[arrivals < window_s]
+    owners = rng.integers(0, 32, size=len(arrivals))
+    outstanding = {}
+    lat = {'sir': [], 'seir': []}
+    t_start = time.perf_counter()
+    k = 0
+
+    def harvest(block=False):
+        for tk in list(outstanding):
+            ch, cl, th = outstanding[tk]
+            r = classes[cl]['server'].poll(tk) if not block else classes[cl]['server'].wait(tk, 600.0)
+            if r is None:
+                continue
+            ll, nf, latency = r
+            lat[cl].append(latency)
+            c = chains[ch]
+            c['done'] += 1
+            if np.log(rng.uniform()) < ll - c['ll']:
+                c['theta'], c['ll'] = th, ll
+                c['accepted'] += 1
+            del outstanding[tk]
+
+    with Clocks(int(os.environ.get('LOCAL_RANK', '0'))) as clk:
+        while k < len(arrivals):
+            now = time.perf_counter() - t_start
+            if now >= arrivals[k]:
+                ch = int(owners[k])
+                c = chains[ch]
+                th = c['theta'] * np.exp(0.02 * rng.standard_normal(c['theta'].shape))
+                sv = classes[c['cls']]['server']
+                tk = sv.submit(classes[c['cls']]['J'], par_cac=th, seed=int(1 + k))
+                outstanding[tk if c['cls'] == 'sir' else tk] = (ch, c['cls'], th)
+                k += 1
+            else:
+                harvest()
+                time.sleep(min(2e-4, max(0.0, arrivals[k] - now)))
+        harvest(block=True)
+    t_total = time.perf_counter() - t_start
+    stats = dict((cl, c['server'].stats()) for cl, c in classes.items())
+    n_req = sum(len(v) for v in lat.values())
+    psteps = sum(len(lat[cl]) * classes[cl]['J'] * classes[cl]['prob'].n_obs for cl in lat)
+    # plain filter per request: one-shot plomgpu_smc_run, sequential, on a sample
+    plain = {}
+    for cl, c in classes.items():
+        ts = []
+        for i in range(3 if cl == 'sir' else 2):
+            p = c['prob']
+            t0 = time.perf_counter()
+            c['eng'].smc(p)
+            ts.append(time.perf_counter() - t0)
+        plain[cl] = statistics.median(ts)
+    plain_time = sum(len(lat[cl]) * plain[cl] for cl in lat)
+    for c in classes.values():
+        c['server'].close()
+    pct = lambda v, q: float(np.percentile(v, q)) if v else None
+    line = {'metric': METRIC, 'value': psteps / t_total, 'unit': 'particle-steps/s', 'n_gpus': 1, 'steps': 1,
+            'warmup': 1, 'ms_per_step': 1000.0 * t_total, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
+            'config': {'workload': 'serve', 'chains': {'sir_J2000_T52': 16, 'seir20x2_J20000_T520': 16},
+                       'arrival_rate_per_s': rate, 'arrival_window_s': window_s, 'requests': n_req,
+                       'memory_budget_GB': 150},
+            'requests_per_s': n_req / t_total,
+            'latency_s': dict((cl, {'p50': pct(lat[cl], 50), 'p99': pct(lat[cl], 99), 'n': len(lat[cl])}) for cl in lat),
+            'plain_filter_per_request': {'latency_s': plain, 'total_s_for_same_requests': plain_time,
+                                         'speedup_of_serving': plain_time / t_total},
+            'server_stats': stats, 'acceptance': [c['accepted'] / max(c['done'], 1) for c in chains],
+            'clocks': clk.summary()}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse()
+    if args.workload == 'serve':
+        return run_serve(args)
     if args.impl == 'reference':
         return run_reference(args)
     if args.workload == 'sir_batch':

@@ -50,6 +50,7 @@ typedef struct plomgpu_model_info {
     int coupled;          /* 1 if the model reads a cac x cac coupling matrix */
     int pop_size_eq_sum_sv;
     const char *name;
+    int n_hat;            /* rows of the filtered summaries: n_par_sv*n_cac [+ n_cac remainders] + n_ts + n_drift*n_cac */
 } plomgpu_model_info;
 
 /* Back-transform of one group of a drifted parameter (back_transform_x,
@@ -98,6 +99,14 @@ typedef struct plomgpu_smc_desc {
      * resampling offset U = u/J of interval n. */
     const double *crn_normals;
     const double *crn_uniforms;
+    /* Inputs of the filtered summaries, read only when result.hat or
+     * result.pred_res is requested:
+     * [n_obs + 1][n_cac] population size N at 0 and at every t_obs, for the
+     * remainder rows (models with a remainder compartment);
+     * [n_cov_ts][n_ts] observation covariates at time 0 (models with
+     * observation covariates). */
+    const double *pop_size;
+    const double *cov_ts0;
 } plomgpu_smc_desc;
 
 typedef struct plomgpu_smc_result {
@@ -109,6 +118,19 @@ typedef struct plomgpu_smc_result {
     uint32_t *ancestors;      /* [n_obs][J] optional: select[n][j] (identity when not resampled) */
     double *x_pred;           /* [n_obs][n_state][J] optional: propagated particles before resampling */
     double *x_final;          /* [n_state][J] optional: particles after the last interval (resampled) */
+    /* [n_obs + 1][n_hat][3] optional: filtered summaries at time 0 and after
+     * every interval (compute_hat / compute_hat_nn, model_builder/C/core/hat.c:68-260):
+     * for every compartment state, remainder, series observation mean and
+     * drifted parameter (natural scale, f_inv of the state word; word
+     * i*n_cac + g for drift i, group g): the weighted 2.5 % quantile, mean,
+     * 97.5 % quantile.  Weights are the interval's normalised weights where it
+     * was weighted, 1/J elsewhere.  Requires a single run. */
+    double *hat;
+    /* [n_obs][n_ts][2] optional: prediction mean and standardised residual per
+     * series over the resampled particles (print_prediction_residuals,
+     * model_builder/C/core/print.c:632-711); written for intervals that were
+     * weighted */
+    double *pred_res;
 } plomgpu_smc_result;
 
 /* Model dimensions of this library. */

@@ -120,7 +120,28 @@ struct plomgpu_plan {
   int* proc_slot = nullptr;
   int* obs_slot = nullptr;
   std::vector<FilterAcc> acc_runs_h;
+  // filtered summaries
+  bool want_hat = false;
+  double* vals = nullptr;      // [kHatVals][J]
+  double* hat = nullptr;       // [n_obs][kHatQ][3]
+  double* pred = nullptr;      // [n_obs][N_TS][2]
+  double* pop = nullptr;       // [n_obs + 1][N_CAC]
+  double* cov_ts0 = nullptr;   // [N_COV_TS][N_TS] at time 0
+  double hat_rank[2] = {1.0, 1.0};  // quantile ranks under equal weights
 };
+
+// Rank (1-based) at which a running sum of 1/J, accumulated as the reference
+// does (get_CI95, model_builder/C/core/hat.c:40-55), first reaches `level`.
+int equal_weight_rank(int J, double level) {
+  const double invJ = 1.0 / (double)J;
+  double cum = 0.0;
+  int k = 0;
+  while (cum < level && k < J) {
+    cum += invJ;
+    ++k;
+  }
+  return k < 1 ? 1 : k;
+}
 
 namespace {
 
@@ -188,6 +209,21 @@ PropKernel<T> pick_prop(int noises_off, bool crn, bool mif) {
   return pick_v<T, false, false>(v, d);
 }
 
+// Filtered summaries of the particles in X (row `row` of the summary table:
+// 0 = time 0, n + 1 = after interval n), weighted by the normalised weights of
+// the interval when `weighted`, by 1/J otherwise.
+template <class T>
+int enqueue_hat(plomgpu_plan* p, const T* X, int row, const double* cov_ts, double t, bool weighted, cudaStream_t s) {
+  const int J = p->J;
+  const double* pop = p->pop ? p->pop + (size_t)row * M::N_CAC : nullptr;
+  const int g = (J + 255) / 256 < 4096 ? (J + 255) / 256 : 4096;
+  k_hat_values<T><<<g, 256, 0, s>>>(X, J, pop, p->par_ts, cov_ts, t, p->drift_bt, (const T*)p->lw, p->st,
+                                    weighted ? 1 : 0, p->thresh, p->vals);
+  k_hat_stats<T, 256><<<kHatQ, 256, 0, s>>>(p->vals, J, p->st, weighted ? 1 : 0, p->hat_rank[0], p->hat_rank[1],
+                                            p->hat + (size_t)row * kHatQ * 3);
+  return 2;
+}
+
 template <class T>
 int enqueue_filter(plomgpu_plan* p) {
   cudaStream_t s = p->stream;
@@ -235,6 +271,8 @@ int enqueue_filter(plomgpu_plan* p) {
     k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, (int)RJ, (T*)p->X[0]);
     ++kernels;
   }
+  // summaries of the initial particles (time 0, incidences reset, equal weights)
+  if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)p->X[0], 0, p->cov_ts0, 0.0, false, s);
   int th_cur = 0;
   if (p->mif) {
     const int g = (int)((RJ + 255) / 256 < 4096 ? (RJ + 255) / 256 : 4096);
@@ -263,7 +301,7 @@ int enqueue_filter(plomgpu_plan* p) {
     a.crn = p->crn ? p->crn_tab + crn_off : nullptr;
     a.crn_d = D;
     a.x_hist = p->x_hist ? p->x_hist + (size_t)n * M::S * RJ : nullptr;
-    a.write_inc = (p->x_final != nullptr && n == p->n_obs - 1) ? 1 : 0;
+    a.write_inc = ((p->x_final != nullptr && n == p->n_obs - 1) || p->want_hat) ? 1 : 0;
     a.theta_prev = p->mif ? p->theta[th_cur] : nullptr;
     a.theta_next = p->mif ? p->theta[th_cur ^ 1] : nullptr;
     // the random walk applies where the previous interval resampled (C/mif/mif.c:190-191)
@@ -287,17 +325,23 @@ int enqueue_filter(plomgpu_plan* p) {
                                                             p->n_obs, p->bart, p->vt);
         ++kernels;
       }
+      if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
       k_scan<T, kBtScan, kIptScan><<<dim3(p->ntiles, R), kBtScan, 0, s>>>((const T*)p->lw, J, p->thresh, p->st,
                                                                          p->tstat, p->acc, p->C);
       k_search<kBtSearch><<<dim3((J + kBtSearch - 1) / kBtSearch, R), kBtSearch, 0, s>>>(
           p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
       kernels += 3;
+      if (p->want_hat) {
+        k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
+        ++kernels;
+      }
       anc_cur = nxt;
     } else {
       if (p->anc_hist) {
         k_identity<<<(J + 255) / 256, 256, 0, s>>>(p->anc_hist + (size_t)n * J, J);
         ++kernels;
       }
+      if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, false, s);
       anc_cur = -1;
     }
   }
@@ -437,6 +481,25 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   }
   if (p->want_anc) CK(cudaMalloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
   if (p->want_xpred) CK(cudaMalloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
+  if (p->want_hat) {
+    if (p->R != 1) return fail(PLOMGPU_EINVAL, "filtered summaries need a single run");
+    if (!M::POP_SIZE_EQ_SUM_SV && !d->pop_size) return fail(PLOMGPU_EINVAL, "summaries of a remainder need pop_size");
+    CK(cudaMalloc((void**)&p->vals, (size_t)kHatVals * J * sizeof(double)));
+    p->hat_rank[0] = (double)equal_weight_rank(J, 0.025);
+    p->hat_rank[1] = (double)equal_weight_rank(J, 0.975);
+    CK(cudaMalloc((void**)&p->hat, (size_t)(d->n_obs + 1) * kHatQ * 3 * sizeof(double)));
+    CK(cudaMalloc((void**)&p->pred, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS * 2 * sizeof(double)));
+    CK(cudaMemsetAsync(p->pred, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS * 2 * sizeof(double), s));
+    if (d->pop_size) {
+      int rc2 = upload<double>(d->pop_size, (size_t)(d->n_obs + 1) * M::N_CAC, &p->pop, s);
+      if (rc2) return rc2;
+    }
+    if (M::N_COV_TS > 0) {
+      if (!d->cov_ts0) return fail(PLOMGPU_EINVAL, "summaries of observations with covariates need cov_ts0");
+      int rc3 = upload<double>(d->cov_ts0, (size_t)M::N_COV_TS * M::N_TS, &p->cov_ts0, s);
+      if (rc3) return rc3;
+    }
+  }
   if (p->timing) {
     p->ev.assign(2 * (size_t)d->n_obs, nullptr);
     for (auto& e : p->ev) CK(cudaEventCreate(&e));
@@ -468,7 +531,7 @@ void plan_free(plomgpu_plan* p) {
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
-                  p->obs_slot};
+                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (p->acc_h) cudaFreeHost(p->acc_h);
@@ -479,7 +542,7 @@ void plan_free(plomgpu_plan* p) {
 }
 
 int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bool want_xpred, bool want_final,
-                bool timing = false, const plomgpu_mif_desc* mif = nullptr) {
+                bool timing = false, const plomgpu_mif_desc* mif = nullptr, bool want_hat = false) {
   *out = nullptr;
   int rc = check_desc(d);
   if (rc) return rc;
@@ -495,6 +558,7 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->want_anc = want_anc;
   p->want_xpred = want_xpred;
   p->timing = timing;
+  p->want_hat = want_hat;
   if (mif) {
     p->R = mif->n_runs;
     p->mif = true;
@@ -572,6 +636,12 @@ int plan_results(plomgpu_plan* p, plomgpu_smc_result* r) {
   if (r->x_final && p->x_final)
     CK(cudaMemcpyAsync(r->x_final, p->x_final, (size_t)M::S * p->J * sizeof(double), cudaMemcpyDeviceToHost,
                        p->stream));
+  if (r->hat && p->hat)
+    CK(cudaMemcpyAsync(r->hat, p->hat, (size_t)(p->n_obs + 1) * kHatQ * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                       p->stream));
+  if (r->pred_res && p->pred && p->n_obs > 0)
+    CK(cudaMemcpyAsync(r->pred_res, p->pred, (size_t)p->n_obs * M::N_TS * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                       p->stream));
   CK(cudaStreamSynchronize(p->stream));
   r->loglik = p->acc_h->loglik;
   r->n_all_fail = p->acc_h->n_all_fail;
@@ -611,6 +681,7 @@ int plomgpu_get_model_info(plomgpu_model_info* o) {
   o->coupled = M::COUPLED ? 1 : 0;
   o->pop_size_eq_sum_sv = M::POP_SIZE_EQ_SUM_SV ? 1 : 0;
   o->name = M::NAME;
+  o->n_hat = kHatQ;
   return PLOMGPU_OK;
 }
 
@@ -679,7 +750,8 @@ void plomgpu_plan_destroy(plomgpu_plan* p) { plan_free(p); }
 int plomgpu_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r) {
   if (!r) return fail(PLOMGPU_EINVAL, "null result");
   plomgpu_plan* p = nullptr;
-  int rc = plan_create(d, &p, r->ancestors != nullptr, r->x_pred != nullptr, r->x_final != nullptr);
+  int rc = plan_create(d, &p, r->ancestors != nullptr, r->x_pred != nullptr, r->x_final != nullptr, false, nullptr,
+                       r->hat != nullptr || r->pred_res != nullptr);
   if (rc) {
     r->status = rc;
     return rc;

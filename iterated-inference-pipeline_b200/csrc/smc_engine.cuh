@@ -750,6 +750,220 @@ __global__ void __launch_bounds__(BT) k_mif_moments(const T* __restrict__ lw, co
   }
 }
 
+// ------------------------------------------------------------------ filtered summaries
+// Quantities summarised per interval (compute_hat, model_builder/C/core/hat.c:68-176):
+// state words of the compartments, remainders N(t) - sum of states (when the
+// model has a remainder), observation means per series, drifted parameters
+// mapped to the natural scale by f_inv; the observation variances per series
+// follow them for the prediction residuals (print_prediction_residuals,
+// print.c:632-711).
+constexpr int kHatSv = M::N_PAR_SV * M::N_CAC;
+constexpr int kHatRem = M::POP_SIZE_EQ_SUM_SV ? 0 : M::N_CAC;
+constexpr int kHatObs = M::N_TS;
+constexpr int kHatDrift = M::N_DRIFT * M::N_CAC;
+constexpr int kHatQ = kHatSv + kHatRem + kHatObs + kHatDrift;  // summarised quantities
+constexpr int kHatW = kHatQ + M::N_TS;                         // column of the particle weights
+constexpr int kHatVals = kHatW + 1;                            // + observation variances, + weights
+
+// Read-only view of particle j's state words straight from the SoA array.
+template <class T>
+struct ColumnView {
+  const T* p;
+  size_t ld;
+  __device__ __forceinline__ double operator[](int w) const { return (double)p[(size_t)w * ld]; }
+};
+
+// Values of every summarised quantity per particle (column-major [kHatVals][J])
+// and the particle's weight: its normalised weight when the interval was
+// weighted and not all particles failed, else 1 (a count; the quantile ranks
+// of equal weights are then integers).
+template <class T>
+__global__ void k_hat_values(const T* __restrict__ X, int J, const double* __restrict__ pop_size,
+                             const double* __restrict__ par_ts, const double* __restrict__ cov_ts, double t_obs,
+                             const plomrt::BackTransform* __restrict__ drift_bt, const T* __restrict__ lw,
+                             const StepState* st, int weighted, double thresh, double* __restrict__ vals) {
+  const bool uni = !weighted || st->all_fail;
+  const double m = uni ? 0.0 : st->m, s1 = uni ? 1.0 : st->s1;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J; j += gridDim.x * blockDim.x) {
+    const ColumnView<T> x{X + j, (size_t)J};
+    int q = 0;
+    for (int i = 0; i < kHatSv; ++i) vals[(size_t)(q++) * J + j] = x[i];
+    for (int c = 0; c < kHatRem; ++c) {
+      double sv = 0.0;
+      for (int i = 0; i < M::N_PAR_SV; ++i) sv += x[i * M::N_CAC + c];
+      vals[(size_t)(q++) * J + j] = pop_size[c] - sv;
+    }
+    double obs[M::N_TS];
+    M::template proj2obs<double>(x, obs);
+    ObsEnv oe;
+    oe.par_ts_ = par_ts;
+    oe.cov_ts_ = cov_ts;
+    for (int ts = 0; ts < M::N_TS; ++ts) vals[(size_t)(q++) * J + j] = M::obs_mean(obs[ts], ts, t_obs, oe);
+    for (int i = 0; i < kHatDrift; ++i) {
+      double v = x[M::OFF_DRIFT + i];
+      if (drift_bt) {
+        plomrt::BackTransform b = drift_bt[i];
+        b.scale = 0;
+        b.multiplier = 1.0;
+        b.is_duration = 0;
+        v = plomrt::back_transform<double>(v, b);
+      }
+      vals[(size_t)(q++) * J + j] = v;
+    }
+    for (int ts = 0; ts < M::N_TS; ++ts) vals[(size_t)(q++) * J + j] = M::obs_var(obs[ts], ts, t_obs, oe);
+    double w = 1.0;
+    if (!uni) {
+      const T l = lw[j];
+      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+    }
+    vals[(size_t)kHatW * J + j] = w;
+  }
+}
+
+__device__ __forceinline__ uint64_t order_key(double v) {
+  const uint64_t b = (uint64_t)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double key_value(uint64_t k) {
+  const uint64_t b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+template <int BT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < BT / 32; ++w) t += sh[w];
+  __syncthreads();
+  return t;
+}
+
+// Weighted mean and 2.5 % / 97.5 % quantiles of every quantity (block per
+// quantity).  The quantile is the smallest value whose cumulative weight in
+// value order reaches the target (get_CI95, hat.c:28-57): found by a radix
+// select over the order-preserving 64-bit keys of the values, 8 bits per pass,
+// both quantiles in the same passes.  Targets: the levels for normalised
+// weights; for equal weights the ranks rank_lo / rank_hi at which the
+// reference's running sum of 1/J first reaches the levels (computed once on
+// the host), compared against exact integer counts.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT) k_hat_stats(const double* __restrict__ vals, int J, const StepState* st,
+                                                  int weighted, double rank_lo, double rank_hi,
+                                                  double* __restrict__ hat) {
+  __shared__ double sh[BT / 32];
+  __shared__ double hist[2][256];
+  __shared__ uint64_t s_prefix[2];
+  __shared__ double s_below[2];
+  const int q = blockIdx.x;
+  const double* v = vals + (size_t)q * J;
+  const double* w = vals + (size_t)kHatW * J;
+  const bool uni = !weighted || st->all_fail;
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < J; j += BT) acc += w[j] * v[j];
+  double mean = block_sum<BT>(acc, sh);
+  if (uni) mean /= (double)J;
+  const double target[2] = {uni ? rank_lo : 0.025, uni ? rank_hi : 0.975};
+  if (threadIdx.x < 2) {
+    s_prefix[threadIdx.x] = 0ull;
+    s_below[threadIdx.x] = 0.0;
+  }
+  for (int shift = 56; shift >= 0; shift -= 8) {
+    for (int i = threadIdx.x; i < 512; i += BT) (&hist[0][0])[i] = 0.0;
+    __syncthreads();
+    const uint64_t hi_mask = (shift == 56) ? 0ull : (~0ull << (shift + 8));
+    const uint64_t p0 = s_prefix[0] & hi_mask, p1 = s_prefix[1] & hi_mask;
+    for (int j0 = 0; j0 < J; j0 += BT) {
+      const int j = j0 + threadIdx.x;
+      const bool in = j < J;
+      const uint64_t key = in ? order_key(v[j]) : 0ull;
+      const double wj = in ? w[j] : 0.0;
+      const int bin = (int)((key >> shift) & 255u);
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const bool match = in && ((key & hi_mask) == (k ? p1 : p0));
+        // warp-aggregate when every lane hits the same bin (the common case
+        // in the high passes, where the values share sign and exponent)
+        const unsigned ballot = __ballot_sync(0xffffffffu, match);
+        const int b0 = __shfl_sync(0xffffffffu, bin, 0);
+        const bool same = (ballot == 0xffffffffu) && __all_sync(0xffffffffu, bin == b0);
+        if (same) {
+          double t = wj;
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+          if ((threadIdx.x & 31) == 0) atomicAdd(&hist[k][b0], t);
+        } else if (match) {
+          atomicAdd(&hist[k][bin], wj);
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int k = threadIdx.x;
+      double cum = s_below[k];
+      int d = -1, last = -1;
+      double cum_last = cum;
+      for (int b = 0; b < 256; ++b) {
+        const double h = hist[k][b];
+        if (h == 0.0) continue;
+        if (cum + h >= target[k]) {
+          d = b;
+          break;
+        }
+        last = b;
+        cum_last = cum;
+        cum += h;
+      }
+      if (d < 0) {  // rounding left the total below the target: the largest value
+        d = last >= 0 ? last : 0;
+        cum = cum_last;
+      }
+      s_prefix[k] |= (uint64_t)d << shift;
+      s_below[k] = cum;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    hat[(size_t)q * 3 + 0] = key_value(s_prefix[0]);
+    hat[(size_t)q * 3 + 1] = mean;
+    hat[(size_t)q * 3 + 2] = key_value(s_prefix[1]);
+  }
+}
+
+// Prediction residuals of every series over the resampled particles: mean and
+// variance of the observation means, mean of the observation variances
+// (print_prediction_residuals, print.c:632-711).  Block per series.
+template <int BT>
+__global__ void __launch_bounds__(BT) k_pred_res(const double* __restrict__ vals, const uint32_t* __restrict__ anc,
+                                                 int J, const double* __restrict__ y, double* __restrict__ out) {
+  __shared__ double sh[BT / 32];
+  const int ts = blockIdx.x;
+  const double* om = vals + (size_t)(kHatSv + kHatRem + ts) * J;
+  const double* ov = vals + (size_t)(kHatQ + ts) * J;
+  double a = 0.0, b = 0.0;
+  for (int j = threadIdx.x; j < J; j += BT) {
+    const uint32_t s = anc ? anc[j] : (uint32_t)j;
+    a += om[s];
+    b += ov[s];
+  }
+  const double pred = block_sum<BT>(a, sh) / (double)J;
+  const double var_obs = block_sum<BT>(b, sh) / (double)J;
+  double m2 = 0.0;
+  for (int j = threadIdx.x; j < J; j += BT) {
+    const uint32_t s = anc ? anc[j] : (uint32_t)j;
+    const double d = om[s] - pred;
+    m2 += d * d;
+  }
+  const double M2 = block_sum<BT>(m2, sh);
+  if (threadIdx.x == 0) {
+    const double var_state = M2 / ((double)J - 1.0);
+    out[ts * 2 + 0] = pred;
+    out[ts * 2 + 1] = (y[ts] - pred) / sqrt(var_state + var_obs);
+  }
+}
+
 __global__ void k_sys_points(double U, int J, double* out, int* err) {
   __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
   __shared__ int s_ns;

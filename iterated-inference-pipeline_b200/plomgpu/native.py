@@ -22,7 +22,7 @@ class ModelInfo(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         'n_par_sv', 'n_c', 'n_ac', 'n_cac', 'n_ts', 'n_ts_inc_unique', 'n_obs_inc', 'n_obs_prev',
         'n_drift', 'off_drift', 'off_inc', 'n_state', 'n_par_proc', 'n_par_obs', 'n_cov_cac', 'n_cov_ts',
-        'n_reac', 'n_white_noise', 'coupled', 'pop_size_eq_sum_sv')] + [('name', C.c_char_p)]
+        'n_reac', 'n_white_noise', 'coupled', 'pop_size_eq_sum_sv')] + [('name', C.c_char_p), ('n_hat', C.c_int)]
 
 
 class BackTransform(C.Structure):
@@ -42,7 +42,7 @@ class SmcDesc(C.Structure):
                 ('cov_ts', _dp), ('coupling', _dp), ('drift_group', _ip), ('drift_ngroups', _ip),
                 ('drift_bt', _P(BackTransform)), ('drift_vol', _dp), ('x0', _dp), ('noises_off', C.c_int),
                 ('filter', C.c_int), ('like_min', C.c_double), ('seed', C.c_uint64), ('precision', C.c_int),
-                ('crn_normals', _dp), ('crn_uniforms', _dp)]
+                ('crn_normals', _dp), ('crn_uniforms', _dp), ('pop_size', _dp), ('cov_ts0', _dp)]
 
 
 class BatchDesc(C.Structure):
@@ -72,7 +72,8 @@ class ServerStats(C.Structure):
 
 class SmcResult(C.Structure):
     _fields_ = [('loglik', C.c_double), ('n_all_fail', C.c_int), ('status', C.c_int),
-                ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp)]
+                ('llike_n', _dp), ('ess_n', _dp), ('ancestors', _up), ('x_pred', _dp), ('x_final', _dp),
+                ('hat', _dp), ('pred_res', _dp)]
 
 
 API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_smc_run', 'plomgpu_plan_create',
@@ -126,6 +127,10 @@ class DescHolder(object):
         x0 = keep('x0', p.x0, np.float64)
         crn = keep('crn', crn_normals, np.float64) if crn_normals is not None else None
         crnu = keep('crnu', crn_uniforms, np.float64) if crn_uniforms is not None else None
+        pop = keep('pop_size', getattr(p, 'pop_size', None), np.float64) if getattr(p, 'pop_size', None) is not None \
+            else None
+        cts0 = getattr(p, 'cov_ts0', None)
+        cts0 = keep('cov_ts0', cts0 if cts0 is not None and cts0.size else np.zeros(1), np.float64)
         self.desc = SmcDesc(
             J=p.J, n_obs=p.n_obs, n_sub=_ptr(n_sub, _ip), t_sub=_ptr(t_sub, _dp), t_obs=_ptr(t_obs, _dp),
             dt=p.dt, data=_ptr(data, _dp), par_cac=_ptr(par_cac, _dp), par_ts=_ptr(par_ts, _dp),
@@ -133,18 +138,22 @@ class DescHolder(object):
             drift_group=_ptr(dg, _ip), drift_ngroups=_ptr(dng, _ip), drift_bt=C.cast(bts, _P(BackTransform)),
             drift_vol=_ptr(dvol, _dp), x0=_ptr(x0, _dp), noises_off=p.noises_off, filter=1 if p.filter else 0,
             like_min=p.like_min, seed=p.seed, precision=precision or p.precision,
-            crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp))
+            crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp), pop_size=_ptr(pop, _dp),
+            cov_ts0=_ptr(cts0, _dp))
 
 
 class Outputs(object):
-    def __init__(self, J, n_obs, S, ancestors=False, x_pred=False, x_final=False):
+    def __init__(self, J, n_obs, S, ancestors=False, x_pred=False, x_final=False, n_hat=0, n_ts=0):
         self.llike_n = np.zeros(max(n_obs, 1))
         self.ess_n = np.zeros(max(n_obs, 1))
         self.ancestors = np.zeros((n_obs, J), dtype=np.uint32) if ancestors else None
         self.x_pred = np.zeros((n_obs, S, J)) if x_pred else None
         self.x_final = np.zeros((S, J)) if x_final else None
+        self.hat = np.zeros((n_obs + 1, n_hat, 3)) if n_hat else None
+        self.pred_res = np.zeros((max(n_obs, 1), n_ts, 2)) if n_hat else None
         self.res = SmcResult(0.0, 0, 0, _ptr(self.llike_n, _dp), _ptr(self.ess_n, _dp),
-                             _ptr(self.ancestors, _up), _ptr(self.x_pred, _dp), _ptr(self.x_final, _dp))
+                             _ptr(self.ancestors, _up), _ptr(self.x_pred, _dp), _ptr(self.x_final, _dp),
+                             _ptr(self.hat, _dp), _ptr(self.pred_res, _dp))
 
     @property
     def loglik(self):
@@ -231,9 +240,12 @@ class Engine(object):
         self.info = model_info(self.lib)
 
     def smc(self, problem, crn_normals=None, crn_uniforms=None, ancestors=False, x_pred=False, x_final=False,
-            precision=None):
+            precision=None, hat=False):
+        """One filter.  ``hat`` adds the filtered summaries (out.hat, [n_obs+1][n_hat][low, mean, high])
+        and the prediction residuals (out.pred_res, [n_obs][n_ts][pred, res])."""
         h = DescHolder(problem, crn_normals, crn_uniforms, precision)
-        out = Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final)
+        out = Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final,
+                      self.info.n_hat if hat else 0, self.info.n_ts)
         check(self.lib, self.lib.plomgpu_smc_run(C.byref(h.desc), C.byref(out.res)))
         return out
 

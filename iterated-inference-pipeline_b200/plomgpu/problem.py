@@ -138,11 +138,18 @@ class Problem(object):
             for t in range(m.N_TS):
                 sp = self.splines_ts[k][t]
                 self.cov_ts[:, k, t] = [sp(x) for x in t_obs]
+        # observation covariates at t = 0, for the summaries of the initial particles
+        self.cov_ts0 = np.array([[self.splines_ts[k][t](0.0) for t in range(m.N_TS)]
+                                 for k in range(len(em_cov_ts))]).reshape(len(em_cov_ts), m.N_TS)
         if 'N' in em_cov_cac:
             kN = em_cov_cac.index('N')
             self.pop_size_t0 = np.array([self.splines_cac[kN][c](0.0) for c in range(m.N_CAC)])
+            # N at 0 and at every observation time (remainder rows of the summaries)
+            self.pop_size = np.array([[self.splines_cac[kN][c](t) for c in range(m.N_CAC)]
+                                      for t in [0.0] + list(t_obs)])
         else:
             self.pop_size_t0 = np.ones(m.N_CAC)
+            self.pop_size = None
         self.coupling = (np.array(data['coupling'], dtype=float) if 'coupling' in data else
                          (np.array(m.coupling, dtype=float) if m.coupling is not None else None))
         self.set_theta(theta, u_data)

@@ -42,18 +42,22 @@ class Oracle(object):
                                                  C.POINTER(C.c_uint32)]
         L.oracle_mif_iteration.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.MifDesc), _dp, _dp, _dp, _dp,
                                            _dp, C.POINTER(C.c_int), _dp, _dp]
+        L.oracle_ci95.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
+        L.oracle_ci95.restype = None
         L.oracle_proj2obs.argtypes = [_dp, _dp]
         L.oracle_proj2obs.restype = None
         self.info = native.ModelInfo()
         L.oracle_model_info(C.byref(self.info))
+        self.n_hat = self.info.n_hat
 
     def draws_per_substep(self, noises_off):
         return self.lib.oracle_draws_per_substep(noises_off)
 
     def smc(self, problem, crn_normals=None, crn_uniforms=None, ancestors=False, x_pred=False, x_final=False,
-            n_threads=0):
+            n_threads=0, hat=False):
         h = native.DescHolder(problem, crn_normals, crn_uniforms, precision=64)
-        out = native.Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final)
+        out = native.Outputs(problem.J, problem.n_obs, self.info.n_state, ancestors, x_pred, x_final,
+                             self.n_hat if hat else 0, self.info.n_ts)
         rc = self.lib.oracle_smc_run(C.byref(h.desc), C.byref(out.res), n_threads)
         if rc:
             raise RuntimeError('oracle failed: %d' % rc)
@@ -122,3 +126,12 @@ class Oracle(object):
         obs = np.zeros(self.info.n_ts)
         self.lib.oracle_proj2obs(x.ctypes.data_as(_dp), obs.ctypes.data_as(_dp))
         return obs
+
+    def ci95(self, values, weights=None):
+        """get_CI95: (low, high) of values under weights (None: 1/J)."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+        lo, hi = C.c_double(), C.c_double()
+        self.lib.oracle_ci95(v.ctypes.data_as(_dp), None if w is None else w.ctypes.data_as(_dp), len(v),
+                             C.byref(lo), C.byref(hi))
+        return lo.value, hi.value

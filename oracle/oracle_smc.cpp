@@ -29,6 +29,7 @@
 #include PLOM_MODEL_HEADER
 #include "plomgpu.h"
 
+#include <algorithm>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -238,6 +239,119 @@ void systematic_sampling(const std::vector<double>& prob, int J, double U, uint3
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Filtered summaries.  get_CI95 (model_builder/C/core/hat.c:28-57): sort the
+// values, accumulate the weights in sorted order until they reach 2.5 % /
+// 97.5 %, take the value where the sum crossed.  compute_hat / compute_hat_nn
+// (hat.c:68-260): weighted (or 1/J) mean and interval of every state word,
+// remainder N(t) - sum of states, observation mean per series, and drifted
+// parameter mapped by f_inv.
+namespace {
+
+constexpr int kNHat = M::N_PAR_SV * M::N_CAC + (M::POP_SIZE_EQ_SUM_SV ? 0 : M::N_CAC) + M::N_TS +
+                      M::N_DRIFT * M::N_CAC;
+
+void ci95(const std::vector<double>& v, const double* w, int J, double* lo, double* hi) {
+  std::vector<int> idx(J);
+  for (int j = 0; j < J; ++j) idx[j] = j;
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return v[a] < v[b]; });
+  const double invJ = 1.0 / (double)J;
+  const double level[2] = {0.025, 0.975};
+  double* out[2] = {lo, hi};
+  for (int q = 0; q < 2; ++q) {
+    int k = 0;
+    double cum = 0.0;
+    while (cum < level[q] && k < J) {
+      cum += w ? w[idx[k]] : invJ;
+      ++k;
+    }
+    *out[q] = v[idx[(k - 1) < 0 ? 0 : k - 1]];
+  }
+}
+
+// X: AoS particles [J][S]; w: normalised weights or null (1/J); hat: [kNHat][3]
+void compute_hat(const std::vector<double>& X, int J, const double* w, const plomgpu_smc_desc* d,
+                 const double* cov_ts, const double* pop, double t, double* hat) {
+  const int S = M::S;
+  std::vector<double> v(J);
+  int q = 0;
+  auto summarise = [&]() {
+    double mean = 0.0;
+    for (int j = 0; j < J; ++j) mean += v[j] * (w ? w[j] : 1.0);
+    if (!w) mean /= (double)J;
+    ci95(v, w, J, &hat[q * 3 + 0], &hat[q * 3 + 2]);
+    hat[q * 3 + 1] = mean;
+    ++q;
+  };
+  for (int i = 0; i < M::N_PAR_SV * M::N_CAC; ++i) {
+    for (int j = 0; j < J; ++j) v[j] = X[(size_t)j * S + i];
+    summarise();
+  }
+  if (!M::POP_SIZE_EQ_SUM_SV) {
+    for (int c = 0; c < M::N_CAC; ++c) {
+      for (int j = 0; j < J; ++j) {
+        double sv = 0.0;
+        for (int i = 0; i < M::N_PAR_SV; ++i) sv += X[(size_t)j * S + i * M::N_CAC + c];
+        v[j] = pop[c] - sv;
+      }
+      summarise();
+    }
+  }
+  HostObsEnv oe;
+  oe.par_ts_ = d->par_ts;
+  oe.cov_ts_ = cov_ts;
+  for (int ts = 0; ts < M::N_TS; ++ts) {
+    for (int j = 0; j < J; ++j) {
+      HostState xs;
+      xs.b = const_cast<double*>(&X[(size_t)j * S]);
+      double obs[M::N_TS];
+      M::proj2obs<double>(xs, obs);
+      v[j] = M::obs_mean(obs[ts], ts, t, oe);
+    }
+    summarise();
+  }
+  for (int i = 0; i < M::N_DRIFT * M::N_CAC; ++i) {
+    plomrt::BackTransform b;
+    memcpy(&b, &d->drift_bt[i], sizeof(b));
+    b.scale = 0;
+    b.multiplier = 1.0;
+    b.is_duration = 0;
+    for (int j = 0; j < J; ++j) v[j] = plomrt::back_transform<double>(X[(size_t)j * S + M::OFF_DRIFT + i], b);
+    summarise();
+  }
+}
+
+// print_prediction_residuals (model_builder/C/core/print.c:632-711) on the
+// resampled particles: running mean / M2 of the observation means, mean of
+// the observation variances.  out: [N_TS][2] = pred, res.
+void pred_res(const std::vector<double>& X, int J, const plomgpu_smc_desc* d, const double* cov_ts, double t,
+              const double* y, double* out) {
+  HostObsEnv oe;
+  oe.par_ts_ = d->par_ts;
+  oe.cov_ts_ = cov_ts;
+  for (int ts = 0; ts < M::N_TS; ++ts) {
+    double kn = 0.0, pred = 0.0, var_obs = 0.0, M2 = 0.0;
+    for (int j = 0; j < J; ++j) {
+      HostState xs;
+      xs.b = const_cast<double*>(&X[(size_t)j * M::S]);
+      double obs[M::N_TS];
+      M::proj2obs<double>(xs, obs);
+      kn += 1.0;
+      const double x = M::obs_mean(obs[ts], ts, t, oe);
+      const double delta = x - pred;
+      pred += delta / kn;
+      M2 += delta * (x - pred);
+      var_obs += M::obs_var(obs[ts], ts, t, oe);
+    }
+    const double var_state = M2 / (kn - 1.0);
+    var_obs /= (double)J;
+    out[ts * 2 + 0] = pred;
+    out[ts * 2 + 1] = (y[ts] - pred) / sqrt(var_state + var_obs);
+  }
+}
+
+}  // namespace
+
 extern "C" {
 
 int oracle_model_info(plomgpu_model_info* o) {
@@ -262,12 +376,19 @@ int oracle_model_info(plomgpu_model_info* o) {
   o->coupled = M::COUPLED ? 1 : 0;
   o->pop_size_eq_sum_sv = M::POP_SIZE_EQ_SUM_SV ? 1 : 0;
   o->name = M::NAME;
+  o->n_hat = kNHat;
   return 0;
 }
 
 int oracle_draws_per_substep(int noises_off) { return draws_per_substep(noises_off); }
 
 // run_SMC restated.  n_threads <= 0: OpenMP default.
+// get_CI95 on given values and weights (null: 1/J), known-answer tests.
+void oracle_ci95(const double* v, const double* w, int J, double* lo, double* hi) {
+  std::vector<double> vv(v, v + J);
+  ci95(vv, w, J, lo, hi);
+}
+
 int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threads) {
   const int J = d->J, S = M::S;
   if (J < 1 || d->precision != 64 && d->precision != 32) return PLOMGPU_EINVAL;
@@ -282,12 +403,14 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
     for (int w = 0; w < S; ++w) X[(size_t)j * S + w] = (w < M::OFF_INC) ? d->x0[w] : 0.0;
   std::vector<double> wts(J);
   std::vector<uint32_t> select(J);
+  if (r->hat) compute_hat(X, J, nullptr, d, d->cov_ts0, d->pop_size, 0.0, r->hat);
   double Llike = 0.0;
   int n_all_fail = 0;
   size_t crn_off = 0;
   int sub0 = 0;
   for (int n = 0; n < d->n_obs; ++n) {
     const double* y = d->data + (size_t)n * M::N_TS;
+    const double* cov_n = d->cov_ts ? d->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS : nullptr;
     int n_nonan = 0;
     for (int ts = 0; ts < M::N_TS; ++ts)
       if (!isnan(y[ts])) ++n_nonan;
@@ -319,13 +442,20 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
         const double U = (1.0 / (double)J) * u;
         systematic_sampling(wts, J, U, select.data());
       }
+      if (r->hat)
+        compute_hat(Xn, J, wts.data(), d, cov_n, d->pop_size ? d->pop_size + (size_t)(n + 1) * M::N_CAC : nullptr,
+                    d->t_obs[n], r->hat + (size_t)(n + 1) * kNHat * 3);
       // resample_X: gather the state words (incidences are reset next interval)
       for (int j = 0; j < J; ++j) {
         const size_t s = (size_t)select[j] * S;
         for (int w = 0; w < S; ++w) X[(size_t)j * S + w] = Xn[s + w];
       }
+      if (r->pred_res) pred_res(X, J, d, cov_n, d->t_obs[n], y, r->pred_res + (size_t)n * M::N_TS * 2);
     } else {
       for (int j = 0; j < J; ++j) select[j] = (uint32_t)j;
+      if (r->hat)
+        compute_hat(Xn, J, nullptr, d, cov_n, d->pop_size ? d->pop_size + (size_t)(n + 1) * M::N_CAC : nullptr,
+                    d->t_obs[n], r->hat + (size_t)(n + 1) * kNHat * 3);
       X.swap(Xn);
     }
     if (r->llike_n) r->llike_n[n] = llike_n;

@@ -176,3 +176,40 @@ def test_oracle_crn_is_deterministic_and_sensitive():
     z2 = z.copy()
     z2[0] += 1.0
     assert orc.smc(p, crn_normals=z2, crn_uniforms=u).loglik != a.loglik
+
+
+# ------------------------------------------------------------------ filtered summaries (oracle)
+def test_ci95_known_answer():
+    """get_CI95 (model_builder/C/core/hat.c:28-57): the value at which the sorted running weight reaches the level."""
+    orc = models.build_oracle('sir')
+    v = [3.0, 1.0, 2.0, 4.0]
+    w = [0.1, 0.02, 0.5, 0.38]
+    # sorted 1 (0.02), 2 (0.52), 3 (0.62), 4 (1.0)
+    assert orc.ci95(v, w) == (2.0, 4.0)
+    # equal weights: 40 values, the running sum of 1/40 reaches 0.025 at the first value
+    vals = np.arange(40.0)[::-1].copy()
+    lo, hi = orc.ci95(vals)
+    assert lo == 0.0
+    # 0.975 * 40 = 39 terms of 1/40 summed in sequence
+    cum, k = 0.0, 0
+    while cum < 0.975:
+        cum += 1.0 / 40
+        k += 1
+    assert hi == float(k - 1)
+
+
+def test_oracle_summaries_are_consistent():
+    """Summaries of the oracle's filter: ordered intervals, a constant start, the remainder identity."""
+    orc = models.build_oracle('sir')
+    p = models.make_problem('sir', J=300, dt=1.0, precision=64, seed=3)
+    out = orc.smc(p, hat=True)
+    h = out.hat
+    assert h.shape == (p.n_obs + 1, orc.n_hat, 3)
+    assert np.all(h[:, :, 0] <= h[:, :, 2])
+    # time 0: every particle starts from the same state
+    np.testing.assert_allclose(h[0, :, 0], h[0, :, 2])
+    # the remainder row is N(t) - S - I
+    m = p.model
+    nsv = orc.info.n_par_sv * orc.info.n_cac
+    np.testing.assert_allclose(h[0, nsv, 1], p.pop_size[0, 0] - h[0, :nsv, 1].sum(), rtol=1e-12)
+    assert np.all(np.isfinite(out.pred_res[:, :, 0]))  # res is 0/0 = nan once the epidemic is over, as in the reference
