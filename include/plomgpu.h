@@ -152,9 +152,21 @@ typedef struct plomgpu_plan plomgpu_plan;
 
 int plomgpu_plan_create(const plomgpu_smc_desc *desc, plomgpu_plan **out);
 /* flags: PLOMGPU_PLAN_TIMING records CUDA events around every propagate
- * launch inside the graph, read back with plomgpu_plan_propagate_time(). */
-enum { PLOMGPU_PLAN_TIMING = 1 };
+ * launch inside the graph, read back with plomgpu_plan_propagate_time();
+ * PLOMGPU_PLAN_TRAJ keeps the genealogy and the propagated particles of every
+ * interval (FP64, n_obs * n_state * J doubles) for plomgpu_plan_sample_traj
+ * and for result.ancestors / result.x_pred; PLOMGPU_PLAN_SUMMARIES computes
+ * result.hat and result.pred_res on every launch. */
+enum { PLOMGPU_PLAN_TIMING = 1, PLOMGPU_PLAN_TRAJ = 2, PLOMGPU_PLAN_SUMMARIES = 4 };
 int plomgpu_plan_create_ex(const plomgpu_smc_desc *desc, int flags, plomgpu_plan **out);
+/* One trajectory of the last launch drawn from its genealogy
+ * (sample_traj_and_print, model_builder/C/core/print.c:715-784, with the same
+ * indexing): u in [0, 1) picks the final particle by the last weighted
+ * interval's normalised weights.  Writes n_rows (<= n_obs + 2) rows in the
+ * reference's print order, last time first: rows_t[r] is the time row
+ * (0 = time 0, n + 1 = t_obs[n]) and states[r][n_state] the particle.  Needs
+ * PLOMGPU_PLAN_TRAJ and at least two intervals with data. */
+int plomgpu_plan_sample_traj(plomgpu_plan *plan, double u, int *n_rows, int *rows_t, double *states);
 /* Device time of the propagate launches of the last plomgpu_plan_launch
  * (sum over launches, milliseconds) and their number. */
 int plomgpu_plan_propagate_time(plomgpu_plan *plan, double *total_ms, int *launches);
@@ -163,6 +175,9 @@ int plomgpu_plan_propagate_time(plomgpu_plan *plan, double *total_ms, int *launc
  * values. */
 int plomgpu_plan_update(plomgpu_plan *plan, const double *par_cac, const double *par_ts,
                         const double *x0, uint64_t seed);
+/* Uploads a new volatility table of the drifted parameters ([n_drift][n_cac],
+ * indexed like smc_desc.drift_vol); synchronous. */
+int plomgpu_plan_update_drift(plomgpu_plan *plan, const double *drift_vol);
 /* Enqueues one filter run on the plan's stream; inputs must be resident. */
 int plomgpu_plan_launch(plomgpu_plan *plan);
 /* Waits for the plan's stream and copies the results to host memory. */
@@ -330,6 +345,15 @@ void plomgpu_server_destroy(plomgpu_server *server);
  * before any stream capture on that device. */
 int plomgpu_resample_noalloc(const void *log_weights, int precision, int J, double like_min, double u,
                              uint32_t *ancestors, double *out, void *stream);
+
+/* Per-particle values of the printed quantities: particle i is X[:, i]
+ * (X [n_state][P], host, FP64) at time row rows[i] (0 = time 0, n + 1 =
+ * t_obs[n]).  out ([n_hat + n_ts][P], host) holds the rows of the filtered
+ * summaries (states, remainders, observation means, drifted parameters on
+ * the natural scale) followed by the observation variances: the columns of
+ * print_p_X (model_builder/C/core/print.c:301-357) apart from its random
+ * observation draws. */
+int plomgpu_particle_values(const plomgpu_smc_desc *desc, const double *X, int P, const int *rows, double *out);
 
 const char *plomgpu_last_error(void);
 

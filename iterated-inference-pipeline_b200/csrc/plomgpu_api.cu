@@ -128,6 +128,13 @@ struct plomgpu_plan {
   double* pop = nullptr;       // [n_obs + 1][N_CAC]
   double* cov_ts0 = nullptr;   // [N_COV_TS][N_TS] at time 0
   double hat_rank[2] = {1.0, 1.0};  // quantile ranks under equal weights
+  // sampled trajectories
+  int n_data = 0;
+  int* data_idx = nullptr;     // device: intervals with data, ascending
+  int* traj_t = nullptr;       // device [n_obs + 2]
+  int* traj_j = nullptr;       // device [n_obs + 2]
+  int* traj_n = nullptr;       // device scalar
+  double* traj_x = nullptr;    // device [n_obs + 2][S]
 };
 
 // Rank (1-based) at which a running sum of 1/J, accumulated as the reference
@@ -481,6 +488,20 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   }
   if (p->want_anc) CK(cudaMalloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
   if (p->want_xpred) CK(cudaMalloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
+  if (p->want_anc && p->want_xpred && p->R == 1) {
+    std::vector<int> idx;
+    for (int n = 0; n < d->n_obs; ++n)
+      if (p->weigh[n]) idx.push_back(n);
+    p->n_data = (int)idx.size();
+    if (!idx.empty()) {
+      int rc2 = upload<int>(idx.data(), idx.size(), &p->data_idx, s);
+      if (rc2) return rc2;
+    }
+    CK(cudaMalloc((void**)&p->traj_t, (size_t)(d->n_obs + 2) * sizeof(int)));
+    CK(cudaMalloc((void**)&p->traj_j, (size_t)(d->n_obs + 2) * sizeof(int)));
+    CK(cudaMalloc((void**)&p->traj_n, sizeof(int)));
+    CK(cudaMalloc((void**)&p->traj_x, (size_t)(d->n_obs + 2) * M::S * sizeof(double)));
+  }
   if (p->want_hat) {
     if (p->R != 1) return fail(PLOMGPU_EINVAL, "filtered summaries need a single run");
     if (!M::POP_SIZE_EQ_SUM_SV && !d->pop_size) return fail(PLOMGPU_EINVAL, "summaries of a remainder need pop_size");
@@ -531,7 +552,8 @@ void plan_free(plomgpu_plan* p) {
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
-                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0};
+                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->data_idx, p->traj_t,
+                  p->traj_j, p->traj_n, p->traj_x};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (p->acc_h) cudaFreeHost(p->acc_h);
@@ -694,7 +716,34 @@ int plomgpu_plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out) {
 
 int plomgpu_plan_create_ex(const plomgpu_smc_desc* d, int flags, plomgpu_plan** out) {
   if (!out) return fail(PLOMGPU_EINVAL, "null output");
-  return plan_create(d, out, false, false, false, (flags & PLOMGPU_PLAN_TIMING) != 0);
+  const bool traj = (flags & PLOMGPU_PLAN_TRAJ) != 0;
+  return plan_create(d, out, traj, traj, false, (flags & PLOMGPU_PLAN_TIMING) != 0, nullptr,
+                     (flags & PLOMGPU_PLAN_SUMMARIES) != 0);
+}
+
+int plomgpu_plan_sample_traj(plomgpu_plan* p, double u, int* n_rows, int* rows_t, double* states) {
+  if (!p || !n_rows || !rows_t || !states) return fail(PLOMGPU_EINVAL, "null argument");
+  if (!p->traj_x) return fail(PLOMGPU_EINVAL, "plan was created without PLOMGPU_PLAN_TRAJ");
+  if (p->n_data < 2) return fail(PLOMGPU_EINVAL, "trajectory sampling needs at least two intervals with data");
+  cudaStream_t s = p->stream;
+  if (p->precision == 64)
+    k_sample_traj<double, 256><<<1, 256, 0, s>>>((const double*)p->lw, p->J, p->st, p->thresh, u, p->n_obs,
+                                                 p->data_idx, p->n_data, p->anc_hist, p->x_hist, p->x0, p->traj_t,
+                                                 p->traj_j, p->traj_x, p->traj_n);
+  else
+    k_sample_traj<float, 256><<<1, 256, 0, s>>>((const float*)p->lw, p->J, p->st, p->thresh, u, p->n_obs,
+                                                p->data_idx, p->n_data, p->anc_hist, p->x_hist, p->x0, p->traj_t,
+                                                p->traj_j, p->traj_x, p->traj_n);
+  CK(cudaGetLastError());
+  int n = 0;
+  CK(cudaMemcpyAsync(&n, p->traj_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (n < 1 || n > p->n_obs + 2) return fail(PLOMGPU_ECUDA, "trajectory walk produced a bad row count");
+  CK(cudaMemcpyAsync(rows_t, p->traj_t, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(states, p->traj_x, (size_t)n * M::S * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *n_rows = n;
+  return PLOMGPU_OK;
 }
 
 int plomgpu_plan_propagate_time(plomgpu_plan* p, double* total_ms, int* launches) {
@@ -726,6 +775,20 @@ int plomgpu_plan_update(plomgpu_plan* p, const double* par_cac, const double* pa
   static thread_local uint64_t seed_h;
   seed_h = seed;
   CK(cudaMemcpyAsync(p->seed, &seed_h, sizeof(uint64_t), cudaMemcpyHostToDevice, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
+  return PLOMGPU_OK;
+}
+
+int plomgpu_plan_update_drift(plomgpu_plan* p, const double* drift_vol) {
+  if (!p || !drift_vol) return fail(PLOMGPU_EINVAL, "null argument");
+  if (!p->drift_vol) return PLOMGPU_OK;  // drift off for this plan: nothing reads the table
+  const size_t n = (size_t)M::N_DRIFT * M::N_CAC;
+  if (p->precision == 64) {
+    CK(cudaMemcpyAsync(p->drift_vol, drift_vol, n * sizeof(double), cudaMemcpyHostToDevice, p->stream));
+  } else {
+    std::vector<float> f(drift_vol, drift_vol + n);
+    CK(cudaMemcpyAsync(p->drift_vol, f.data(), n * sizeof(float), cudaMemcpyHostToDevice, p->stream));
+  }
   CK(cudaStreamSynchronize(p->stream));
   return PLOMGPU_OK;
 }
@@ -781,6 +844,54 @@ int plomgpu_debug_systematic_points(double U, int J, double* out) {
   cudaFree(err);
   if (herr) return fail(PLOMGPU_EINVAL, "systematic point table overflow");
   return PLOMGPU_OK;
+}
+
+int plomgpu_particle_values(const plomgpu_smc_desc* d, const double* X, int P, const int* rows, double* out) {
+  if (!d || !X || !rows || !out || P < 1) return fail(PLOMGPU_EINVAL, "bad arguments");
+  for (int i = 0; i < P; ++i)
+    if (rows[i] < 0 || rows[i] > d->n_obs) return fail(PLOMGPU_EINVAL, "time rows must be in [0, n_obs]");
+  if (!M::POP_SIZE_EQ_SUM_SV && !d->pop_size) return fail(PLOMGPU_EINVAL, "a model with a remainder needs pop_size");
+  if (M::N_COV_TS > 0 && (!d->cov_ts0 || (d->n_obs > 0 && !d->cov_ts)))
+    return fail(PLOMGPU_EINVAL, "missing observation covariates");
+  double *dX = nullptr, *dv = nullptr, *dpar = nullptr, *dcov = nullptr, *dcov0 = nullptr, *dpop = nullptr,
+         *dt = nullptr;
+  int* drows = nullptr;
+  plomrt::BackTransform* dbt = nullptr;
+  cudaStream_t s = 0;
+  int rc = PLOMGPU_OK;
+  do {
+    if ((rc = upload<double>(X, (size_t)M::S * P, &dX, s))) break;
+    if ((rc = upload<int>(rows, (size_t)P, &drows, s))) break;
+    if (d->n_obs > 0 && (rc = upload<double>(d->t_obs, (size_t)d->n_obs, &dt, s))) break;
+    if (M::N_PAR_OBS > 0 && (rc = upload<double>(d->par_ts, (size_t)M::N_PAR_OBS * M::N_TS, &dpar, s))) break;
+    if (M::N_COV_TS > 0) {
+      if ((rc = upload<double>(d->cov_ts0, (size_t)M::N_COV_TS * M::N_TS, &dcov0, s))) break;
+      if (d->n_obs > 0 && (rc = upload<double>(d->cov_ts, (size_t)d->n_obs * M::N_COV_TS * M::N_TS, &dcov, s))) break;
+    }
+    if (d->pop_size && (rc = upload<double>(d->pop_size, (size_t)(d->n_obs + 1) * M::N_CAC, &dpop, s))) break;
+    if (M::N_DRIFT > 0 && d->drift_bt) {
+      if (cudaMalloc((void**)&dbt, (size_t)M::N_DRIFT * M::N_CAC * sizeof(plomrt::BackTransform)) != cudaSuccess ||
+          cudaMemcpy(dbt, d->drift_bt, (size_t)M::N_DRIFT * M::N_CAC * sizeof(plomrt::BackTransform),
+                     cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = fail(PLOMGPU_ECUDA, "drift table upload failed");
+        break;
+      }
+    }
+    const size_t n_out = (size_t)(kHatQ + M::N_TS) * P;
+    if (cudaMalloc((void**)&dv, n_out * sizeof(double)) != cudaSuccess) {
+      rc = fail(PLOMGPU_ECUDA, "allocation failed");
+      break;
+    }
+    const int g = (P + 255) / 256 < 4096 ? (P + 255) / 256 : 4096;
+    k_particle_values<<<g, 256, 0, s>>>(dX, P, drows, dt, dpop, dpar, dcov, dcov0, dbt, dv);
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpy(out, dv, n_out * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = fail(PLOMGPU_ECUDA, "particle values kernel failed");
+  } while (0);
+  for (void* b : {(void*)dX, (void*)dv, (void*)dpar, (void*)dcov, (void*)dcov0, (void*)dpop, (void*)dt, (void*)drows,
+                  (void*)dbt})
+    if (b) cudaFree(b);
+  return rc;
 }
 
 const char* plomgpu_last_error(void) { return g_err.c_str(); }

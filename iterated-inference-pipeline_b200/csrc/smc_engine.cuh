@@ -773,6 +773,40 @@ struct ColumnView {
   __device__ __forceinline__ double operator[](int w) const { return (double)p[(size_t)w * ld]; }
 };
 
+// The printed quantities of one particle: state words, remainders, observation
+// means, drifted parameters (f_inv of their state word), then observation
+// variances; out[q * stride] for q < kHatQ + N_TS.
+template <class X>
+__device__ __forceinline__ void particle_values(const X& x, const double* pop_size, const double* par_ts,
+                                                const double* cov_ts, double t,
+                                                const plomrt::BackTransform* drift_bt, double* out, size_t stride) {
+  int q = 0;
+  for (int i = 0; i < kHatSv; ++i) out[(size_t)(q++) * stride] = x[i];
+  for (int c = 0; c < kHatRem; ++c) {
+    double sv = 0.0;
+    for (int i = 0; i < M::N_PAR_SV; ++i) sv += x[i * M::N_CAC + c];
+    out[(size_t)(q++) * stride] = pop_size[c] - sv;
+  }
+  double obs[M::N_TS];
+  M::template proj2obs<double>(x, obs);
+  ObsEnv oe;
+  oe.par_ts_ = par_ts;
+  oe.cov_ts_ = cov_ts;
+  for (int ts = 0; ts < M::N_TS; ++ts) out[(size_t)(q++) * stride] = M::obs_mean(obs[ts], ts, t, oe);
+  for (int i = 0; i < kHatDrift; ++i) {
+    double v = x[M::OFF_DRIFT + i];
+    if (drift_bt) {
+      plomrt::BackTransform b = drift_bt[i];
+      b.scale = 0;
+      b.multiplier = 1.0;
+      b.is_duration = 0;
+      v = plomrt::back_transform<double>(v, b);
+    }
+    out[(size_t)(q++) * stride] = v;
+  }
+  for (int ts = 0; ts < M::N_TS; ++ts) out[(size_t)(q++) * stride] = M::obs_var(obs[ts], ts, t, oe);
+}
+
 // Values of every summarised quantity per particle (column-major [kHatVals][J])
 // and the particle's weight: its normalised weight when the interval was
 // weighted and not all particles failed, else 1 (a count; the quantile ranks
@@ -786,37 +820,32 @@ __global__ void k_hat_values(const T* __restrict__ X, int J, const double* __res
   const double m = uni ? 0.0 : st->m, s1 = uni ? 1.0 : st->s1;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J; j += gridDim.x * blockDim.x) {
     const ColumnView<T> x{X + j, (size_t)J};
-    int q = 0;
-    for (int i = 0; i < kHatSv; ++i) vals[(size_t)(q++) * J + j] = x[i];
-    for (int c = 0; c < kHatRem; ++c) {
-      double sv = 0.0;
-      for (int i = 0; i < M::N_PAR_SV; ++i) sv += x[i * M::N_CAC + c];
-      vals[(size_t)(q++) * J + j] = pop_size[c] - sv;
-    }
-    double obs[M::N_TS];
-    M::template proj2obs<double>(x, obs);
-    ObsEnv oe;
-    oe.par_ts_ = par_ts;
-    oe.cov_ts_ = cov_ts;
-    for (int ts = 0; ts < M::N_TS; ++ts) vals[(size_t)(q++) * J + j] = M::obs_mean(obs[ts], ts, t_obs, oe);
-    for (int i = 0; i < kHatDrift; ++i) {
-      double v = x[M::OFF_DRIFT + i];
-      if (drift_bt) {
-        plomrt::BackTransform b = drift_bt[i];
-        b.scale = 0;
-        b.multiplier = 1.0;
-        b.is_duration = 0;
-        v = plomrt::back_transform<double>(v, b);
-      }
-      vals[(size_t)(q++) * J + j] = v;
-    }
-    for (int ts = 0; ts < M::N_TS; ++ts) vals[(size_t)(q++) * J + j] = M::obs_var(obs[ts], ts, t_obs, oe);
+    particle_values(x, pop_size, par_ts, cov_ts, t_obs, drift_bt, vals + j, (size_t)J);
     double w = 1.0;
     if (!uni) {
       const T l = lw[j];
       w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
     }
     vals[(size_t)kHatW * J + j] = w;
+  }
+}
+
+// Printed quantities of particles taken at different times: particle i is
+// X[:, i] at time row rows[i] (0 = time 0, n + 1 = t_obs[n]); out is
+// [kHatQ + N_TS][P].  Tables: pop_size [n_obs + 1][N_CAC], cov_ts
+// [n_obs][N_COV_TS][N_TS], cov_ts0 [N_COV_TS][N_TS].
+__global__ void k_particle_values(const double* __restrict__ X, int P, const int* __restrict__ rows,
+                                  const double* __restrict__ t_obs, const double* __restrict__ pop_size,
+                                  const double* __restrict__ par_ts, const double* __restrict__ cov_ts,
+                                  const double* __restrict__ cov_ts0, const plomrt::BackTransform* __restrict__ drift_bt,
+                                  double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P; i += gridDim.x * blockDim.x) {
+    const int r = rows[i];
+    const ColumnView<double> x{X + i, (size_t)P};
+    const double* cov = r == 0 ? cov_ts0 : (cov_ts ? cov_ts + (size_t)(r - 1) * M::N_COV_TS * M::N_TS : nullptr);
+    const double t = r == 0 ? 0.0 : t_obs[r - 1];
+    particle_values(x, pop_size ? pop_size + (size_t)r * M::N_CAC : nullptr, par_ts, cov, t, drift_bt, out + i,
+                    (size_t)P);
   }
 }
 
@@ -961,6 +990,92 @@ __global__ void __launch_bounds__(BT) k_pred_res(const double* __restrict__ vals
     const double var_state = M2 / ((double)J - 1.0);
     out[ts * 2 + 0] = pred;
     out[ts * 2 + 1] = (y[ts] - pred) / sqrt(var_state + var_obs);
+  }
+}
+
+// ------------------------------------------------------------------ sampled trajectory
+// One trajectory drawn from the filter's genealogy as sample_traj_and_print
+// does (model_builder/C/core/print.c:715-784), including its indexing:
+// * the final particle j is the first whose running weight (last weighted
+//   interval, in particle order) reaches u, and it indexes the resampled
+//   population;
+// * walking back, the ancestor index at a data interval is taken from that
+//   interval's own selection (select[indn]) for every data interval but the
+//   last, and intervals without data keep j.
+// post(n, j) = x_hist[n][:, anc_hist[n][j]] is particle j after interval n
+// (anc_hist is the identity where nothing was resampled); time -1 is x0.
+// Rows are written in print order: rows_t[r] = time row (n + 1), states
+// [r][S].  One block; the walk is serial (T steps), the gathers parallel.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT) k_sample_traj(const T* __restrict__ lw, int J, const StepState* st,
+                                                    double thresh, double u, int n_obs,
+                                                    const int* __restrict__ data_idx, int n_data,
+                                                    const uint32_t* __restrict__ anc_hist,
+                                                    const double* __restrict__ x_hist, const double* __restrict__ x0,
+                                                    int* __restrict__ rows_t, int* __restrict__ rows_j,
+                                                    double* __restrict__ states, int* __restrict__ n_rows) {
+  __shared__ double s_part[BT];
+  __shared__ int s_sel;
+  const bool uni = st->all_fail;
+  const double m = uni ? 0.0 : st->m, s1 = uni ? 1.0 : st->s1;
+  auto wgt = [&](int j) -> double {
+    if (uni) return 1.0 / (double)J;
+    const T l = lw[j];
+    return weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+  };
+  // first j with inclusive running weight >= u: chunk sums, a serial scan of
+  // BT partial sums, then a serial search inside the chunk that crosses
+  const int chunk = (J + BT - 1) / BT;
+  const int lo = threadIdx.x * chunk, hi = min(J, lo + chunk);
+  double acc = 0.0;
+  for (int j = lo; j < hi; ++j) acc += wgt(j);
+  s_part[threadIdx.x] = acc;
+  if (threadIdx.x == 0) s_sel = J - 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double run = 0.0;
+    for (int t = 0; t < BT; ++t) {
+      const double next = run + s_part[t];
+      if (next >= u && t * chunk < J) {
+        int j = t * chunk;
+        const int e = min(J, j + chunk);
+        double c = run;
+        for (; j < e; ++j) {
+          c += wgt(j);
+          if (c >= u) break;
+        }
+        s_sel = j < e ? j : e - 1;
+        break;
+      }
+      run = next;
+    }
+    // the walk
+    int j = s_sel, r = 0;
+    auto put = [&](int n, int jj) {
+      rows_t[r] = n + 1;
+      rows_j[r] = (n < 0) ? 0 : (int)anc_hist[(size_t)n * J + jj];
+      ++r;
+    };
+    put(n_obs - 1, j);
+    for (int nn = data_idx[n_data - 1] - 1; nn > data_idx[n_data - 2]; --nn) put(nn, j);
+    for (int k = n_data - 2; k >= 1; --k) {
+      const int indn = data_idx[k];
+      j = (int)anc_hist[(size_t)indn * J + j];
+      put(indn, j);
+      for (int nn = indn - 1; nn > data_idx[k - 1]; --nn) put(nn, j);
+    }
+    const int indn = data_idx[0];
+    j = (int)anc_hist[(size_t)indn * J + j];
+    for (int nn = indn; nn >= -1; --nn) put(nn, j);
+    *n_rows = r;
+    s_sel = r;
+  }
+  __syncthreads();
+  const int R = s_sel;
+  for (int i = threadIdx.x; i < R * M::S; i += BT) {
+    const int r = i / M::S, w = i % M::S;
+    const int n = rows_t[r] - 1;
+    states[i] = (n < 0) ? (w < M::OFF_INC ? x0[w] : 0.0) : x_hist[((size_t)n * M::S + w) * J + rows_j[r]];
   }
 }
 

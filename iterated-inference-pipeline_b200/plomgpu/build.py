@@ -52,7 +52,7 @@ def write_header(model, name):
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in ('plom_rt.h', 'smc_engine.cuh', 'plomgpu_api.cu')] + \
+    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.h', '.cuh', '.cu'))) + \
         [os.path.join(INCLUDE, 'plomgpu.h')]
 
 
@@ -80,16 +80,16 @@ def nvcc_command(name, S, out=None, verbose_ptxas=False):
     return cmd
 
 
-def build_model(model, name, force=False, verbose=False):
+def build_model(model, name, force=False, verbose=False, out=None):
     """Emit + compile; skips the compile when sources and header are unchanged."""
     _, S = write_header(model, name)
-    os.makedirs(LIB, exist_ok=True)
-    out = lib_path(name)
+    out = out or lib_path(name)
+    os.makedirs(os.path.dirname(out), exist_ok=True)
     stamp_file = out + '.stamp'
     stamp = _stamp(name, {'S': S, 'arch': ARCH})
     if not force and os.path.exists(out) and os.path.exists(stamp_file) and open(stamp_file).read() == stamp:
         return out
-    cmd = nvcc_command(name, S)
+    cmd = nvcc_command(name, S, out=out)
     if verbose:
         print(' '.join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
@@ -100,3 +100,37 @@ def build_model(model, name, force=False, verbose=False):
 
 def build_from_files(context, process, link, name, **kw):
     return build_model(PlomModel(context, process, link), name, **kw)
+
+
+LAUNCHER = """#!/bin/sh
+# %(cmd)s for this model directory, on the B200 engine
+PYTHONPATH="%(pkg)s${PYTHONPATH:+:$PYTHONPATH}" exec "%(python)s" -m plomgpu %(cmd)s "$@"
+"""
+
+
+def model_dir_name(context, process, link):
+    h = hashlib.sha256(json.dumps([context, process, link], sort_keys=True).encode()).hexdigest()
+    return 'm%s' % h[:12]
+
+
+def build_model_dir(context, process, link, out_dir, force=False, name=None, shared_lib=False):
+    """A model directory: .settings.json (Builder.write_settings, model_builder/Builder.py:349-351),
+    the manifest read by the drivers, the engine library, and smc / pmcmc / mif launchers.
+    ``shared_lib`` keeps the library in the package's library folder under ``name``
+    (models built once and used from several directories)."""
+    model = PlomModel(context, process, link)
+    os.makedirs(out_dir, exist_ok=True)
+    name = name or model_dir_name(context, process, link)
+    lib = lib_path(name) if shared_lib else os.path.join(out_dir, 'lib', 'libplomgpu_%s.so' % name)
+    build_model(model, name, force=force, out=lib)
+    with open(os.path.join(out_dir, '.settings.json'), 'w') as f:
+        json.dump(model.settings(), f)
+    with open(os.path.join(out_dir, '.plomgpu.json'), 'w') as f:
+        json.dump({'context': context, 'process': process, 'link': link, 'name': name,
+                   'library': lib if shared_lib else os.path.join('lib', os.path.basename(lib))}, f)
+    for cmd in ('smc', 'pmcmc', 'mif'):
+        p = os.path.join(out_dir, cmd)
+        with open(p, 'w') as f:
+            f.write(LAUNCHER % {'cmd': cmd, 'pkg': PKG_ROOT, 'python': sys.executable})
+        os.chmod(p, 0o755)
+    return out_dir

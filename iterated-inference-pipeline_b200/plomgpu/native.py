@@ -84,7 +84,8 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
                'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
                'plomgpu_server_create', 'plomgpu_server_submit', 'plomgpu_server_poll', 'plomgpu_server_wait',
-               'plomgpu_server_get_stats', 'plomgpu_server_destroy']
+               'plomgpu_server_get_stats', 'plomgpu_server_destroy', 'plomgpu_particle_values',
+               'plomgpu_plan_sample_traj', 'plomgpu_plan_update_drift']
 
 
 def _ptr(a, t):
@@ -173,6 +174,8 @@ def _declare(lib):
     lib.plomgpu_plan_propagate_time.argtypes = [C.c_void_p, _dp, _ip]
     lib.plomgpu_plan_update.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_uint64]
     lib.plomgpu_plan_launch.argtypes = [C.c_void_p]
+    lib.plomgpu_plan_sample_traj.argtypes = [C.c_void_p, C.c_double, _ip, _ip, _dp]
+    lib.plomgpu_plan_update_drift.argtypes = [C.c_void_p, _dp]
     lib.plomgpu_plan_results.argtypes = [C.c_void_p, _P(SmcResult)]
     lib.plomgpu_plan_stream.argtypes = [C.c_void_p]
     lib.plomgpu_plan_stream.restype = C.c_void_p
@@ -183,6 +186,7 @@ def _declare(lib):
     lib.plomgpu_resample_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
     lib.plomgpu_last_error.restype = C.c_char_p
+    lib.plomgpu_particle_values.argtypes = [_P(SmcDesc), _dp, C.c_int, _ip, _dp]
     lib.plomgpu_batch_create.argtypes = [_P(BatchDesc), _P(C.c_void_p)]
     lib.plomgpu_batch_launch.argtypes = [C.c_void_p]
     lib.plomgpu_batch_results.argtypes = [C.c_void_p, _dp, _ip, _dp]
@@ -252,22 +256,49 @@ class Engine(object):
     def draws_per_substep(self, noises_off):
         return self.lib.plomgpu_draws_per_substep(noises_off)
 
+    def particle_values(self, problem, X, rows):
+        """[n_hat + n_ts][P]: summarised quantities then observation variances of particles X ([S][P]),
+        particle i at time row rows[i] (0 = time 0, n + 1 = t_obs[n]; an int applies to all)."""
+        h = DescHolder(problem, precision=64)
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        P = X.shape[1]
+        r = np.ascontiguousarray(np.broadcast_to(np.asarray(rows, dtype=np.int32), (P,)))
+        out = np.zeros((self.info.n_hat + self.info.n_ts, P))
+        check(self.lib, self.lib.plomgpu_particle_values(C.byref(h.desc), _ptr(X, _dp), P, _ptr(r, _ip),
+                                                         _ptr(out, _dp)))
+        return out
+
     def systematic_points(self, U, J):
         out = np.zeros(J)
         check(self.lib, self.lib.plomgpu_debug_systematic_points(U, J, _ptr(out, _dp)))
         return out
 
 
+PLAN_TIMING, PLAN_TRAJ, PLAN_SUMMARIES = 1, 2, 4
+
+
 class Plan(object):
     """A captured filter (plomgpu_plan_*), for repeated likelihood evaluations."""
 
-    def __init__(self, engine, problem, precision=None, timing=False):
+    def __init__(self, engine, problem, precision=None, timing=False, traj=False, summaries=False):
         self.engine = engine
         self.lib = engine.lib
         self.h = DescHolder(problem, precision=precision)
         self.p = C.c_void_p()
-        check(self.lib, self.lib.plomgpu_plan_create_ex(C.byref(self.h.desc), 1 if timing else 0, C.byref(self.p)))
+        flags = (PLAN_TIMING if timing else 0) | (PLAN_TRAJ if traj else 0) | (PLAN_SUMMARIES if summaries else 0)
+        self.flags = flags
+        check(self.lib, self.lib.plomgpu_plan_create_ex(C.byref(self.h.desc), flags, C.byref(self.p)))
         self.problem = problem
+
+    def sample_traj(self, u):
+        """(time rows [R], states [R][S]) of one trajectory of the last launch, in print order."""
+        T, S = self.problem.n_obs, self.engine.info.n_state
+        rows = np.zeros(T + 2, dtype=np.int32)
+        states = np.zeros((T + 2, S))
+        n = C.c_int()
+        check(self.lib, self.lib.plomgpu_plan_sample_traj(self.p, float(u), C.byref(n), _ptr(rows, _ip),
+                                                          _ptr(states, _dp)))
+        return rows[:n.value].copy(), states[:n.value].copy()
 
     def propagate_time(self):
         """(total ms, launches) of the propagate kernels of the last launch."""
@@ -282,11 +313,18 @@ class Plan(object):
         check(self.lib, self.lib.plomgpu_plan_update(
             self.p, *(k.ctypes.data_as(_dp) if k is not None else None for k in keep), C.c_uint64(seed)))
 
+    def update_drift(self, drift_vol):
+        v = np.ascontiguousarray(drift_vol, dtype=np.float64)
+        check(self.lib, self.lib.plomgpu_plan_update_drift(self.p, _ptr(v, _dp)))
+
     def launch(self):
         check(self.lib, self.lib.plomgpu_plan_launch(self.p))
 
-    def results(self):
-        out = Outputs(self.problem.J, self.problem.n_obs, self.engine.info.n_state)
+    def results(self, ancestors=False, x_pred=False):
+        info = self.engine.info
+        summ = bool(self.flags & PLAN_SUMMARIES)
+        out = Outputs(self.problem.J, self.problem.n_obs, info.n_state, ancestors, x_pred, False,
+                      info.n_hat if summ else 0, info.n_ts)
         check(self.lib, self.lib.plomgpu_plan_results(self.p, C.byref(out.res)))
         return out
 

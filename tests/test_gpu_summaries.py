@@ -50,18 +50,23 @@ def test_summaries_match_oracle(name, J, dt, noises_off, filt):
     np.testing.assert_allclose(gp[:, :, 1][fin], op[:, :, 1][fin], rtol=1e-7, atol=1e-9)
 
 
-def test_summaries_large_J_properties():
-    """J = 2^18, FP32 production mode: intervals ordered, the time-0 row constant, the
-    remainder row equal to N(t) minus the summed states, the obs mean consistent."""
-    eng = models.engine('sir')
-    p = models.make_problem('sir', J=1 << 18, dt=1.0, precision=32, seed=5)
+@pytest.mark.parametrize('name', ['sir', 'noise'])
+def test_summaries_large_J_properties(name):
+    """J = 2^18, FP32 production mode: intervals ordered, the time-0 row constant,
+    the remainder rows (where the model has one) equal to N(t) minus the summed states."""
+    eng = models.engine(name)
+    p = models.make_problem(name, J=1 << 18, dt=1.0, precision=32, seed=5)
     g = eng.smc(p, hat=True)
     h = g.hat
     assert np.all(np.isfinite(h))
     assert np.all(h[:, :, 0] <= h[:, :, 2])
     np.testing.assert_allclose(h[0, :, 0], h[0, :, 2])
-    nsv = eng.info.n_par_sv * eng.info.n_cac
-    np.testing.assert_allclose(h[:, nsv, 1], p.pop_size[:, 0] - h[:, :nsv, 1].sum(axis=1), rtol=1e-6)
+    info = eng.info
+    if not info.pop_size_eq_sum_sv:
+        nc, nsv = info.n_cac, info.n_par_sv * info.n_cac
+        states = h[:, :nsv, 1].reshape(len(h), info.n_par_sv, nc).sum(axis=1)
+        np.testing.assert_allclose(h[:, nsv:nsv + nc, 1], p.pop_size - states, rtol=1e-5,
+                                   atol=1e-6 * p.pop_size.max())
     # the log-likelihood is unchanged by asking for summaries (same draws)
     assert eng.smc(p).loglik == g.loglik
 
@@ -69,8 +74,8 @@ def test_summaries_large_J_properties():
 def test_summaries_need_pop_size():
     """A model with a remainder needs N(t) for its summaries: a clear error, not a guess."""
     from plomgpu.native import PlomGpuError
-    eng = models.engine('sir')
-    p = models.make_problem('sir', J=100, dt=1.0, precision=64)
+    eng = models.engine('noise')
+    p = models.make_problem('noise', J=100, dt=1.0, precision=64)
     p.pop_size = None
     with pytest.raises(PlomGpuError):
         eng.smc(p, hat=True)

@@ -208,8 +208,12 @@ def test_oracle_summaries_are_consistent():
     assert np.all(h[:, :, 0] <= h[:, :, 2])
     # time 0: every particle starts from the same state
     np.testing.assert_allclose(h[0, :, 0], h[0, :, 2])
-    # the remainder row is N(t) - S - I
-    m = p.model
-    nsv = orc.info.n_par_sv * orc.info.n_cac
-    np.testing.assert_allclose(h[0, nsv, 1], p.pop_size[0, 0] - h[0, :nsv, 1].sum(), rtol=1e-12)
     assert np.all(np.isfinite(out.pred_res[:, :, 0]))  # res is 0/0 = nan once the epidemic is over, as in the reference
+    # a model with a remainder: its rows are N(t) minus the summed states
+    orc = models.build_oracle('noise')
+    p = models.make_problem('noise', J=200, dt=1.0, precision=64, seed=3)
+    h = orc.smc(p, hat=True).hat
+    info = orc.info
+    nc, nsv = info.n_cac, info.n_par_sv * info.n_cac
+    states = h[:, :nsv, 1].reshape(len(h), info.n_par_sv, nc).sum(axis=1)
+    np.testing.assert_allclose(h[:, nsv:nsv + nc, 1], p.pop_size - states, rtol=1e-9)
