@@ -107,6 +107,22 @@ typedef struct plomgpu_smc_desc {
      * observation covariates). */
     const double *pop_size;
     const double *cov_ts0;
+    /* Deterministic skeleton, the reference's "ode" implementation
+     * (f_prediction_ode, model_builder/C/core/prediction_util.c:176-193): when
+     * ode is 1 the process is integrated without noise by an embedded
+     * Runge-Kutta-Fehlberg 4(5) pair with step control (eps_abs, eps_rel;
+     * every interval starts from the step dt) and noises_off is ignored.  The
+     * process covariates are then evaluated at every stage time from their
+     * interpolants: cov_spline_meta [n_cov_cac * n_cac][3] = kind (0 constant,
+     * 1 linear, 2 natural cubic), number of knots, offset into the knot
+     * arrays x / y / m2 (second derivatives) of total length cov_spline_knots. */
+    int ode;
+    double eps_abs, eps_rel;
+    const int *cov_spline_meta;
+    const double *cov_spline_x;
+    const double *cov_spline_y;
+    const double *cov_spline_m2;
+    int cov_spline_knots;
 } plomgpu_smc_desc;
 
 typedef struct plomgpu_smc_result {

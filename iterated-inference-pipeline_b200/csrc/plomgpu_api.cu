@@ -41,6 +41,16 @@ int fail(int code, const std::string& msg) {
 
 constexpr bool kSmem = (M::S > 48);
 constexpr int kBtProp = 128;
+// lanes per particle of the team kernel (state in shared memory); 1 = one
+// thread per particle
+#ifndef PLOM_TEAM
+#define PLOM_TEAM 4
+#endif
+constexpr int kTeam = kSmem ? PLOM_TEAM : 1;
+constexpr int kBtOde = 64;
+constexpr int kOdeMaxSteps = 1000000;  // attempted RKF45 steps per interval
+static_assert(kTeam == 1 || kTeam == 2 || kTeam == 4 || kTeam == 8 || kTeam == 16 || kTeam == 32,
+              "team size must be a power of two up to 32");
 constexpr int kBtWeight = 256;
 constexpr int kBtScan = 256;
 constexpr int kIptScan = 8;
@@ -128,6 +138,12 @@ struct plomgpu_plan {
   double* pop = nullptr;       // [n_obs + 1][N_CAC]
   double* cov_ts0 = nullptr;   // [N_COV_TS][N_TS] at time 0
   double hat_rank[2] = {1.0, 1.0};  // quantile ranks under equal weights
+  // deterministic skeleton
+  bool ode = false;
+  double eps_abs = 1e-6, eps_rel = 1e-3;
+  std::vector<double> t_start;  // start of every interval
+  int* sp_meta = nullptr;
+  double *sp_x = nullptr, *sp_y = nullptr, *sp_m2 = nullptr;
   // sampled trajectories
   int n_data = 0;
   int* data_idx = nullptr;     // device: intervals with data, ascending
@@ -179,13 +195,36 @@ int upload(const U* h, size_t n, U** d, cudaStream_t s) {
 template <class T>
 using PropKernel = void (*)(const Tables<T>, const StepArgs);
 
+// a propagate kernel with its launch shape
+template <class T>
+struct PropLaunch {
+  PropKernel<T> k = nullptr;
+  int bt = 0;         // threads per block
+  int per_block = 0;  // particles per block
+  size_t smem = 0;    // dynamic shared memory
+  explicit operator bool() const { return k != nullptr; }
+};
+
 template <class T, int V, bool DRIFT, bool CRN, bool MIF>
-PropKernel<T> pick4() {
-  return &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp>;
+PropLaunch<T> pick4() {
+  PropLaunch<T> l;
+  if constexpr (kTeam > 1 && !MIF) {
+    typedef TeamLayout<T, V, kBtProp, kTeam> L;
+    l.k = &k_propagate_team<T, V, DRIFT, CRN, kBtProp, kTeam>;
+    l.bt = kBtProp;
+    l.per_block = L::PB;
+    l.smem = L::bytes();
+  } else {
+    l.k = &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp>;
+    l.bt = kBtProp;
+    l.per_block = kBtProp;
+    l.smem = propagate_smem_bytes<T, kSmem, kBtProp>();
+  }
+  return l;
 }
 
 template <class T, bool CRN, bool MIF>
-PropKernel<T> pick_v(int v, bool drift) {
+PropLaunch<T> pick_v(int v, bool drift) {
   if (drift) {
     if constexpr (M::N_DRIFT > 0) {
       switch (v) {
@@ -205,11 +244,11 @@ PropKernel<T> pick_v(int v, bool drift) {
 }
 
 template <class T>
-PropKernel<T> pick_prop(int noises_off, bool crn, bool mif) {
+PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif) {
   const int v = variant_of(noises_off);
   const bool d = drift_on(noises_off);
   if (mif) {
-    if (crn) return nullptr;
+    if (crn) return PropLaunch<T>();
     return pick_v<T, false, true>(v, d);
   }
   if (crn) return pick_v<T, true, false>(v, d);
@@ -260,10 +299,10 @@ int enqueue_filter(plomgpu_plan* p) {
   const int R = p->R;
   const size_t RJ = (size_t)R * J;
 
-  PropKernel<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif);
+  const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif);
   if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
-  const size_t smem = propagate_smem_bytes<T, kSmem, kBtProp>();
-  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const size_t smem = kp.smem;
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
   const int n_par = M::N_PAR_PROC * M::N_CAC;
   if (n_par > 0) {
@@ -291,7 +330,7 @@ int enqueue_filter(plomgpu_plan* p) {
   size_t crn_off = 0;
   int cur = 0;           // generation holding the particles before interval n
   int anc_cur = -1;      // ancestors to apply when loading (index into p->anc), -1 = identity
-  const int gprop = (int)((RJ + kBtProp - 1) / kBtProp);
+  const int gprop = (int)((RJ + kp.per_block - 1) / kp.per_block);
   for (int n = 0; n < p->n_obs; ++n) {
     StepArgs a;
     a.n = n;
@@ -315,7 +354,21 @@ int enqueue_filter(plomgpu_plan* p) {
     a.sd_mut = (p->mif && n > 0 && p->weigh[n - 1]) ? p->sd_mut + (size_t)(n - 1) * p->Q : nullptr;
     crn_off += RJ * p->n_sub[n] * D;
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
-    kp<<<gprop, kBtProp, smem, s>>>(tb, a);
+    if (p->ode) {
+      OdeArgs o;
+      o.t0 = p->t_start[n];
+      o.eps_abs = p->eps_abs;
+      o.eps_rel = p->eps_rel;
+      o.max_steps = kOdeMaxSteps;
+      o.cs.meta = p->sp_meta;
+      o.cs.x = p->sp_x;
+      o.cs.y = p->sp_y;
+      o.cs.m2 = p->sp_m2;
+      o.acc = p->acc;
+      k_propagate_ode<T, kBtOde><<<(unsigned)((RJ + kBtOde - 1) / kBtOde), kBtOde, 0, s>>>(tb, a, o);
+    } else {
+      kp.k<<<gprop, kp.bt, smem, s>>>(tb, a);
+    }
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n + 1], s, cudaEventRecordExternal));
     ++kernels;
     cur ^= 1;
@@ -458,6 +511,12 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
     CK(cudaStreamSynchronize(s));
   }
   if ((rc = upload<double>(d->x0, (size_t)M::S, &p->x0, s))) return rc;
+  if (p->ode && M::N_COV_CAC > 0) {
+    if ((rc = upload<int>(d->cov_spline_meta, (size_t)3 * M::N_COV_CAC * M::N_CAC, &p->sp_meta, s))) return rc;
+    if ((rc = upload<double>(d->cov_spline_x, (size_t)d->cov_spline_knots, &p->sp_x, s))) return rc;
+    if ((rc = upload<double>(d->cov_spline_y, (size_t)d->cov_spline_knots, &p->sp_y, s))) return rc;
+    if ((rc = upload<double>(d->cov_spline_m2, (size_t)d->cov_spline_knots, &p->sp_m2, s))) return rc;
+  }
   CK(cudaMalloc((void**)&p->seed, sizeof(uint64_t)));
   CK(cudaMemcpyAsync(p->seed, &d->seed, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   if (d->crn_normals) {
@@ -552,7 +611,7 @@ void plan_free(plomgpu_plan* p) {
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
-                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->data_idx, p->traj_t,
+                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->sp_meta, p->sp_x, p->sp_y, p->sp_m2, p->data_idx, p->traj_t,
                   p->traj_j, p->traj_n, p->traj_x};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -581,6 +640,23 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->want_xpred = want_xpred;
   p->timing = timing;
   p->want_hat = want_hat;
+  p->ode = d->ode != 0;
+  if (p->ode) {
+    if (mif) {
+      delete p;
+      return fail(PLOMGPU_EINVAL, "iterated filtering runs the stochastic implementations only");
+    }
+    if (!(d->eps_abs > 0.0) || !(d->eps_rel >= 0.0)) {
+      delete p;
+      return fail(PLOMGPU_EINVAL, "ode needs eps_abs > 0 and eps_rel >= 0");
+    }
+    if (M::N_COV_CAC > 0 && (!d->cov_spline_meta || !d->cov_spline_x || !d->cov_spline_y || !d->cov_spline_m2)) {
+      delete p;
+      return fail(PLOMGPU_EINVAL, "ode needs the covariate interpolants");
+    }
+    p->eps_abs = d->eps_abs;
+    p->eps_rel = d->eps_rel;
+  }
   if (mif) {
     p->R = mif->n_runs;
     p->mif = true;
@@ -606,6 +682,8 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
       if (!isnan(d->data[(size_t)n * M::N_TS + ts])) any = true;
     p->weigh[n] = (d->filter && any) ? 1 : 0;
   }
+  p->t_start.resize(d->n_obs);
+  for (int n = 0; n < d->n_obs; ++n) p->t_start[n] = d->n_sub[n] > 0 ? d->t_sub[p->sub0[n]] : d->t_obs[n];
   p->sub_total = tot;
   if (p->crn) p->crn_u.assign(d->crn_uniforms, d->crn_uniforms + d->n_obs);
   cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
@@ -669,6 +747,10 @@ int plan_results(plomgpu_plan* p, plomgpu_smc_result* r) {
   r->n_all_fail = p->acc_h->n_all_fail;
   if (p->acc_h->error) {
     r->status = PLOMGPU_ETIMEOUT;
+    if (p->acc_h->error & ERR_ODE) {
+      r->status = PLOMGPU_EINVAL;
+      return fail(PLOMGPU_EINVAL, "ode: integration time step is too small to match the desired precision");
+    }
     return fail(PLOMGPU_ETIMEOUT, (p->acc_h->error & ERR_SCAN_WAIT) ? "cumulative-weight scan wait ran out"
                                                                       : "systematic point table overflow");
   }
@@ -1506,6 +1588,7 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   if (!d || !o || !out) return fail(PLOMGPU_EINVAL, "null argument");
   *out = nullptr;
   if (o->max_J < 1) return fail(PLOMGPU_EINVAL, "max_J must be >= 1");
+  if (d->ode) return fail(PLOMGPU_EINVAL, "the server runs the stochastic implementations only");
   plomgpu_smc_desc chk = *d;
   chk.J = o->max_J;
   chk.crn_normals = nullptr;

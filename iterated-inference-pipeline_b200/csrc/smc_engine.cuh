@@ -24,6 +24,7 @@
 #include <stdint.h>
 #include <type_traits>
 #include "plom_rt.h"
+#include "ode_rkf45.h"
 
 namespace plomgpu {
 
@@ -325,6 +326,157 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   }
 }
 
+// ------------------------------------------------------------------ propagate, one team per particle
+// For models whose state lives in shared memory, a team of TP lanes of one
+// warp advances one particle: the compartment-age classes are split between
+// the team's lanes (M::step_team), so a block holds BT / TP particles and an
+// SM several times more warps than with one thread per particle.  Draws,
+// equations and the order of the incidence and likelihood sums are those of
+// the single-thread kernel up to the association of the team sums.
+template <int TP_>
+struct Team {
+  static constexpr int TP = TP_;
+  int rank;
+  unsigned mask;
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+  // sum over the team, the same butterfly on every lane (identical results)
+  template <class U>
+  __device__ __forceinline__ U sum(U v) const {
+#pragma unroll
+    for (int o = 1; o < TP; o <<= 1) v += __shfl_xor_sync(mask, v, o);
+    return v;
+  }
+};
+
+// Column stride (in words) of the state in shared memory: the smallest
+// stride >= PB that minimises bank conflicts when the TP ranks of the teams
+// of a warp touch compartments G apart (the access pattern of cac_body).
+template <int TP, int G>
+constexpr int team_stride(int PB) {
+  int best = PB, best_deg = 1 << 30;
+  for (int st = PB; st < PB + 32; ++st) {
+    int deg = 0;
+    for (int bank = 0; bank < 32; ++bank) {
+      int cnt = 0;
+      for (int lane = 0; lane < 32; ++lane) {
+        const int t = lane / TP, r = lane % TP;
+        const long addr = (long)r * G * st + t;
+        if ((int)(addr % 32) == bank) ++cnt;
+      }
+      if (cnt > deg) deg = cnt;
+    }
+    if (deg < best_deg) {
+      best_deg = deg;
+      best = st;
+    }
+  }
+  return best;
+}
+
+template <class T, int V, int BT, int TP>
+struct TeamLayout {
+  static constexpr int NW = M::draws_per_cac(V);
+  static constexpr int G = M::draw_group(NW, plomrt::NormalGen<T>::per_block());
+  static constexpr int PB = BT / TP;
+  static constexpr int STRIDE = team_stride<TP, G>(PB);
+  static constexpr size_t pre_bytes = sizeof(typename M::template Pre<T>);
+  static constexpr size_t bytes() {
+    return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) + (size_t)M::S * STRIDE * sizeof(T) + (size_t)PB * pre_bytes +
+           16;
+  }
+};
+
+#ifndef PLOM_TEAM_MIN_BLOCKS
+#define PLOM_TEAM_MIN_BLOCKS 4
+#endif
+
+template <class T, int V, bool DRIFT, bool CRN, int BT, int TP>
+__global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(const Tables<T> tb, const StepArgs a) {
+  typedef TeamLayout<T, V, BT, TP> L;
+  typedef typename M::template Pre<T> PreT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* s_coup = reinterpret_cast<T*>(smem_raw);
+  T* s_par = s_coup + kSmemCoup;
+  T* s_state = s_par + kSmemPar;
+  unsigned char* pre_raw = reinterpret_cast<unsigned char*>(s_state + (size_t)M::S * L::STRIDE);
+  pre_raw += (16 - ((uintptr_t)pre_raw & 15)) & 15;
+  PreT* s_pre = reinterpret_cast<PreT*>(pre_raw);
+  if constexpr (M::COUPLED) {
+    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = tb.coupling[i];
+  }
+  for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
+  __syncthreads();
+  const int J = tb.J;
+  const size_t RJ = (size_t)tb.R * J;
+  const int lp = threadIdx.x / TP;
+  const size_t g = (size_t)blockIdx.x * L::PB + lp;  // particle of all runs
+  if (g >= RJ) return;                               // the whole team leaves together
+  Team<TP> tm;
+  tm.rank = threadIdx.x % TP;
+  tm.mask = (TP == 32) ? 0xffffffffu : (((1u << TP) - 1u) << ((threadIdx.x & 31) & ~(TP - 1)));
+  const int r = (int)(g / J);
+  const int j = (int)(g - (size_t)r * J);
+  const size_t src = (size_t)r * J + (a.anc ? __ldg(a.anc + g) : (uint32_t)j);
+  const T* __restrict__ Xp = (const T*)a.X_prev;
+  T* __restrict__ Xn = (T*)a.X_next;
+  SmemState<T, L::STRIDE> x;
+  x.b = s_state + lp;
+  for (int w = tm.rank; w < M::OFF_INC; w += TP) x[w] = Xp[(size_t)w * RJ + src];
+  for (int w = M::OFF_INC + tm.rank; w < M::S; w += TP) x[w] = T(0);  // reset_inc
+  tm.sync();
+
+  ProcEnv<T> e;
+  e.par_ = s_par;
+  e.coup_ = s_coup;
+  e.dgroup_ = tb.drift_group;
+  e.dng_ = tb.drift_ngroups;
+  e.dbt_ = tb.drift_bt;
+  e.dvol_ = tb.drift_vol;
+  const T dt = (T)tb.dt;
+  const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id + (uint32_t)r);
+  for (int k = 0; k < a.n_sub; ++k) {
+    const int sub = a.sub0 + k;
+    e.cov_ = tb.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
+    const T t = (T)__ldg(tb.t_sub + sub);
+    if constexpr (CRN) {
+      TableDraws<T, V> d;
+      d.p = a.crn + ((size_t)g * a.n_sub + k) * a.crn_d;
+      M::template step_team<V, DRIFT, T>(x, t, dt, e, d, tm, s_pre[lp]);
+    } else {
+      PhiloxDraws<T, V> d;
+      d.key = key;
+      d.j = (uint32_t)j;
+      d.n = (uint32_t)a.n;
+      d.sub = (uint32_t)k;
+      M::template step_team<V, DRIFT, T>(x, t, dt, e, d, tm, s_pre[lp]);
+    }
+  }
+  for (int w = tm.rank; w < M::S; w += TP)
+    if (w < M::OFF_INC || a.write_inc) Xn[(size_t)w * RJ + g] = x[w];
+  if (a.x_hist) {
+    for (int w = tm.rank; w < M::S; w += TP) a.x_hist[(size_t)w * RJ + g] = (double)x[w];
+  }
+  if (a.weigh) {
+    double obs[M::N_TS];
+    M::template proj2obs<T>(x, obs);
+    ObsEnv oe;
+    oe.par_ts_ = tb.par_ts;
+    oe.cov_ts_ = a.cov_ts;
+    double ll = 0.0;
+#pragma unroll
+    for (int ts = 0; ts < M::N_TS; ++ts) {
+      if (ts % TP != tm.rank) continue;
+      const double y = __ldg(a.y + ts);
+      if (isnan(y)) continue;
+      const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
+      const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
+      ll += log(plomrt::disc_normal_like(y, mu, var, tb.like_min));
+    }
+    ll = tm.sum(ll);
+    if (tm.rank == 0) ((T*)a.lw)[g] = (T)ll;
+  }
+}
+
 // ------------------------------------------------------------------ weights
 struct LseAcc {
   double m;   // running max of the surviving log-weights
@@ -376,12 +528,12 @@ struct StepState {
 struct FilterAcc {
   double loglik;
   int n_all_fail;
-  int error;        // bit 0: scan wait ran out; bit 1: systematic table overflow
+  int error;        // bit 0: scan wait ran out; bit 1: systematic table overflow; bit 2: ODE step control failed
   unsigned ticket;  // block ticket of k_weight
   unsigned tile_ticket;
 };
 
-enum { ERR_SCAN_WAIT = 1, ERR_SYS_TABLE = 2 };
+enum { ERR_SCAN_WAIT = 1, ERR_SYS_TABLE = 2, ERR_ODE = 4 };
 
 template <class T>
 __device__ __forceinline__ bool weight_fails(T l, double thresh) {
@@ -747,6 +899,87 @@ __global__ void __launch_bounds__(BT) k_mif_moments(const T* __restrict__ lw, co
     const size_t o = ((size_t)r * n_obs + n) * Q + q;
     bart[o] = a;
     vt[o] = var + vt_add[(size_t)n * Q + q];
+  }
+}
+
+// ------------------------------------------------------------------ deterministic skeleton (ode)
+// Process environment of the ODE right-hand side: covariates come from a
+// per-thread buffer refreshed at every stage time.
+template <class T>
+struct OdeProcEnv : ProcEnv<T> {
+  T* covl_;
+  __device__ __forceinline__ T cov(int k, int cac) const { return covl_[k * M::N_CAC + cac]; }
+};
+
+struct OdeArgs {
+  double t0;          // start of the interval
+  double eps_abs, eps_rel;
+  int max_steps;      // attempted steps per interval before giving up
+  plomrt::CovSplines cs;
+  FilterAcc* acc;     // error flags
+};
+
+// One particle per thread: gather from the ancestor, reset the incidences,
+// integrate the skeleton over [t0, t_obs] with RKF45 (f_prediction_ode,
+// model_builder/C/core/prediction_util.c:176-193), store, weigh.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT) k_propagate_ode(const Tables<T> tb, const StepArgs a, const OdeArgs o) {
+  __shared__ __align__(16) T s_coup[kSmemCoup > 0 ? kSmemCoup : 1];
+  __shared__ __align__(16) T s_par[kSmemPar > 0 ? kSmemPar : 1];
+  if constexpr (M::COUPLED) {
+    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = tb.coupling[i];
+  }
+  for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
+  __syncthreads();
+  const int J = tb.J;
+  const size_t RJ = (size_t)tb.R * J;
+  const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;
+  if (g >= RJ) return;
+  const int r = (int)(g / J);
+  const int j = (int)(g - (size_t)r * J);
+  const size_t src = (size_t)r * J + (a.anc ? __ldg(a.anc + g) : (uint32_t)j);
+  const T* __restrict__ Xp = (const T*)a.X_prev;
+  T* __restrict__ Xn = (T*)a.X_next;
+  T y[M::S];
+  T work[8 * M::S];
+  T covl[M::N_COV_CAC * M::N_CAC > 0 ? M::N_COV_CAC * M::N_CAC : 1];
+  for (int w = 0; w < M::OFF_INC; ++w) y[w] = Xp[(size_t)w * RJ + src];
+  for (int w = M::OFF_INC; w < M::S; ++w) y[w] = T(0);  // reset_inc
+  OdeProcEnv<T> e;
+  e.par_ = s_par;
+  e.coup_ = s_coup;
+  e.cov_ = nullptr;
+  e.dgroup_ = tb.drift_group;
+  e.dng_ = tb.drift_ngroups;
+  e.dbt_ = tb.drift_bt;
+  e.dvol_ = tb.drift_vol;
+  e.covl_ = covl;
+  int steps = 0;
+  const int rc = plomrt::rkf45_interval<M, T>(y, o.t0, a.t_obs, tb.dt, o.eps_abs, o.eps_rel, e, o.cs, work,
+                                              o.max_steps, &steps);
+  if (rc != plomrt::ODE_OK) atomicOr(&o.acc[r].error, (int)ERR_ODE);
+  for (int w = 0; w < M::S; ++w)
+    if (w < M::OFF_INC || a.write_inc) Xn[(size_t)w * RJ + g] = y[w];
+  if (a.x_hist) {
+    for (int w = 0; w < M::S; ++w) a.x_hist[(size_t)w * RJ + g] = (double)y[w];
+  }
+  if (a.weigh) {
+    const plomrt::ArrayView<T> xv{y};
+    double obs[M::N_TS];
+    M::template proj2obs<T>(xv, obs);
+    ObsEnv oe;
+    oe.par_ts_ = tb.par_ts;
+    oe.cov_ts_ = a.cov_ts;
+    double ll = 0.0;
+#pragma unroll
+    for (int ts = 0; ts < M::N_TS; ++ts) {
+      const double yy = __ldg(a.y + ts);
+      if (isnan(yy)) continue;
+      const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
+      const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
+      ll += log(plomrt::disc_normal_like(yy, mu, var, tb.like_min));
+    }
+    ((T*)a.lw)[g] = (T)ll;
   }
 }
 

@@ -148,6 +148,77 @@ struct Model {
       }
     }
   }
+  template <int V, bool DRIFT, class T, class X, class E, class D, class TM>
+  PLOM_HD static void step_team(X& x, const T t, const T dt, const E& e, D& draws, const TM& tm, Pre<T>& pre) {
+    constexpr int NW = draws_per_cac(V);
+    constexpr int G = draw_group(NW, D::PER_BLOCK);
+    constexpr int NG = N_CAC / G;
+    constexpr int NMAIN = NG * G;
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+    PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    PLOM_PRAGMA_CAC
+    for (int gi = tm.rank; gi < NG; gi += TM::TP) {
+      const int cac0 = gi * G;
+      T nz[NW * G > 0 ? NW * G : 1];
+      draws.template normals<NW * G>(cac0, nz);
+      PLOM_UNROLL
+      for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);
+    }
+    for (int cac = NMAIN + tm.rank; cac < N_CAC; cac += TM::TP) {
+      T nz[NW > 0 ? NW : 1];
+      draws.template normals<NW>(cac, nz);
+      cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);
+    }
+    PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = tm.sum(inc_acc[w]);
+    tm.sync();
+    if (tm.rank == 0) {
+      PLOM_UNROLL
+      for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {
+        const T f = x[OFF_INC+w] + inc_acc[w];
+        x[OFF_INC+w] = (f < T(0)) ? T(0) : f;
+      }
+    }
+    if (DRIFT) {
+      for (int i = 0; i < N_DRIFT; ++i) {
+        const int ng = e.drift_ngroups(i);
+        for (int g = tm.rank; g < ng; g += TM::TP)
+          x[OFF_DRIFT+i*N_CAC+g] += e.drift_vol(i, g)*sqrt(dt)*draws.drift_normal(i, g);
+      }
+    }
+    tm.sync();
+  }
+  template <class T, class X, class F, class E>
+  PLOM_HD static void deriv(const X& x, F& f, const T t, const E& e) {
+    (void)t;
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    Pre<T> pre;
+    pre.unused = 0;
+    for (int cac = 0; cac < N_CAC; ++cac) {
+      const T xo_S = x[0*N_CAC+cac];
+      const T xo_I = x[1*N_CAC+cac];
+      const T drift_0 = e.par(0, cac);
+      const T r0 = e.cov(0, cac)*e.cov(1, cac);
+      const T r1 = xo_I*drift_0*e.par(1, cac)/e.cov(0, cac);
+      const T r2 = e.par(1, cac);
+      const T r3 = e.cov(2, cac);
+      const T incterm_0 = + (r2*xo_I) + (r3*xo_I);
+      const T incterm_1 = + (r1*xo_S);
+      f[0*N_CAC+cac] = - (r1*xo_S) - (r3*xo_S) + (r0);
+      f[1*N_CAC+cac] = - (r2*xo_I) - (r3*xo_I) + (r1*xo_S);
+      for (int k = 0; k < INC_PER_CAC; ++k) {
+        const int l = inc_link(cac, k);
+        if (l < 0) break;
+        const int o = l >> 10, w = l & 1023;
+        if (o == 0) inc_acc[w] += incterm_0;
+        if (o == 1) inc_acc[w] += incterm_1;
+      }
+    }
+    for (int w = OFF_DRIFT; w < OFF_INC; ++w) f[w] = T(0);
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];
+  }
   template <class T, class X>
   PLOM_HD static void proj2obs(const X& x, double* obs) {
     obs[0] = (double)x[OFF_INC+0];

@@ -123,7 +123,8 @@ def make_problem(model, settings, theta, args, J=None, filter=True):
     dt = args.DT
     return Problem(model, settings, theta, J=J or args.J, dt=dt, nb_obs=args.nb_obs, like_min=args.LIKE_MIN,
                    noises_off=noises_off_of(args), filter=filter, seed=seed, precision=args.precision,
-                   freeze_forcing=args.freeze_forcing)
+                   freeze_forcing=args.freeze_forcing, ode=(args.implementation == 'ode'),
+                   eps_abs=args.eps_abs, eps_rel=args.eps_rel)
 
 
 # ---------------------------------------------------------------- output formats

@@ -279,6 +279,7 @@ class Emitter(object):
         a('  static constexpr int N_INC_LINKS = %d;' % self._n_inc_links())
         self._emit_inc_tables(a)
         self._emit_step(a, caches, ode, inc)
+        self._emit_deriv(a, caches, ode, inc)
         self._emit_proj2obs(a)
         self._emit_obs(a)
         a('};')
@@ -457,6 +458,113 @@ class Emitter(object):
         a('        }')
         a('      }')
         a('    }')
+        a('  }')
+        self._emit_step_team(a, foi_states)
+
+    def _emit_step_team(self, a, foi_states):
+        """The substep of one particle shared by a team of TM::TP threads.
+
+        Team member `rank` takes the draw groups rank, rank + TP, ... (the same
+        Philox blocks as the single-thread step, so the same draws); the
+        coupling terms of the substep start are written by the team into the
+        particle's shared-memory Pre; incidence partial sums are reduced over the
+        team in a fixed order (TM::sum) and applied by rank 0; drift groups are
+        split by rank.  Team barriers (TM::sync) separate the reads of the
+        substep-start state from its updates.
+        """
+        m = self.m
+        a('  template <int V, bool DRIFT, class T, class X, class E, class D, class TM>')
+        a('  PLOM_HD static void step_team(X& x, const T t, const T dt, const E& e, D& draws, const TM& tm, Pre<T>& pre) {')
+        a('    constexpr int NW = draws_per_cac(V);')
+        a('    constexpr int G = draw_group(NW, D::PER_BLOCK);')
+        a('    constexpr int NG = N_CAC / G;')
+        a('    constexpr int NMAIN = NG * G;')
+        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
+        a('    PLOM_UNROLL')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        for s_ in foi_states:
+            si = m.par_sv.index(s_)
+            a('    for (int c2 = tm.rank; c2 < N_CAC; c2 += TM::TP) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;'
+              % (s_, si, self._npop_expr('c2')))
+        if foi_states:
+            a('    tm.sync();')
+        a('    PLOM_PRAGMA_CAC')
+        a('    for (int gi = tm.rank; gi < NG; gi += TM::TP) {')
+        a('      const int cac0 = gi * G;')
+        a('      T nz[NW * G > 0 ? NW * G : 1];')
+        a('      draws.template normals<NW * G>(cac0, nz);')
+        a('      PLOM_UNROLL')
+        a('      for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);')
+        a('    }')
+        a('    for (int cac = NMAIN + tm.rank; cac < N_CAC; cac += TM::TP) {')
+        a('      T nz[NW > 0 ? NW : 1];')
+        a('      draws.template normals<NW>(cac, nz);')
+        a('      cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);')
+        a('    }')
+        a('    PLOM_UNROLL')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = tm.sum(inc_acc[w]);')
+        a('    tm.sync();')
+        a('    if (tm.rank == 0) {')
+        a('      PLOM_UNROLL')
+        a('      for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {')
+        a('        const T f = x[OFF_INC+w] + inc_acc[w];')
+        a('        x[OFF_INC+w] = (f < T(0)) ? T(0) : f;')
+        a('      }')
+        a('    }')
+        a('    if (DRIFT) {')
+        a('      for (int i = 0; i < N_DRIFT; ++i) {')
+        a('        const int ng = e.drift_ngroups(i);')
+        a('        for (int g = tm.rank; g < ng; g += TM::TP)')
+        a('          x[OFF_DRIFT+i*N_CAC+g] += e.drift_vol(i, g)*sqrt(dt)*draws.drift_normal(i, g);')
+        a('      }')
+        a('    }')
+        a('    tm.sync();')
+        a('  }')
+
+    def _emit_deriv(self, a, caches, ode, inc):
+        """Right-hand side of the deterministic skeleton (step_ode,
+        model_builder/C/templates/core_template.c:215-339 with noises_off == 'ode'):
+        f = dX/dt for the compartment words, the incidence words, and zero for the
+        drift words (drifted parameters take their table values)."""
+        m = self.m
+        foi_states = sorted(set(self._foi_states()))
+        a('  template <class T, class X, class F, class E>')
+        a('  PLOM_HD static void deriv(const X& x, F& f, const T t, const E& e) {')
+        a('    (void)t;')
+        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        a('    Pre<T> pre;')
+        a('    pre.unused = 0;')
+        for s_ in foi_states:
+            si = m.par_sv.index(s_)
+            a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
+        a('    for (int cac = 0; cac < N_CAC; ++cac) {')
+        for i, s_ in enumerate(m.par_sv):
+            a('      const T xo_%s = x[%d*N_CAC+cac];' % (s_, i))
+        for k, p_ in enumerate(self.drift):
+            a('      const T drift_%d = e.par(%d, cac);' % (k, m.par_proc.index(p_)))
+        for s_ in foi_states:
+            a('      T foi_%s = T(0);' % s_)
+            a('      for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * pre.yf_%s[c2];' % (s_, s_))
+        for k, c in enumerate(caches):
+            a('      const T r%d = %s;' % (k, c))
+        for o, eq in enumerate(inc):
+            rhs = ' '.join('%s (%s)' % (d['sign'], d['term']) for d in eq) or '0'
+            a('      const T incterm_%d = %s;' % (o, rhs))
+        for i, s_ in enumerate(m.par_sv):
+            rhs = ' '.join('%s (%s)' % (d['sign'], d['term']) for d in ode[s_]) or '0'
+            a('      f[%d*N_CAC+cac] = %s;' % (i, rhs))
+        if inc:
+            a('      for (int k = 0; k < INC_PER_CAC; ++k) {')
+            a('        const int l = inc_link(cac, k);')
+            a('        if (l < 0) break;')
+            a('        const int o = l >> 10, w = l & 1023;')
+            for o in range(len(inc)):
+                a('        if (o == %d) inc_acc[w] += incterm_%d;' % (o, o))
+            a('      }')
+        a('    }')
+        a('    for (int w = OFF_DRIFT; w < OFF_INC; ++w) f[w] = T(0);')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];')
         a('  }')
 
     def _foi_states(self):

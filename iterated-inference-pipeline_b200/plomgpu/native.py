@@ -42,7 +42,9 @@ class SmcDesc(C.Structure):
                 ('cov_ts', _dp), ('coupling', _dp), ('drift_group', _ip), ('drift_ngroups', _ip),
                 ('drift_bt', _P(BackTransform)), ('drift_vol', _dp), ('x0', _dp), ('noises_off', C.c_int),
                 ('filter', C.c_int), ('like_min', C.c_double), ('seed', C.c_uint64), ('precision', C.c_int),
-                ('crn_normals', _dp), ('crn_uniforms', _dp), ('pop_size', _dp), ('cov_ts0', _dp)]
+                ('crn_normals', _dp), ('crn_uniforms', _dp), ('pop_size', _dp), ('cov_ts0', _dp),
+                ('ode', C.c_int), ('eps_abs', C.c_double), ('eps_rel', C.c_double), ('cov_spline_meta', _ip),
+                ('cov_spline_x', _dp), ('cov_spline_y', _dp), ('cov_spline_m2', _dp), ('cov_spline_knots', C.c_int)]
 
 
 class BatchDesc(C.Structure):
@@ -141,6 +143,21 @@ class DescHolder(object):
             like_min=p.like_min, seed=p.seed, precision=precision or p.precision,
             crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp), pop_size=_ptr(pop, _dp),
             cov_ts0=_ptr(cts0, _dp))
+        if getattr(p, 'ode', False):
+            meta, xs, ys, m2 = p.spline_tables()
+            meta = keep('sp_meta', meta if meta.size else np.zeros(3, np.int32), np.int32)
+            xs = keep('sp_x', xs if xs.size else np.zeros(1), np.float64)
+            ys = keep('sp_y', ys if ys.size else np.zeros(1), np.float64)
+            m2 = keep('sp_m2', m2 if m2.size else np.zeros(1), np.float64)
+            d = self.desc
+            d.ode = 1
+            d.eps_abs = p.eps_abs
+            d.eps_rel = p.eps_rel
+            d.cov_spline_meta = _ptr(meta, _ip)
+            d.cov_spline_x = _ptr(xs, _dp)
+            d.cov_spline_y = _ptr(ys, _dp)
+            d.cov_spline_m2 = _ptr(m2, _dp)
+            d.cov_spline_knots = int(xs.size)
 
 
 class Outputs(object):

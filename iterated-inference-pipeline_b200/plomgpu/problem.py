@@ -93,7 +93,8 @@ class Problem(object):
     """Everything one filter needs, as numpy arrays in the descriptor layout."""
 
     def __init__(self, model, settings, theta, J=1000, dt=1.0, nb_obs=-1, like_min=1e-17,
-                 noises_off=0, filter=True, seed=2, precision=32, u_data='D', freeze_forcing=-1.0):
+                 noises_off=0, filter=True, seed=2, precision=32, u_data='D', freeze_forcing=-1.0,
+                 ode=False, eps_abs=1e-6, eps_rel=1e-3):
         if not isinstance(model, PlomModel):
             raise TypeError('model must be a PlomModel')
         m = self.model = model
@@ -105,6 +106,12 @@ class Problem(object):
         self.seed = int(seed)
         self.precision = int(precision)
         self.dt = round_dt(dt)
+        # deterministic skeleton integrated with step control (the "ode" implementation)
+        self.ode = bool(ode)
+        self.eps_abs = float(eps_abs)
+        self.eps_rel = float(eps_rel)
+        if self.ode:
+            self.noises_off = 7
         data = settings['data']
         times = data['times']
         rows = data['data']
@@ -167,6 +174,20 @@ class Problem(object):
             c = sp(min(freeze_forcing, x[-1]))
             return Spline([x[0]], [c])
         return Spline(x, y)
+
+    def spline_tables(self):
+        """(meta [n_cov_cac * N_CAC][3], x, y, m2): the interpolants of the process covariates for
+        the ODE integrator (kind 0 constant, 1 linear, 2 natural cubic; knots, offset)."""
+        meta, xs, ys, ms = [], [], [], []
+        kinds = {'const': 0, 'linear': 1, 'cspline': 2}
+        for per_cac in self.splines_cac:
+            for sp in per_cac:
+                meta.append((kinds[sp.kind], len(sp.x), len(xs)))
+                xs.extend(sp.x.tolist())
+                ys.extend(sp.y.tolist())
+                ms.extend(sp.m.tolist() if sp.kind == 'cspline' else [0.0] * len(sp.x))
+        return (np.array(meta, dtype=np.int32).reshape(-1, 3), np.array(xs, dtype=float),
+                np.array(ys, dtype=float), np.array(ms, dtype=float))
 
     def set_theta(self, theta, u_data='D'):
         self.theta = theta

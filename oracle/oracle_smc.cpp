@@ -28,6 +28,7 @@
 // would read past the end of prob[]).
 #include PLOM_MODEL_HEADER
 #include "plomgpu.h"
+#include "ode_rkf45.h"
 
 #include <algorithm>
 #include <math.h>
@@ -72,6 +73,34 @@ struct HostEnv {
     return plomrt::back_transform<double>(xw, bt);
   }
 };
+
+// the ODE right-hand side reads its covariates from a buffer refreshed at
+// every stage time (plomrt::rkf45_interval)
+struct HostOdeEnv : HostEnv {
+  double* covl_;
+  double cov(int k, int cac) const { return covl_[k * M::N_CAC + cac]; }
+};
+
+// Deterministic skeleton over interval n (f_prediction_ode restated by
+// plomrt::rkf45_interval, the integrator the GPU engine uses).
+int ode_propagate(double* x, const plomgpu_smc_desc* d, int n, int sub0) {
+  HostOdeEnv e;
+  e.par_ = d->par_cac;
+  e.cov_ = nullptr;
+  e.coup_ = d->coupling;
+  e.dgroup_ = d->drift_group;
+  e.dng_ = d->drift_ngroups;
+  e.dbt_ = d->drift_bt;
+  e.dvol_ = d->drift_vol;
+  std::vector<double> covl(M::N_COV_CAC * M::N_CAC > 0 ? M::N_COV_CAC * M::N_CAC : 1);
+  e.covl_ = covl.data();
+  plomrt::CovSplines cs{d->cov_spline_meta, d->cov_spline_x, d->cov_spline_y, d->cov_spline_m2};
+  std::vector<double> work(8 * M::S);
+  const double t0 = d->n_sub[n] > 0 ? d->t_sub[sub0] : d->t_obs[n];
+  int steps = 0;
+  return plomrt::rkf45_interval<M, double>(x, t0, d->t_obs[n], d->dt, d->eps_abs, d->eps_rel, e, cs, work.data(),
+                                           1000000, &steps);
+}
 
 struct HostObsEnv {
   const double* par_ts_;
@@ -382,13 +411,13 @@ int oracle_model_info(plomgpu_model_info* o) {
 
 int oracle_draws_per_substep(int noises_off) { return draws_per_substep(noises_off); }
 
-// run_SMC restated.  n_threads <= 0: OpenMP default.
 // get_CI95 on given values and weights (null: 1/J), known-answer tests.
 void oracle_ci95(const double* v, const double* w, int J, double* lo, double* hi) {
   std::vector<double> vv(v, v + J);
   ci95(vv, w, J, lo, hi);
 }
 
+// run_SMC restated.  n_threads <= 0: OpenMP default.
 int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threads) {
   const int J = d->J, S = M::S;
   if (J < 1 || d->precision != 64 && d->precision != 32) return PLOMGPU_EINVAL;
@@ -396,6 +425,7 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
   if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
   const PropFn prop = pick(d->noises_off);
+  int ode_fail = 0;
   const int D = d->crn_normals ? draws_per_substep(d->noises_off) : 0;
   // AoS particles: proj[S] per particle, two generations
   std::vector<double> X((size_t)J * S), Xn((size_t)J * S);
@@ -421,7 +451,11 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
       double* x = &Xn[(size_t)j * S];
       memcpy(x, &X[(size_t)j * S], sizeof(double) * S);
       for (int w = M::OFF_INC; w < S; ++w) x[w] = 0.0;  // reset_inc
-      prop(x, d, n, j, sub0, crn_n, D);
+      if (d->ode) {
+        if (ode_propagate(x, d, n, sub0) != plomrt::ODE_OK) ode_fail = 1;
+      } else {
+        prop(x, d, n, j, sub0, crn_n, D);
+      }
       if (n_nonan) wts[j] = exp(log_likelihood(x, d, n));
     }
     if (r->x_pred) {
@@ -468,8 +502,8 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
   }
   r->loglik = Llike;
   r->n_all_fail = n_all_fail;
-  r->status = 0;
-  return 0;
+  r->status = ode_fail ? PLOMGPU_EINVAL : 0;
+  return ode_fail ? PLOMGPU_EINVAL : 0;
 }
 
 // weight() + systematic_sampling() on given likelihoods (known-answer tests).

@@ -19,15 +19,27 @@ pytestmark = pytest.mark.gpu
 PKG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'iterated-inference-pipeline_b200')
 
 
-@pytest.fixture(scope='module')
-def model_dir(tmp_path_factory):
+def _model_dir(tmp_path_factory, name):
     from plomgpu import build
-    c, p, l, th = models.files('noise')
-    d = str(tmp_path_factory.mktemp('cli') / 'noise')
-    build.build_model_dir(c, p, l, d, name='noise', shared_lib=True)
+    c, p, l, th = models.files(name)
+    if name == 'sir':  # fit r0 and v
+        for k in ('r0', 'v'):
+            th['parameter'][k]['sd_transf'] = 0.1
+    d = str(tmp_path_factory.mktemp('cli') / name)
+    build.build_model_dir(c, p, l, d, name=name, shared_lib=True)
     with open(os.path.join(d, 'theta.json'), 'w') as f:
         f.write(json.dumps(th) + '\n')
     return d
+
+
+@pytest.fixture(scope='module')
+def model_dir(tmp_path_factory):
+    return _model_dir(tmp_path_factory, 'noise')
+
+
+@pytest.fixture(scope='module')
+def sir_dir(tmp_path_factory):
+    return _model_dir(tmp_path_factory, 'sir')
 
 
 def _run(d, cmd, *args):
@@ -84,8 +96,9 @@ def test_pmcmc_cli_outputs(model_dir):
     assert json.load(open(os.path.join(d, '.done_7.json')))['parameter']
 
 
-def test_mif_cli_outputs(model_dir):
-    d = model_dir
+def test_mif_cli_outputs(sir_dir):
+    """MIF fits parameters that take one value for every population (the SIR workload)."""
+    d = sir_dir
     _run(d, 'mif', 'sde', '-J', '300', '-s', '1', '-M', '3', '-i', '9', '-r')
     head, rows = _csv(os.path.join(d, 'trace_9.csv'))
     assert len(rows) == 4 and rows[0][-1] == 'nan'

@@ -199,3 +199,30 @@ def test_fp32_precision_bias_with_common_draws():
     diffs = np.array(diffs)
     assert abs(diffs.mean()) < 0.25
     assert np.median(np.abs(diffs)) < 0.5
+
+
+@pytest.mark.parametrize('noises_off', [0, 3])
+def test_crn_parity_team_kernel(noises_off):
+    """seir20x2 (180 state words in shared memory, one team of lanes per particle) against the
+    oracle with common draws, FP64: trajectories, ancestors, log-likelihood."""
+    eng = models.engine('seir20x2')
+    orc = models.build_oracle('seir20x2')
+    p = models.make_problem('seir20x2', J=300, dt=1.0, noises_off=noises_off, precision=64, seed=11, nb_obs=30)
+    D = eng.draws_per_substep(noises_off)
+    z, u = crn_draws(p, D, 77)
+    g = eng.smc(p, crn_normals=z, crn_uniforms=u, ancestors=True, x_pred=True)
+    o = orc.smc(p, crn_normals=z, crn_uniforms=u, ancestors=True, x_pred=True)
+    np.testing.assert_array_equal(g.ancestors, o.ancestors)
+    np.testing.assert_allclose(g.x_pred, o.x_pred, rtol=1e-6, atol=1e-9)
+    assert g.loglik == pytest.approx(o.loglik, rel=1e-9)
+
+
+def test_philox_fp64_team_kernel_matches_oracle():
+    """The team kernel consumes the same Philox blocks as the single-thread oracle (FP64)."""
+    eng = models.engine('seir20x2')
+    orc = models.build_oracle('seir20x2')
+    p = models.make_problem('seir20x2', J=200, dt=1.0, precision=64, seed=5, nb_obs=20)
+    g = eng.smc(p, ancestors=True)
+    o = orc.smc(p, ancestors=True)
+    np.testing.assert_array_equal(g.ancestors, o.ancestors)
+    assert g.loglik == pytest.approx(o.loglik, rel=1e-9)
