@@ -123,6 +123,12 @@ typedef struct plomgpu_smc_desc {
     const double *cov_spline_y;
     const double *cov_spline_m2;
     int cov_spline_knots;
+    /* 1: Poisson system with stochastic rates, the reference's default "psr"
+     * implementation (step_psr, model_builder/C/templates/core_template.c:
+     * 105-209): multinomial splits of the integer compartments, Poisson
+     * arrivals, Gamma white noise (off with PLOMGPU_NO_ENV_STO; the
+     * demographic flag has no effect).  Philox draws only. */
+    int psr;
 } plomgpu_smc_desc;
 
 typedef struct plomgpu_smc_result {

@@ -42,9 +42,12 @@ int fail(int code, const std::string& msg) {
 constexpr bool kSmem = (M::S > 48);
 constexpr int kBtProp = 128;
 // lanes per particle of the team kernel (state in shared memory); 1 = one
-// thread per particle
+// thread per particle.  One thread per particle is the default: on SEIR 20x2
+// (J = 1e5) it measured 1.02 ms per interval against 1.26 / 1.80 / 2.96 ms
+// for teams of 2 / 4 / 8 lanes (the team's shared coupling terms and
+// barriers cost more than the extra warps recover).
 #ifndef PLOM_TEAM
-#define PLOM_TEAM 4
+#define PLOM_TEAM 1
 #endif
 constexpr int kTeam = kSmem ? PLOM_TEAM : 1;
 constexpr int kBtOde = 64;
@@ -138,6 +141,7 @@ struct plomgpu_plan {
   double* pop = nullptr;       // [n_obs + 1][N_CAC]
   double* cov_ts0 = nullptr;   // [N_COV_TS][N_TS] at time 0
   double hat_rank[2] = {1.0, 1.0};  // quantile ranks under equal weights
+  bool psr = false;  // Poisson system with stochastic rates
   // deterministic skeleton
   bool ode = false;
   double eps_abs = 1e-6, eps_rel = 1e-3;
@@ -205,10 +209,15 @@ struct PropLaunch {
   explicit operator bool() const { return k != nullptr; }
 };
 
-template <class T, int V, bool DRIFT, bool CRN, bool MIF>
+template <class T, int V, bool DRIFT, bool CRN, bool MIF, bool PSR = false>
 PropLaunch<T> pick4() {
   PropLaunch<T> l;
-  if constexpr (kTeam > 1 && !MIF) {
+  if constexpr (PSR) {
+    l.k = &k_propagate<T, V, DRIFT, false, kSmem, false, kBtProp, true>;
+    l.bt = kBtProp;
+    l.per_block = kBtProp;
+    l.smem = propagate_smem_bytes<T, kSmem, kBtProp>();
+  } else if constexpr (kTeam > 1 && !MIF) {
     typedef TeamLayout<T, V, kBtProp, kTeam> L;
     l.k = &k_propagate_team<T, V, DRIFT, CRN, kBtProp, kTeam>;
     l.bt = kBtProp;
@@ -243,8 +252,24 @@ PropLaunch<T> pick_v(int v, bool drift) {
   }
 }
 
+// the Poisson-system step: white noise on / off, drift on / off
 template <class T>
-PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif) {
+PropLaunch<T> pick_psr(int noises_off) {
+  const bool noenv = (noises_off & PLOMGPU_NO_ENV_STO) != 0;
+  if (drift_on(noises_off)) {
+    if constexpr (M::N_DRIFT > 0) {
+      return noenv ? pick4<T, 2, true, false, false, true>() : pick4<T, 0, true, false, false, true>();
+    }
+  }
+  return noenv ? pick4<T, 2, false, false, false, true>() : pick4<T, 0, false, false, false, true>();
+}
+
+template <class T>
+PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif, bool psr = false) {
+  if (psr) {
+    if (crn || mif) return PropLaunch<T>();
+    return pick_psr<T>(noises_off);
+  }
   const int v = variant_of(noises_off);
   const bool d = drift_on(noises_off);
   if (mif) {
@@ -299,7 +324,7 @@ int enqueue_filter(plomgpu_plan* p) {
   const int R = p->R;
   const size_t RJ = (size_t)R * J;
 
-  const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif);
+  const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif, p->psr);
   if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
   const size_t smem = kp.smem;
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -641,6 +666,11 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->timing = timing;
   p->want_hat = want_hat;
   p->ode = d->ode != 0;
+  p->psr = d->psr != 0;
+  if (p->psr && (p->ode || p->crn || mif)) {
+    delete p;
+    return fail(PLOMGPU_EINVAL, "psr runs with Philox draws, without ode, common random numbers or iterated filtering");
+  }
   if (p->ode) {
     if (mif) {
       delete p;
@@ -1588,7 +1618,7 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   if (!d || !o || !out) return fail(PLOMGPU_EINVAL, "null argument");
   *out = nullptr;
   if (o->max_J < 1) return fail(PLOMGPU_EINVAL, "max_J must be >= 1");
-  if (d->ode) return fail(PLOMGPU_EINVAL, "the server runs the stochastic implementations only");
+  if (d->ode || d->psr) return fail(PLOMGPU_EINVAL, "the server runs the sde implementation only");
   plomgpu_smc_desc chk = *d;
   chk.J = o->max_J;
   chk.crn_normals = nullptr;

@@ -1,0 +1,228 @@
+// Samplers of the Poisson-system-with-stochastic-rates step (the reference's
+// default ``psr`` implementation, model_builder/C/templates/core_template.c:
+// 105-209): binomial and multinomial splits of a compartment, Poisson
+// arrivals, Gamma white noise.  The reference draws them with GSL
+// (gsl_ran_binomial, gsl_ran_poisson, gsl_ran_gamma on mt19937); here they
+// are exact samplers from published methods, fed by a counter-based Philox
+// stream so that the GPU and the oracle draw the same numbers:
+//
+// * binomial: inversion of the CDF when n·min(p, 1-p) < 14, otherwise BTRD,
+//   the transformed rejection with decomposition of W. Hörmann, "The
+//   generation of binomial random variates", J. Statist. Comput. Simul. 46
+//   (1993);
+// * Poisson: inversion when mu < 10, otherwise PTRS, the transformed
+//   rejection with squeeze of W. Hörmann, "The transformed rejection method
+//   for generating Poisson random variables", Insurance: Mathematics and
+//   Economics 12 (1993);
+// * Gamma: G. Marsaglia and W. W. Tsang, "A simple method for generating
+//   gamma variables", ACM TOMS 26 (2000), with the boost U^(1/a) for a < 1;
+// * multinomial: sequential conditional binomials (plom_ran_multinomial,
+//   model_builder/C/core/prediction_util.c:327-345).
+//
+// Everything is computed in double whatever the state precision.
+#pragma once
+
+#include "plom_rt.h"
+
+namespace plomrt {
+
+enum { STREAM_PSR = 4 };
+
+// Uniforms of one (particle, interval, substep, cac) group: Philox counter
+// (x = particle slot, y = interval, z = substep * (N_CAC + 1) + cac,
+// w = STREAM_PSR + 16 * block); two 53-bit uniforms per block.
+struct UniformStream {
+  PhiloxKey key;
+  uint32_t j, n, group;
+  uint32_t block;
+  double cache;
+  bool has;
+  PLOM_HD void init(PhiloxKey k, uint32_t j_, uint32_t n_, uint32_t group_) {
+    key = k;
+    j = j_;
+    n = n_;
+    group = group_;
+    block = 0;
+    has = false;
+    cache = 0.0;
+  }
+  // uniform in (0, 1)
+  PLOM_HD double next() {
+    if (has) {
+      has = false;
+      return cache;
+    }
+    const U4 c = {j, n, group, (uint32_t)STREAM_PSR + (block << 4)};
+    ++block;
+    const U4 r = philox4x32_10(c, key.k0, key.k1);
+    cache = u01d(r.z, r.w);
+    has = true;
+    return u01d(r.x, r.y);
+  }
+  PLOM_HD double normal() {
+    const double u1 = next(), u2 = next();
+    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+  }
+};
+
+// log k! - Stirling's approximation of it (the correction term of BTRD)
+PLOM_HD double stirling_correction(double k) {
+  if (k < 10.0) return lgamma(k + 1.0) - ((k + 0.5) * log(k + 1.0) - (k + 1.0) + 0.9189385332046728);
+  const double r = 1.0 / (k + 1.0), r2 = r * r;
+  return (1.0 / 12.0 - (1.0 / 360.0 - (1.0 / 1260.0) * r2) * r2) * r;
+}
+
+// bound on rejection rounds: far beyond any realistic count (the expected
+// number is below 2); a sampler that reaches it returns its mode
+constexpr int kMaxRejection = 1000;
+
+PLOM_HD double binomial_inversion(UniformStream& rs, double n, double p) {
+  const double q = 1.0 - p;
+  const double s = p / q, a = (n + 1.0) * s;
+  const double r0 = pow(q, n);
+  for (int round = 0; round < kMaxRejection; ++round) {
+    double u = rs.next(), r = r0, x = 0.0;
+    while (u > r) {
+      u -= r;
+      x += 1.0;
+      if (x > n) break;
+      r *= (a / x - s);
+    }
+    if (x <= n) return x;
+  }
+  return floor(n * p);
+}
+
+PLOM_HD double binomial_btrd(UniformStream& rs, double n, double p) {
+  const double q = 1.0 - p;
+  const double spq = sqrt(n * p * q);
+  const double b = 1.15 + 2.53 * spq;
+  const double a = -0.0873 + 0.0248 * b + 0.01 * p;
+  const double c = n * p + 0.5;
+  const double vr = 0.92 - 4.2 / b;
+  const double alpha = (2.83 + 5.1 / b) * spq;
+  const double m = floor((n + 1.0) * p);
+  const double r = p / q, nr = (n + 1.0) * r, npq = n * p * q;
+  for (int round = 0; round < kMaxRejection; ++round) {
+    double v = rs.next();
+    double u;
+    if (v <= 0.86 * vr) {
+      u = v / vr - 0.43;
+      return floor((2.0 * a / (0.5 - fabs(u)) + b) * u + c);
+    }
+    if (v >= vr) {
+      u = rs.next() - 0.5;
+    } else {
+      u = v / vr - 0.93;
+      u = ((u > 0.0) ? 0.5 : -0.5) - u;
+      v = rs.next() * vr;
+    }
+    const double us = 0.5 - fabs(u);
+    const double k = floor((2.0 * a / us + b) * u + c);
+    if (k < 0.0 || k > n) continue;
+    v = v * alpha / (a / (us * us) + b);
+    const double km = fabs(k - m);
+    if (km <= 15.0) {
+      // recursive evaluation of f(k) / f(m)
+      double f = 1.0;
+      if (m < k) {
+        for (double i = m + 1.0; i <= k; i += 1.0) f *= (nr / i - r);
+      } else if (m > k) {
+        for (double i = k + 1.0; i <= m; i += 1.0) v *= (nr / i - r);
+      }
+      if (v <= f) return k;
+      continue;
+    }
+    // squeeze
+    v = log(v);
+    const double rho = (km / npq) * (((km / 3.0 + 0.625) * km + 1.0 / 6.0) / npq + 0.5);
+    const double t = -km * km / (2.0 * npq);
+    if (v < t - rho) return k;
+    if (v > t + rho) continue;
+    const double nm = n - m + 1.0;
+    const double h = (m + 0.5) * log((m + 1.0) / (r * nm)) + stirling_correction(m) + stirling_correction(n - m);
+    const double nk = n - k + 1.0;
+    if (v <= h + (n + 1.0) * log(nm / nk) + (k + 0.5) * log(nk * r / (k + 1.0)) - stirling_correction(k) -
+                 stirling_correction(n - k))
+      return k;
+  }
+  return m;
+}
+
+// Binomial(n, p), n a non-negative integer held in a double
+PLOM_HD double binomial(UniformStream& rs, double n, double p) {
+  if (n <= 0.0 || !(p > 0.0)) return 0.0;
+  if (p >= 1.0) return n;
+  const bool flip = p > 0.5;  // sample the smaller tail
+  const double pp = flip ? 1.0 - p : p;
+  const double x = (n * pp < 14.0) ? binomial_inversion(rs, n, pp) : binomial_btrd(rs, n, pp);
+  return flip ? n - x : x;
+}
+
+PLOM_HD double poisson(UniformStream& rs, double mu) {
+  if (!(mu > 0.0)) return 0.0;
+  if (mu < 10.0) {
+    for (int round = 0; round < kMaxRejection; ++round) {
+      double u = rs.next(), p = exp(-mu), x = 0.0;
+      while (u > p) {
+        u -= p;
+        x += 1.0;
+        p *= mu / x;
+        if (x > 1000.0) break;
+      }
+      if (x <= 1000.0) return x;
+    }
+    return floor(mu);
+  }
+  const double smu = sqrt(mu);
+  const double b = 0.931 + 2.53 * smu;
+  const double a = -0.059 + 0.02483 * b;
+  const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
+  const double vr = 0.9277 - 3.6224 / (b - 2.0);
+  const double lmu = log(mu);
+  for (int round = 0; round < kMaxRejection; ++round) {
+    const double u = rs.next() - 0.5;
+    const double v = rs.next();
+    const double us = 0.5 - fabs(u);
+    const double k = floor((2.0 * a / us + b) * u + mu + 0.43);
+    if (us >= 0.07 && v <= vr) return k;
+    if (k < 0.0 || (us < 0.013 && v > us)) continue;
+    if (log(v) + log(inv_alpha) - log(a / (us * us) + b) <= -mu + k * lmu - lgamma(k + 1.0)) return k;
+  }
+  return floor(mu);
+}
+
+// Gamma with shape a and scale theta
+PLOM_HD double gamma(UniformStream& rs, double a, double theta) {
+  if (!(a > 0.0) || !(theta > 0.0)) return 0.0;
+  double boost = 1.0;
+  if (a < 1.0) {
+    boost = pow(rs.next(), 1.0 / a);
+    a += 1.0;
+  }
+  const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
+  for (int round = 0; round < kMaxRejection; ++round) {
+    const double z = rs.normal();
+    double v = 1.0 + c * z;
+    if (v <= 0.0) continue;
+    v = v * v * v;
+    const double u = rs.next();
+    if (u < 1.0 - 0.0331 * z * z * z * z) return d * v * theta * boost;
+    if (log(u) < 0.5 * z * z + d * (1.0 - v + log(v))) return d * v * theta * boost;
+  }
+  return d * theta * boost;
+}
+
+// plom_ran_multinomial: K categories with probabilities p summing to one,
+// N trials; out[k] = counts
+template <int K>
+PLOM_HD void multinomial(UniformStream& rs, double N, const double (&p)[K], double (&out)[K]) {
+  double sum_p = 0.0, sum_n = 0.0;
+  for (int k = 0; k < K; ++k) {
+    out[k] = (p[k] > 0.0) ? binomial(rs, N - sum_n, p[k] / (1.0 - sum_p)) : 0.0;
+    sum_p += p[k];
+    sum_n += out[k];
+  }
+}
+
+}  // namespace plomrt

@@ -190,7 +190,10 @@ constexpr size_t propagate_smem_bytes() {
   return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) + (SMEM ? (size_t)M::S * BT * sizeof(T) : 0);
 }
 
-template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT>
+// PSR: the Poisson-system step (M::step_psr, the reference's default "psr"
+// implementation) instead of Euler-Maruyama; bit 1 of V turns its white
+// noise off.
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_coup = reinterpret_cast<T*>(smem_raw);
@@ -287,7 +290,14 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     const int sub = a.sub0 + k;
     e.cov_ = tb.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
     const T t = (T)__ldg(tb.t_sub + sub);
-    if constexpr (CRN) {
+    if constexpr (PSR) {
+      PhiloxDraws<T, V> d;
+      d.key = key;
+      d.j = (uint32_t)j;
+      d.n = (uint32_t)a.n;
+      d.sub = (uint32_t)k;
+      M::template step_psr<DRIFT, (V & 2) != 0, T>(x, t, dt, e, key, (uint32_t)j, (uint32_t)a.n, (uint32_t)k, d);
+    } else if constexpr (CRN) {
       TableDraws<T, V> d;
       d.p = a.crn + ((size_t)g * a.n_sub + k) * a.crn_d;
       M::template step<V, DRIFT, T>(x, t, dt, e, d);

@@ -117,14 +117,15 @@ def read_theta(stream=None):
 
 def make_problem(model, settings, theta, args, J=None, filter=True):
     from .problem import Problem
-    if args.implementation == 'psr':
-        raise CliError("implementation 'psr' is not available in this engine yet; use 'sde' or 'ode'")
     seed = args.seed if args.seed is not None else 2 + args.id
-    dt = args.DT
-    return Problem(model, settings, theta, J=J or args.J, dt=dt, nb_obs=args.nb_obs, like_min=args.LIKE_MIN,
-                   noises_off=noises_off_of(args), filter=filter, seed=seed, precision=args.precision,
-                   freeze_forcing=args.freeze_forcing, ode=(args.implementation == 'ode'),
-                   eps_abs=args.eps_abs, eps_rel=args.eps_rel)
+    noises_off = noises_off_of(args)
+    # sde with every noise and the drift off is integrated as the ode (get_f_pred,
+    # model_builder/C/core/prediction_util.c:138-150)
+    ode = args.implementation == 'ode' or (args.implementation == 'sde' and noises_off == 7)
+    return Problem(model, settings, theta, J=J or args.J, dt=args.DT, nb_obs=args.nb_obs, like_min=args.LIKE_MIN,
+                   noises_off=noises_off, filter=filter, seed=seed, precision=args.precision,
+                   freeze_forcing=args.freeze_forcing, ode=ode, eps_abs=args.eps_abs, eps_rel=args.eps_rel,
+                   psr=(args.implementation == 'psr'))
 
 
 # ---------------------------------------------------------------- output formats

@@ -257,6 +257,7 @@ class Emitter(object):
         a('// Generated by plomgpu.emit for model "%s".  Do not edit.' % name)
         a('#pragma once')
         a('#include "plom_rt.h"')
+        a('#include "psr_samplers.h"')
         a('namespace plomgen {')
         a('struct Model {')
         a('  static constexpr const char* NAME = "%s";' % name)
@@ -280,6 +281,7 @@ class Emitter(object):
         self._emit_inc_tables(a)
         self._emit_step(a, caches, ode, inc)
         self._emit_deriv(a, caches, ode, inc)
+        self._emit_step_psr(a, caches)
         self._emit_proj2obs(a)
         self._emit_obs(a)
         a('};')
@@ -566,6 +568,178 @@ class Emitter(object):
         a('    for (int w = OFF_DRIFT; w < OFF_INC; ++w) f[w] = T(0);')
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];')
         a('  }')
+
+    def _emit_step_psr(self, a, caches):
+        """Poisson system with stochastic rates (step_psr,
+        model_builder/C/templates/core_template.c:105-209; equations of
+        Ccoder.step_psr / psr_multinomial / obs_inc_step_psr,
+        model_builder/Ccoder.py:155-322).  Per cac: Gamma white noises (rate 1
+        mean) unless NOENV; for every compartment with exits a multinomial
+        split of its (integer) content into the exits and the stay, with exit
+        probabilities (1 - exp(-sum h)) h / sum h, h = rate * dt; Poisson
+        arrivals from outside (U, remainder); the new contents; incidence
+        words summed from the split counts.  The coupling terms are those of
+        the substep start, as in the SDE step."""
+        m = self.m
+        univ = (UNIVERSE, m.remainder)
+        rates = []
+        for r in m.proc_model:
+            if r['rate'] not in rates:
+                rates.append(r['rate'])
+        sm = self._proc_symmap()
+        foi_states = sorted(set(self._foi_states()))
+        noises = []
+        for r in m.proc_model:
+            wn = r.get('white_noise')
+            if wn and wn['name'] not in [n for n, _ in noises]:
+                noises.append((wn['name'], sm[wn['sd']]))
+
+        def rate_expr(r):
+            k = rates.index(r['rate'])
+            e = '(double)r%d' % k
+            wn = r.get('white_noise')
+            if wn:
+                e = '%s*wn_%d' % (e, [n for n, _ in noises].index(wn['name']))
+            return e
+
+        a('  template <bool DRIFT, bool NOENV, class T, class X, class E>')
+        a('  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e, plomrt::UniformStream& rs,')
+        a('                              double (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
+        a('    (void)t; (void)pre;')
+        a('    const double ddt = (double)dt;')
+        for i, s_ in enumerate(m.par_sv):
+            a('    const T xo_%s = x[%d*N_CAC+cac];' % (s_, i))
+        for k, p_ in enumerate(self.drift):
+            pk = m.par_proc.index(p_)
+            a('    T drift_%d;' % k)
+            a('    if (DRIFT) {')
+            a('      const int g = e.drift_group(%d, cac);' % k)
+            a('      T xw = T(0);')
+            a('      if constexpr (X::DYNAMIC) {')
+            a('        xw = x[OFF_DRIFT+%d*N_CAC+g];' % k)
+            a('      } else {')
+            a('        PLOM_UNROLL')
+            a('        for (int gg = 0; gg < N_CAC; ++gg) if (gg == g) xw = x[OFF_DRIFT+%d*N_CAC+gg];' % k)
+            a('      }')
+            a('      drift_%d = e.drift_value(%d, g, xw);' % (k, k))
+            a('    } else {')
+            a('      drift_%d = e.par(%d, cac);' % (k, pk))
+            a('    }')
+        for s_ in foi_states:
+            a('    T foi_%s = T(0);' % s_)
+            a('    for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * pre.yf_%s[c2];' % (s_, s_))
+        # 1: white noises
+        for j, (name, sd) in enumerate(noises):
+            a('    double wn_%d = 1.0;' % j)
+            a('    if (!NOENV) {')
+            a('      const double sd = (double)(%s);' % sd)
+            a('      wn_%d = plomrt::gamma(rs, ddt / (sd * sd), sd * sd) / ddt;' % j)
+            a('    }')
+        # 2: rates
+        for k, c in enumerate(caches):
+            a('    const T r%d = %s;' % (k, c))
+        # 3: multinomial splits, in compartment order
+        for s_ in m.par_sv:
+            exits = [r for r in m.proc_model if r['from'] == s_]
+            if not exits:
+                continue
+            K = len(exits) + 1
+            a('    double inc_%s[%d];' % (s_, K))
+            a('    {')
+            for q, r in enumerate(exits):
+                a('      const double h%d = %s * ddt;' % (q, rate_expr(r)))
+            a('      const double sum = %s;' % ' + '.join('h%d' % q for q in range(len(exits))))
+            a('      double p[%d];' % K)
+            a('      if (sum > 0.0) {')
+            a('        const double ome = 1.0 - exp(-sum);')
+            for q in range(len(exits)):
+                a('        p[%d] = ome * (h%d / sum);' % (q, q))
+            a('        p[%d] = 1.0%s;' % (len(exits), ''.join(' - p[%d]' % q for q in range(len(exits)))))
+            a('      } else {')
+            for q in range(len(exits)):
+                a('        p[%d] = 0.0;' % q)
+            a('        p[%d] = 1.0;' % len(exits))
+            a('      }')
+            a('      const double xs = (double)xo_%s;' % s_)
+            a('      plomrt::multinomial<%d>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_%s);' % (K, s_))
+            a('    }')
+        # 4: arrivals from outside
+        for src in univ:
+            if src is None:
+                continue
+            arr = [r for r in m.proc_model if r['from'] == src]
+            if not arr:
+                continue
+            a('    double inc_%s[%d];' % (self._univ_name(src), len(arr)))
+            for q, r in enumerate(arr):
+                a('    inc_%s[%d] = plomrt::poisson(rs, %s * ddt);' % (self._univ_name(src), q, rate_expr(r)))
+        # 5: new contents
+        for i, s_ in enumerate(m.par_sv):
+            exits = [r for r in m.proc_model if r['from'] == s_]
+            terms = ['inc_%s[%d]' % (s_, len(exits))] if exits else ['(double)xo_%s' % s_]
+            for s2 in m.par_sv:
+                for q, r in enumerate([r for r in m.proc_model if r['from'] == s2]):
+                    if r['to'] == s_:
+                        terms.append('inc_%s[%d]' % (s2, q))
+            for src in univ:
+                if src is None:
+                    continue
+                for q, r in enumerate([r for r in m.proc_model if r['from'] == src]):
+                    if r['to'] == s_:
+                        terms.append('inc_%s[%d]' % (self._univ_name(src), q))
+            a('    x[%d*N_CAC+cac] = (T)(%s);' % (i, ' + '.join(terms)))
+        # 6: incidence of the observed flows
+        inc_terms = []
+        for defs in m.obs_var_def:
+            if not isinstance(defs[0], dict):
+                continue
+            t_ = []
+            for item in defs:
+                for r in m.proc_model:
+                    if r['from'] == item['from'] and r['to'] == item['to'] and r['rate'] == item['rate']:
+                        src = r['from']
+                        same = [x for x in m.proc_model if x['from'] == src]
+                        name = self._univ_name(src) if src in univ else src
+                        t_.append('inc_%s[%d]' % (name, same.index(r)))
+            inc_terms.append(' + '.join(t_) or '0.0')
+        if inc_terms:
+            a('    for (int k = 0; k < INC_PER_CAC; ++k) {')
+            a('      const int l = inc_link(cac, k);')
+            a('      if (l < 0) break;')
+            a('      const int o = l >> 10, w = l & 1023;')
+            for o, t_ in enumerate(inc_terms):
+                a('      if (o == %d) inc_acc[w] += %s;' % (o, t_))
+            a('    }')
+        a('  }')
+        a('  template <bool DRIFT, bool NOENV, class T, class X, class E, class D>')
+        a('  PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,')
+        a('                               const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {')
+        a('    double inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;')
+        a('    Pre<T> pre;')
+        a('    pre.unused = 0;')
+        for s_ in foi_states:
+            si = m.par_sv.index(s_)
+            a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
+        a('    for (int cac = 0; cac < N_CAC; ++cac) {')
+        a('      plomrt::UniformStream rs;')
+        a('      rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);')
+        a('      psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);')
+        a('    }')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = (T)((double)x[OFF_INC+w] + inc_acc[w]);')
+        a('    if (DRIFT) {')
+        a('      // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)')
+        a('      for (int i = 0; i < N_DRIFT; ++i) {')
+        a('        const int ng = e.drift_ngroups(i);')
+        a('        for (int g = 0; g < ng; ++g)')
+        a('          x[OFF_DRIFT+i*N_CAC+g] += e.drift_vol(i, g)*sqrt(dt)*draws.drift_normal(i, g);')
+        a('      }')
+        a('    }')
+        a('  }')
+
+    @staticmethod
+    def _univ_name(src):
+        return 'U' if src == UNIVERSE else 'rem_' + src
 
     def _foi_states(self):
         out = []

@@ -44,7 +44,8 @@ class SmcDesc(C.Structure):
                 ('filter', C.c_int), ('like_min', C.c_double), ('seed', C.c_uint64), ('precision', C.c_int),
                 ('crn_normals', _dp), ('crn_uniforms', _dp), ('pop_size', _dp), ('cov_ts0', _dp),
                 ('ode', C.c_int), ('eps_abs', C.c_double), ('eps_rel', C.c_double), ('cov_spline_meta', _ip),
-                ('cov_spline_x', _dp), ('cov_spline_y', _dp), ('cov_spline_m2', _dp), ('cov_spline_knots', C.c_int)]
+                ('cov_spline_x', _dp), ('cov_spline_y', _dp), ('cov_spline_m2', _dp), ('cov_spline_knots', C.c_int),
+                ('psr', C.c_int)]
 
 
 class BatchDesc(C.Structure):
@@ -143,6 +144,7 @@ class DescHolder(object):
             like_min=p.like_min, seed=p.seed, precision=precision or p.precision,
             crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp), pop_size=_ptr(pop, _dp),
             cov_ts0=_ptr(cts0, _dp))
+        self.desc.psr = 1 if getattr(p, 'psr', False) else 0
         if getattr(p, 'ode', False):
             meta, xs, ys, m2 = p.spline_tables()
             meta = keep('sp_meta', meta if meta.size else np.zeros(3, np.int32), np.int32)

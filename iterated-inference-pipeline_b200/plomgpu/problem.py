@@ -94,7 +94,7 @@ class Problem(object):
 
     def __init__(self, model, settings, theta, J=1000, dt=1.0, nb_obs=-1, like_min=1e-17,
                  noises_off=0, filter=True, seed=2, precision=32, u_data='D', freeze_forcing=-1.0,
-                 ode=False, eps_abs=1e-6, eps_rel=1e-3):
+                 ode=False, eps_abs=1e-6, eps_rel=1e-3, psr=False):
         if not isinstance(model, PlomModel):
             raise TypeError('model must be a PlomModel')
         m = self.model = model
@@ -112,6 +112,10 @@ class Problem(object):
         self.eps_rel = float(eps_rel)
         if self.ode:
             self.noises_off = 7
+        # Poisson system with stochastic rates (the "psr" implementation)
+        self.psr = bool(psr)
+        if self.psr and self.ode:
+            raise ValueError('psr and ode exclude each other')
         data = settings['data']
         times = data['times']
         rows = data['data']

@@ -42,6 +42,8 @@ class Oracle(object):
                                                  C.POINTER(C.c_uint32)]
         L.oracle_mif_iteration.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.MifDesc), _dp, _dp, _dp, _dp,
                                            _dp, C.POINTER(C.c_int), _dp, _dp]
+        L.oracle_psr_samples.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, _dp]
+        L.oracle_psr_samples.restype = None
         L.oracle_ci95.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
         L.oracle_ci95.restype = None
         L.oracle_proj2obs.argtypes = [_dp, _dp]
@@ -135,3 +137,10 @@ class Oracle(object):
         self.lib.oracle_ci95(v.ctypes.data_as(_dp), None if w is None else w.ctypes.data_as(_dp), len(v),
                              C.byref(lo), C.byref(hi))
         return lo.value, hi.value
+
+    def psr_samples(self, kind, a, b=0.0, seed=1, count=10000):
+        """Draws of the psr samplers: 'binomial' (n=a, p=b), 'poisson' (mu=a), 'gamma' (shape a, scale b)."""
+        out = np.zeros(count)
+        k = {'binomial': 0, 'poisson': 1, 'gamma': 2}[kind]
+        self.lib.oracle_psr_samples(k, float(a), float(b), int(seed), int(count), out.ctypes.data_as(_dp))
+        return out

@@ -137,6 +137,42 @@ struct PhiloxSource {
   }
 };
 
+// Poisson-system step over interval n (step_psr + f_prediction_psr,
+// model_builder/C/core/prediction_util.c:290-317) with the GPU's Philox
+// streams.
+template <bool DRIFT, bool NOENV>
+void propagate_psr(double* x, const plomgpu_smc_desc* d, int n, int j, int sub0) {
+  HostEnv e;
+  e.par_ = d->par_cac;
+  e.coup_ = d->coupling;
+  e.dgroup_ = d->drift_group;
+  e.dng_ = d->drift_ngroups;
+  e.dbt_ = d->drift_bt;
+  e.dvol_ = d->drift_vol;
+  HostState xs;
+  xs.b = x;
+  const plomrt::PhiloxKey key = plomrt::make_key(d->seed, 0u);
+  for (int k = 0; k < d->n_sub[n]; ++k) {
+    const int sub = sub0 + k;
+    e.cov_ = d->cov_cac ? d->cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC : nullptr;
+    PhiloxSource<0> src;
+    src.key = key;
+    src.j = (uint32_t)j;
+    src.n = (uint32_t)n;
+    src.sub = (uint32_t)k;
+    M::step_psr<DRIFT, NOENV, double>(xs, d->t_sub[sub], d->dt, e, key, (uint32_t)j, (uint32_t)n, (uint32_t)k, src);
+  }
+}
+
+typedef void (*PsrFn)(double*, const plomgpu_smc_desc*, int, int, int);
+
+PsrFn pick_psr(int noises_off) {
+  const bool drift = M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT);
+  const bool noenv = (noises_off & PLOMGPU_NO_ENV_STO) != 0;
+  if (drift) return noenv ? &propagate_psr<true, true> : &propagate_psr<true, false>;
+  return noenv ? &propagate_psr<false, true> : &propagate_psr<false, false>;
+}
+
 int draws_per_substep(int noises_off) {
   const bool drift = M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT);
   return M::N_CAC * M::draws_per_cac(noises_off & 3) + (drift ? M::N_DRIFT * M::N_CAC : 0);
@@ -411,6 +447,18 @@ int oracle_model_info(plomgpu_model_info* o) {
 
 int oracle_draws_per_substep(int noises_off) { return draws_per_substep(noises_off); }
 
+// Draws of the psr samplers from one uniform stream (distribution tests).
+// kind 0 binomial(a, b), 1 Poisson(a), 2 Gamma(shape a, scale b).
+void oracle_psr_samples(int kind, double a, double b, uint64_t seed, int count, double* out) {
+  plomrt::UniformStream rs;
+  rs.init(plomrt::make_key(seed, 0u), 0u, 0u, 0u);
+  for (int i = 0; i < count; ++i) {
+    if (kind == 0) out[i] = plomrt::binomial(rs, a, b);
+    else if (kind == 1) out[i] = plomrt::poisson(rs, a);
+    else out[i] = plomrt::gamma(rs, a, b);
+  }
+}
+
 // get_CI95 on given values and weights (null: 1/J), known-answer tests.
 void oracle_ci95(const double* v, const double* w, int J, double* lo, double* hi) {
   std::vector<double> vv(v, v + J);
@@ -425,7 +473,9 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
   if (n_threads > 0) omp_set_num_threads(n_threads);
 #endif
   const PropFn prop = pick(d->noises_off);
+  const PsrFn psr_prop = pick_psr(d->noises_off);
   int ode_fail = 0;
+  if (d->psr && (d->ode || d->crn_normals)) return PLOMGPU_EINVAL;
   const int D = d->crn_normals ? draws_per_substep(d->noises_off) : 0;
   // AoS particles: proj[S] per particle, two generations
   std::vector<double> X((size_t)J * S), Xn((size_t)J * S);
@@ -453,6 +503,8 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
       for (int w = M::OFF_INC; w < S; ++w) x[w] = 0.0;  // reset_inc
       if (d->ode) {
         if (ode_propagate(x, d, n, sub0) != plomrt::ODE_OK) ode_fail = 1;
+      } else if (d->psr) {
+        psr_prop(x, d, n, j, sub0);
       } else {
         prop(x, d, n, j, sub0, crn_n, D);
       }

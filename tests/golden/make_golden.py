@@ -17,7 +17,9 @@ here with a minimal source shim (print statements, ``iteritems``, list-valued
 
 Recorded per model: the parsed model (``Cmodel``), the settings document
 (``PlomModelBuilder.make_settings_json``), the generated equations
-(``Ccoder.step_ode_sde``, ``print_like``, ``print_obs_prev``) and, for seeded
+(``Ccoder.step_ode_sde``, ``print_like``, ``print_obs_prev``, and the
+Poisson-system code of ``step_psr``, ``psr_multinomial`` and
+``obs_inc_step_psr``) and, for seeded
 random inputs, the numbers those generated C expressions produce for one
 Euler-Maruyama step of every noise variant and for the observation model.
 The C expressions are evaluated in IEEE double through a mechanical
@@ -249,6 +251,12 @@ def main(ref_root):
         entry = {'context': c, 'process': p, 'link': l, 'theta': th, 'ir': ir_of(ref), 'settings': settings,
                  'ts_id': b.ts_id, 'cac_id': b.cac_id}
         entry.update(step_cases(ref, c, p, l, 6, rng))
+        # Poisson-system-with-stochastic-rates code generation (Ccoder.step_psr,
+        # psr_multinomial, obs_inc_step_psr)
+        psr = ref.step_psr()
+        entry['psr'] = {'caches': list(psr['caches']), 'code': psr['code'], 'poisson': list(psr['poisson']),
+                        'update': psr['update'], 'multinomial': ref.psr_multinomial(),
+                        'obs_inc': ref.obs_inc_step_psr()}
         out_models[name] = entry
     fixtures['models'] = out_models
     path = os.path.join(HERE, 'reference_codegen.json')
@@ -258,5 +266,8 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    os.environ.setdefault('PYTHONHASHSEED', '0')
+    # the reference iterates over sets when it orders its rate caches: fix the
+    # string hash so that the fixture is reproducible
+    if os.environ.get('PYTHONHASHSEED') != '0':
+        os.execve(sys.executable, [sys.executable] + sys.argv, dict(os.environ, PYTHONHASHSEED='0'))
     main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')

@@ -155,7 +155,8 @@ def test_sampled_trajectory_follows_the_genealogy(precision):
     w /= w.sum()
     x0 = p.x0.copy()
     x0[eng.info.off_inc:] = 0.0
-    for u in (0.01, 0.37, 0.93):
+    # u away from multiples of 1/J: with equal weights the crossing index would hinge on rounding
+    for u in (0.0123, 0.3777, 0.9191):
         rows_t, states = plan.sample_traj(u)
         ref = _walk(w, u, out.ancestors, out.x_pred, x0, weigh)
         assert list(rows_t) == [r[0] for r in ref]

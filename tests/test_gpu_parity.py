@@ -202,9 +202,9 @@ def test_fp32_precision_bias_with_common_draws():
 
 
 @pytest.mark.parametrize('noises_off', [0, 3])
-def test_crn_parity_team_kernel(noises_off):
-    """seir20x2 (180 state words in shared memory, one team of lanes per particle) against the
-    oracle with common draws, FP64: trajectories, ancestors, log-likelihood."""
+def test_crn_parity_shared_memory_state(noises_off):
+    """seir20x2 (180 state words per particle, held in shared memory) against the oracle with
+    common draws, FP64: trajectories, ancestors, log-likelihood."""
     eng = models.engine('seir20x2')
     orc = models.build_oracle('seir20x2')
     p = models.make_problem('seir20x2', J=300, dt=1.0, noises_off=noises_off, precision=64, seed=11, nb_obs=30)
@@ -217,8 +217,8 @@ def test_crn_parity_team_kernel(noises_off):
     assert g.loglik == pytest.approx(o.loglik, rel=1e-9)
 
 
-def test_philox_fp64_team_kernel_matches_oracle():
-    """The team kernel consumes the same Philox blocks as the single-thread oracle (FP64)."""
+def test_philox_fp64_shared_memory_state_matches_oracle():
+    """The shared-memory-state kernel consumes the same Philox blocks as the oracle (FP64)."""
     eng = models.engine('seir20x2')
     orc = models.build_oracle('seir20x2')
     p = models.make_problem('seir20x2', J=200, dt=1.0, precision=64, seed=5, nb_obs=20)
