@@ -49,6 +49,7 @@ def parse():
     ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
+    ap.add_argument('--plan-pool', type=int, default=8, help='serve: concurrent plans of the shared-memory model')
     return ap.parse_args()
 
 
@@ -339,7 +340,8 @@ def run_serve(args, window_s=0.25, rate=2000.0):
     }
     for c in classes.values():
         c['eng'] = Engine(c['lib'])
-        c['server'] = Server(c['eng'], c['prob'], max_J=c['J'], memory_budget=150e9 / 2, plan_pool=8, precision=32)
+        c['server'] = Server(c['eng'], c['prob'], max_J=c['J'], memory_budget=150e9 / 2, plan_pool=args.plan_pool,
+                             precision=32)
     rng = np.random.Generator(np.random.Philox(12))
     chains = []
     for i in range(32):

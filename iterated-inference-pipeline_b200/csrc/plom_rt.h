@@ -104,6 +104,22 @@ PLOM_HD double disc_normal_like(double y, double mu, double var, double like_min
   return (like <= like_min) ? like_min : like;
 }
 
+// Log of one series' density, counting the series whose density sits on the
+// LIKE_MIN floor.
+PLOM_HD double log_like_term(double y, double mu, double var, double like_min, int* floor_hits) {
+  const double l = disc_normal_like(y, mu, var, like_min);
+  if (l == like_min) ++*floor_hits;
+  return log(l);
+}
+
+// A particle's log-weight.  The reference fails a particle when
+// exp(loglik) <= LIKE_MIN^N_TS (smc.c:44); since every density is at least
+// LIKE_MIN, that holds in exact arithmetic exactly when all N_TS series are on
+// the floor, a case the rounding of exp / pow would otherwise decide one way
+// or the other.  Such a particle gets -inf (weight 0, a failure); integer
+// (psr) counts meet the case often.
+PLOM_HD double finish_loglik(double ll, int floor_hits, int n_ts) { return floor_hits >= n_ts ? -INFINITY : ll; }
+
 // ---------------------------------------------------------------- Philox4x32-10
 struct U4 { uint32_t x, y, z, w; };
 

@@ -227,15 +227,16 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
         double obs[M::N_TS];
         M::template proj2obs<T>(x, obs);
         double ll = 0.0;
+        int fl = 0;
 #pragma unroll
         for (int ts = 0; ts < M::N_TS; ++ts) {
           const double yy = y[ts];
           if (isnan(yy)) continue;
           const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
           const double var = M::obs_var(obs[ts], ts, t_obs, oe);
-          ll += log(plomrt::disc_normal_like(yy, mu, var, a.like_min));
+          ll += plomrt::log_like_term(yy, mu, var, a.like_min, &fl);
         }
-        const T l = (T)ll;
+        const T l = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
         ws.lw[j] = l;
         if (weight_fails(l, a.thresh)) {
           acc.nfail += 1;

@@ -324,15 +324,16 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     double obs[M::N_TS];
     M::template proj2obs<T>(x, obs);
     double ll = 0.0;
+    int fl = 0;
 #pragma unroll
     for (int ts = 0; ts < M::N_TS; ++ts) {
       const double y = __ldg(a.y + ts);
       if (isnan(y)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += log(plomrt::disc_normal_like(y, mu, var, tb.like_min));
+      ll += plomrt::log_like_term(y, mu, var, tb.like_min, &fl);
     }
-    ((T*)a.lw)[g] = (T)ll;
+    ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
   }
 }
 
@@ -473,6 +474,7 @@ __global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(con
     oe.par_ts_ = tb.par_ts;
     oe.cov_ts_ = a.cov_ts;
     double ll = 0.0;
+    int fl = 0;
 #pragma unroll
     for (int ts = 0; ts < M::N_TS; ++ts) {
       if (ts % TP != tm.rank) continue;
@@ -480,10 +482,11 @@ __global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(con
       if (isnan(y)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += log(plomrt::disc_normal_like(y, mu, var, tb.like_min));
+      ll += plomrt::log_like_term(y, mu, var, tb.like_min, &fl);
     }
     ll = tm.sum(ll);
-    if (tm.rank == 0) ((T*)a.lw)[g] = (T)ll;
+    fl = tm.sum(fl);
+    if (tm.rank == 0) ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
   }
 }
 
@@ -981,15 +984,16 @@ __global__ void __launch_bounds__(BT) k_propagate_ode(const Tables<T> tb, const 
     oe.par_ts_ = tb.par_ts;
     oe.cov_ts_ = a.cov_ts;
     double ll = 0.0;
+    int fl = 0;
 #pragma unroll
     for (int ts = 0; ts < M::N_TS; ++ts) {
       const double yy = __ldg(a.y + ts);
       if (isnan(yy)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += log(plomrt::disc_normal_like(yy, mu, var, tb.like_min));
+      ll += plomrt::log_like_term(yy, mu, var, tb.like_min, &fl);
     }
-    ((T*)a.lw)[g] = (T)ll;
+    ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
   }
 }
 

@@ -240,13 +240,14 @@ double log_likelihood(const double* x, const plomgpu_smc_desc* d, int n) {
   oe.cov_ts_ = d->cov_ts ? d->cov_ts + (size_t)n * M::N_COV_TS * M::N_TS : nullptr;
   const double* y = d->data + (size_t)n * M::N_TS;
   double ll = 0.0;
+  int fl = 0;
   for (int ts = 0; ts < M::N_TS; ++ts) {
     if (isnan(y[ts])) continue;
     const double mu = M::obs_mean(obs[ts], ts, d->t_obs[n], oe);
     const double var = M::obs_var(obs[ts], ts, d->t_obs[n], oe);
-    ll += log(plomrt::disc_normal_like(y[ts], mu, var, d->like_min));
+    ll += plomrt::log_like_term(y[ts], mu, var, d->like_min, &fl);
   }
-  return ll;
+  return plomrt::finish_loglik(ll, fl, M::N_TS);
 }
 
 // weight(), smc.c:27-83
@@ -688,13 +689,14 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
           xs.b = x;
           M::proj2obs<double>(xs, obs);
           double ll = 0.0;
+          int fl = 0;
           for (int ts = 0; ts < M::N_TS; ++ts) {
             if (isnan(y[ts])) continue;
             const double mu = M::obs_mean(obs[ts], ts, d->t_obs[n], oe);
             const double var = M::obs_var(obs[ts], ts, d->t_obs[n], oe);
-            ll += log(plomrt::disc_normal_like(y[ts], mu, var, d->like_min));
+            ll += plomrt::log_like_term(y[ts], mu, var, d->like_min, &fl);
           }
-          w[j] = exp(ll);
+          w[j] = exp(plomrt::finish_loglik(ll, fl, M::N_TS));
         }
       }
       sub0 += d->n_sub[n];
