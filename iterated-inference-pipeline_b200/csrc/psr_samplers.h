@@ -214,15 +214,20 @@ PLOM_HD double gamma(UniformStream& rs, double a, double theta) {
 }
 
 // plom_ran_multinomial: K categories with probabilities p summing to one,
-// N trials; out[k] = counts
+// N trials; out[k] = counts.  The last category takes the remaining trials:
+// its conditional probability p[K-1] / (1 - sum of the others) is one in
+// exact arithmetic, and deciding it in floating point would make the number
+// of uniforms drawn (and so every later draw of the stream) depend on the
+// last bits of the probabilities.
 template <int K>
 PLOM_HD void multinomial(UniformStream& rs, double N, const double (&p)[K], double (&out)[K]) {
   double sum_p = 0.0, sum_n = 0.0;
-  for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < K - 1; ++k) {
     out[k] = (p[k] > 0.0) ? binomial(rs, N - sum_n, p[k] / (1.0 - sum_p)) : 0.0;
     sum_p += p[k];
     sum_n += out[k];
   }
+  out[K - 1] = (p[K - 1] > 0.0) ? N - sum_n : 0.0;
 }
 
 }  // namespace plomrt
