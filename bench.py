@@ -148,6 +148,19 @@ def ncu_traffic(workload):
         return None
 
 
+def ncu_issue(workload):
+    """Issue-side utilisation of the propagate kernel from the committed ncu summary (the bound that
+    binds: the full-noise step is instruction-issue bound, not HBM bound)."""
+    path = os.path.join(ROOT, 'profiles', 'k_propagate_%s.json' % workload)
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return {'issue_slots_active_pct': d['issue_active_pct'], 'ipc': d['ipc'],
+                'warps_active_per_sm': d['warps_active_per_sm'], 'source': 'profiles/k_propagate_%s.md' % workload}
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def cpu_baseline(workload, budget_s=12.0, threads=0):
     """Times the FP64 oracle (OpenMP, all host threads) on a bounded sample of the workload."""
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
@@ -522,7 +535,8 @@ def main():
                          'frac': achieved / peak, 'traffic': traffic,
                          'kernel': 'k_propagate', 'bytes_per_particle_step': B,
                          'avg_launch_ms': avg_prop_ms, 'peak_kind': peak_kind,
-                         'propagate_share': tot_prop / (ms_total / args.steps)},
+                         'propagate_share': tot_prop / (ms_total / args.steps),
+                         'issue': ncu_issue(args.workload)},
             'clocks': clk.summary(),
             'e2e': {'value': e2e_value, 'unit': 'particle-steps/s', 'h2d_bytes_per_step': h2d,
                     'd2h_bytes_per_step': d2h, 'call': 'plomgpu_smc_run (host buffers, one-shot)'},

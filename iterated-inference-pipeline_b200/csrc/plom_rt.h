@@ -134,10 +134,17 @@ PLOM_HD uint32_t mulhilo32(uint32_t a, uint32_t b, uint32_t* hi) {
 #endif
 }
 
+// rounds unrolled per loop iteration (code size against loop overhead)
+#ifndef PLOM_PHILOX_UNROLL
+#define PLOM_PHILOX_UNROLL 10
+#endif
+#define PLOM_STR_(x) #x
+#define PLOM_PRAGMA_UNROLL_N(n) _Pragma(PLOM_STR_(unroll n))
+
 PLOM_HD U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
   const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
+  PLOM_PRAGMA_UNROLL_N(PLOM_PHILOX_UNROLL)
   for (int r = 0; r < 10; ++r) {
     uint32_t hi0, hi1;
     const uint32_t lo0 = mulhilo32(M0, c.x, &hi0);

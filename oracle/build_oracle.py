@@ -26,8 +26,9 @@ def build(name, force=False):
     if not os.path.exists(header):
         raise FileNotFoundError(header)
     out = lib_path(name)
-    srcs = [os.path.join(HERE, 'oracle_smc.cpp'), header, os.path.join(PKG, 'csrc', 'plom_rt.h'),
-            os.path.join(REPO, 'include', 'plomgpu.h')]
+    csrc = os.path.join(PKG, 'csrc')
+    srcs = [os.path.join(HERE, 'oracle_smc.cpp'), header, os.path.join(REPO, 'include', 'plomgpu.h')] + \
+        [os.path.join(csrc, f) for f in sorted(os.listdir(csrc)) if f.endswith('.h')]
     if not force and os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(s) for s in srcs):
         return out
     os.makedirs(OUT, exist_ok=True)
