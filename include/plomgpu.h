@@ -224,8 +224,7 @@ int plomgpu_debug_systematic_points(double U, int J, double *out);
  * parameters are resampled with the particles and perturbed by a Gaussian
  * random walk on the estimated components (resample_and_mut_theta_mif,
  * methods.c:261-367).  The theta-hat update between iterations is left to
- * the host (update_theta_best_*, methods.c:394-467).  Fitted parameters take
- * one value for all populations / series (one group). */
+ * the host (update_theta_best_*, methods.c:394-467). */
 typedef struct plomgpu_mif_desc {
     int n_runs;
     int n_theta;
@@ -233,6 +232,12 @@ typedef struct plomgpu_mif_desc {
     const int *obs_slot;    /* [n_par_obs] component of each observation parameter, -1: from par_ts */
     const plomgpu_back_transform *theta_bt; /* [n_theta] transformed -> natural scale */
     const int *estimated;   /* [n_theta] 1: perturbed by the random walk */
+    /* Parameters fitted per group: a slot of -2 above means that the
+     * component depends on the population (process, [n_par_proc][n_cac]) or
+     * series (observation, [n_par_obs][n_ts]) through these tables; null when
+     * no slot is -2. */
+    const int *proc_cac_slot;
+    const int *obs_ts_slot;
 } plomgpu_mif_desc;
 
 typedef struct plomgpu_plan plomgpu_mif;
@@ -317,7 +322,9 @@ typedef struct plomgpu_server_opts {
     int max_J;              /* largest particle count of a request */
     double memory_budget;   /* bytes of HBM the requests may hold (0: 150e9) */
     int ring_slots;         /* requests in flight on the device loop (0: 1024) */
-    int plan_pool;          /* concurrent plans for models served per plan (0: 8) */
+    int plan_pool;          /* concurrent plans for models served per plan (0: 2; one SEIR 20x2 filter of
+                             * 2e4 particles nearly fills a B200, and 8 concurrent plans measured 1.5x
+                             * slower than 2) */
     int precision;          /* 32 or 64 */
 } plomgpu_server_opts;
 

@@ -24,6 +24,9 @@
 // Loop unrolling: ``PLOM_UNROLL`` fully unrolls short fixed loops; the loop
 // over compartment-age classes is unrolled when the particle state lives in
 // registers (small models) and kept rolled when it lives in shared memory.
+// ``PLOM_PRAGMA_GROUP`` covers the cacs of one draw group (unrolled unless
+// PLOM_GROUP_ROLLED is defined, which trades registers / code size for
+// indexed draws).
 #if defined(__CUDACC__)
 #define PLOM_UNROLL _Pragma("unroll")
 #if defined(PLOM_SMEM_STATE) && PLOM_SMEM_STATE
@@ -31,9 +34,15 @@
 #else
 #define PLOM_PRAGMA_CAC _Pragma("unroll")
 #endif
+#if defined(PLOM_GROUP_ROLLED)
+#define PLOM_PRAGMA_GROUP _Pragma("unroll 1")
+#else
+#define PLOM_PRAGMA_GROUP _Pragma("unroll")
+#endif
 #else
 #define PLOM_UNROLL
 #define PLOM_PRAGMA_CAC
+#define PLOM_PRAGMA_GROUP
 #endif
 
 namespace plomrt {

@@ -142,6 +142,8 @@ struct plomgpu_plan {
   double* cov_ts0 = nullptr;   // [N_COV_TS][N_TS] at time 0
   double hat_rank[2] = {1.0, 1.0};  // quantile ranks under equal weights
   bool psr = false;  // Poisson system with stochastic rates
+  int* proc_cslot = nullptr;  // iterated filtering, per-group components
+  int* obs_tslot = nullptr;
   // deterministic skeleton
   bool ode = false;
   double eps_abs = 1e-6, eps_rel = 1e-3;
@@ -321,6 +323,8 @@ int enqueue_filter(plomgpu_plan* p) {
   tb.theta_bt = p->theta_bt;
   tb.proc_slot = p->proc_slot;
   tb.obs_slot = p->obs_slot;
+  tb.proc_cslot = p->proc_cslot;
+  tb.obs_tslot = p->obs_tslot;
   const int R = p->R;
   const size_t RJ = (size_t)R * J;
 
@@ -636,7 +640,7 @@ void plan_free(plomgpu_plan* p) {
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
-                  p->obs_slot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->sp_meta, p->sp_x, p->sp_y, p->sp_m2, p->data_idx, p->traj_t,
+                  p->obs_slot, p->proc_cslot, p->obs_tslot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->sp_meta, p->sp_x, p->sp_y, p->sp_m2, p->data_idx, p->traj_t,
                   p->traj_j, p->traj_n, p->traj_x};
   for (void* b : bufs)
     if (b) cudaFree(b);
@@ -645,6 +649,21 @@ void plan_free(plomgpu_plan* p) {
     if (e) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
+}
+
+// per-group component tables of iterated filtering (slots of -2)
+int mif_group_tables(const plomgpu_mif_desc* mif, plomgpu_plan* p) {
+  bool proc_multi = false, obs_multi = false;
+  for (int k = 0; k < M::N_PAR_PROC; ++k) proc_multi |= mif->proc_slot[k] == -2;
+  for (int k = 0; k < M::N_PAR_OBS; ++k) obs_multi |= mif->obs_slot[k] == -2;
+  if ((proc_multi && !mif->proc_cac_slot) || (obs_multi && !mif->obs_ts_slot))
+    return fail(PLOMGPU_EINVAL, "a slot of -2 needs its per-group table");
+  int rc = PLOMGPU_OK;
+  if (proc_multi && (rc = upload<int>(mif->proc_cac_slot, (size_t)M::N_PAR_PROC * M::N_CAC, &p->proc_cslot, p->stream)))
+    return rc;
+  if (obs_multi && (rc = upload<int>(mif->obs_ts_slot, (size_t)M::N_PAR_OBS * M::N_TS, &p->obs_tslot, p->stream)))
+    return rc;
+  return PLOMGPU_OK;
 }
 
 int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bool want_xpred, bool want_final,
@@ -733,7 +752,8 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
     if ((rc2 = upload<plomrt::BackTransform>((const plomrt::BackTransform*)mif->theta_bt, (size_t)mif->n_theta,
                                              &p->theta_bt, p->stream)) ||
         (rc2 = upload<int>(mif->proc_slot, (size_t)(M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 0), &p->proc_slot, p->stream)) ||
-        (rc2 = upload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream))) {
+        (rc2 = upload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream)) ||
+        (rc2 = mif_group_tables(mif, p))) {
       std::string keep = g_err;
       plan_free(p);
       g_err = keep;
@@ -1633,7 +1653,7 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->precision = o->precision;
   sv->max_J = o->max_J;
   sv->ring = o->ring_slots > 0 ? o->ring_slots : 1024;
-  sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 8;
+  sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 2;
   sv->budget = o->memory_budget > 0 ? (size_t)o->memory_budget : (size_t)150e9;
   // keep host copies of the shared problem
   const int n = d->n_obs;

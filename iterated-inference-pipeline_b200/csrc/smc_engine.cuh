@@ -132,8 +132,10 @@ struct Tables {
   int Q;                                 // theta components (<= kMaxTheta)
   unsigned est_mask;                     // components perturbed by the random walk
   const plomrt::BackTransform* theta_bt; // [Q] transformed -> natural
-  const int* proc_slot;                  // [N_PAR_PROC] component of each process parameter, -1: table
-  const int* obs_slot;                   // [N_PAR_OBS] component of each observation parameter, -1: table
+  const int* proc_slot;                  // [N_PAR_PROC] component of each process parameter, -1: table, -2: per cac
+  const int* obs_slot;                   // [N_PAR_OBS] component of each observation parameter, -1: table, -2: per series
+  const int* proc_cslot;                 // [N_PAR_PROC][N_CAC] components of the per-cac parameters
+  const int* obs_tslot;                  // [N_PAR_OBS][N_TS] components of the per-series parameters
 };
 
 constexpr int kMaxTheta = 16;
@@ -160,20 +162,41 @@ struct StepArgs {
 };
 
 // environments with per-particle parameters (iterated filtering)
+// uni: parameters taken from the particle; multi: those of them whose
+// component depends on the population / series (one per group), looked up
+// in cslot and selected from the particle's natural values natq.
 template <class T>
 struct MifProcEnv : ProcEnv<T> {
   T parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
-  unsigned uni;
+  unsigned uni, multi;
+  const int* cslot;  // [N_PAR_PROC][N_CAC]
+  T natq[kMaxTheta];
   __device__ __forceinline__ T par(int p, int cac) const {
-    return ((uni >> p) & 1u) ? parp[p] : this->par_[p * M::N_CAC + cac];
+    if (!((uni >> p) & 1u)) return this->par_[p * M::N_CAC + cac];
+    if (!((multi >> p) & 1u)) return parp[p];
+    const int q = __ldg(cslot + p * M::N_CAC + cac);
+    T v = T(0);
+#pragma unroll
+    for (int qq = 0; qq < kMaxTheta; ++qq)
+      if (qq == q) v = natq[qq];
+    return v;
   }
 };
 
 struct MifObsEnv : ObsEnv {
   double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
-  unsigned uni;
+  unsigned uni, multi;
+  const int* tslot;  // [N_PAR_OBS][N_TS]
+  double natq[kMaxTheta];
   __device__ __forceinline__ double par_ts(int p, int ts) const {
-    return ((uni >> p) & 1u) ? obsp[p] : par_ts_[p * M::N_TS + ts];
+    if (!((uni >> p) & 1u)) return par_ts_[p * M::N_TS + ts];
+    if (!((multi >> p) & 1u)) return obsp[p];
+    const int q = __ldg(tslot + p * M::N_TS + ts);
+    double v = 0.0;
+#pragma unroll
+    for (int qq = 0; qq < kMaxTheta; ++qq)
+      if (qq == q) v = natq[qq];
+    return v;
   }
 };
 
@@ -263,6 +286,10 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       }
     }
     e.uni = 0u;
+    e.multi = 0u;
+    e.cslot = tb.proc_cslot;
+#pragma unroll
+    for (int q = 0; q < kMaxTheta; ++q) e.natq[q] = (T)nat[q];
 #pragma unroll
     for (int k = 0; k < M::N_PAR_PROC; ++k) {
       const int slot = __ldg(tb.proc_slot + k);
@@ -271,9 +298,14 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       for (int q = 0; q < kMaxTheta; ++q)
         if (q == slot) v = (T)nat[q];
       e.parp[k] = v;
-      if (slot >= 0) e.uni |= 1u << k;
+      if (slot >= 0 || slot == -2) e.uni |= 1u << k;
+      if (slot == -2) e.multi |= 1u << k;
     }
     oe.uni = 0u;
+    oe.multi = 0u;
+    oe.tslot = tb.obs_tslot;
+#pragma unroll
+    for (int q = 0; q < kMaxTheta; ++q) oe.natq[q] = nat[q];
 #pragma unroll
     for (int k = 0; k < M::N_PAR_OBS; ++k) {
       const int slot = __ldg(tb.obs_slot + k);
@@ -282,7 +314,8 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       for (int q = 0; q < kMaxTheta; ++q)
         if (q == slot) v = nat[q];
       oe.obsp[k] = v;
-      if (slot >= 0) oe.uni |= 1u << k;
+      if (slot >= 0 || slot == -2) oe.uni |= 1u << k;
+      if (slot == -2) oe.multi |= 1u << k;
     }
   }
 

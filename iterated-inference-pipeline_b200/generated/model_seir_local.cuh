@@ -124,7 +124,7 @@ struct Model {
     for (int cac0 = 0; cac0 < NMAIN; cac0 += G) {
       T nz[NW * G > 0 ? NW * G : 1];
       draws.template normals<NW * G>(cac0, nz);
-      PLOM_UNROLL
+      PLOM_PRAGMA_GROUP
       for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);
     }
     PLOM_UNROLL

@@ -467,7 +467,7 @@ def mif_main(argv, stdin=None, model_dir='.'):
                                                 fmt_g(args.heat), fmt_g(args.lag), args.switch, args.n_thread))
     t_all = time.time()
     index = dict(((e['name'], e['g']), k) for k, e in enumerate(best.entries))
-    slots = [index[(c['name'], 0)] for c in run.comp]
+    slots = [index[(c['name'], c['g'])] for c in run.comp]
     f_trace = open(path_of(args, 'trace'), 'w')
     f_trace.write(best.trace_header())
     f_trace.write(best.trace_row(0, float('nan')))

@@ -435,7 +435,7 @@ class Emitter(object):
         a('    for (int cac0 = 0; cac0 < NMAIN; cac0 += G) {')
         a('      T nz[NW * G > 0 ? NW * G : 1];')
         a('      draws.template normals<NW * G>(cac0, nz);')
-        a('      PLOM_UNROLL')
+        a('      PLOM_PRAGMA_GROUP')
         a('      for (int g = 0; g < G; ++g) cac_body<V, DRIFT, T>(x, cac0 + g, nz + g * NW, t, dt, e, inc_acc, pre);')
         a('    }')
         a('    PLOM_UNROLL')

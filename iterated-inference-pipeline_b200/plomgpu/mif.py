@@ -15,8 +15,9 @@ once (plomgpu_mif_*).  This module restates the host part of the reference's
   ``switch`` iterations (update_theta_best_stable_mif, methods.c:394-420),
   then the Ionides 2006 formula (update_theta_best_king_mif, methods.c:429-467).
 
-Fitted parameters must take one value for every population / series (one
-group); initial conditions are not fitted (no fixed-lag smoothing).
+A parameter fitted per group contributes one component per group (the
+populations or series of the group read it); initial conditions are not
+fitted (no fixed-lag smoothing).
 """
 
 import numpy as np
@@ -29,34 +30,38 @@ class MifError(Exception):
 
 
 def components(problem, names=None):
-    """theta components: the estimated (sd_transf > 0) process and observation parameters."""
+    """theta components: one per group of every estimated (sd_transf > 0 in some group) process
+    and observation parameter."""
     m = problem.model
     params = problem.params
     out = []
     for kind, plist in (('proc', m.par_proc), ('obs', m.par_obs)):
         for idx, name in enumerate(plist):
             r = params.routers[name]
-            th = params.routers[name]
             if names is not None and name not in names:
                 continue
-            sd = _sd_transf(problem, name)
-            if names is None and not sd > 0.0:
+            sds = _sd_transf(problem, name, r)
+            if names is None and not max(sds) > 0.0:
                 continue
-            if r.n_gp != 1:
-                raise MifError('parameter %r has %d groups; fitted parameters take one value' % (name, r.n_gp))
-            out.append({'name': name, 'kind': kind, 'index': idx, 'bt': r.bt(0), 'sd_transf': sd,
-                        'theta0': th.transformed_guess(0)})
+            for g in range(r.n_gp):
+                members = None if r.n_gp == 1 else [c for c in range(len(r.map)) if r.map[c] == g]
+                out.append({'name': name, 'kind': kind, 'index': idx, 'g': g, 'bt': r.bt(g), 'sd_transf': sds[g],
+                            'theta0': r.transformed_guess(g), 'members': members})
     if not out:
         raise MifError('no parameter to fit (sd_transf > 0)')
+    if len(out) > 16:
+        raise MifError('%d components to fit; the engine takes at most 16' % len(out))
     return out
 
 
-def _sd_transf(problem, name):
+def _sd_transf(problem, name, router):
     from .theta import adapt_theta
     th = adapt_theta(problem.theta, problem.model)
-    g = th['parameter'][name]['group']
-    first = list(g.values())[0]
-    return float(first.get('sd_transf', {}).get('value', 0.0))
+    par = th['parameter'][name]
+    if 'follow' in par:
+        par = th['parameter'][par['follow']]
+    g = par['group']
+    return [float(g[gid].get('sd_transf', {}).get('value', 0.0)) for gid in router.group_name]
 
 
 class Mif(object):
@@ -72,8 +77,8 @@ class Mif(object):
         self.R = int(n_runs)
         self.Q = len(self.comp)
         self.a, self.b, self.switch = float(a), float(b), int(switch)
-        self.holder = MifDescHolder(self.R, [(c['kind'], c['index'], c['bt'], c['sd_transf'] > 0) for c in self.comp],
-                                    len(m.par_proc), len(m.par_obs))
+        self.holder = MifDescHolder(self.R, [(c['kind'], c['index'], c['bt'], c['sd_transf'] > 0, c['members'])
+                                             for c in self.comp], len(m.par_proc), len(m.par_obs), m.N_CAC, m.N_TS)
         self.plan = MifPlan(engine, problem, self.holder, precision=precision)
         n_data = problem.n_obs
         self.var = np.array([c['sd_transf'] ** 2 / n_data for c in self.comp])

@@ -59,7 +59,7 @@ class BatchDesc(C.Structure):
 
 class MifDesc(C.Structure):
     _fields_ = [('n_runs', C.c_int), ('n_theta', C.c_int), ('proc_slot', _ip), ('obs_slot', _ip),
-                ('theta_bt', _P(BackTransform)), ('estimated', _ip)]
+                ('theta_bt', _P(BackTransform)), ('estimated', _ip), ('proc_cac_slot', _ip), ('obs_ts_slot', _ip)]
 
 
 class ServerOpts(C.Structure):
@@ -452,23 +452,38 @@ class Batch(object):
 
 
 class MifDescHolder(object):
-    """plomgpu_mif_desc of n_runs runs over the components ``components``:
-    list of (kind, index, back_transform tuple, estimated) with kind 'proc' or 'obs'."""
+    """plomgpu_mif_desc of n_runs runs over the components ``components``: list of
+    (kind, index, back_transform tuple, estimated[, members]) with kind 'proc' or 'obs';
+    ``members`` lists the populations (process) or series (observation) a
+    component applies to when the parameter is fitted per group (None: all)."""
 
-    def __init__(self, n_runs, components, n_par_proc, n_par_obs):
+    def __init__(self, n_runs, components, n_par_proc, n_par_obs, n_cac=1, n_ts=1):
         self.R = int(n_runs)
         self.Q = len(components)
         self.proc_slot = np.full(max(n_par_proc, 1), -1, dtype=np.int32)
         self.obs_slot = np.full(max(n_par_obs, 1), -1, dtype=np.int32)
+        self.proc_cac = np.full((max(n_par_proc, 1), max(n_cac, 1)), -1, dtype=np.int32)
+        self.obs_ts = np.full((max(n_par_obs, 1), max(n_ts, 1)), -1, dtype=np.int32)
         self.bts = (BackTransform * max(self.Q, 1))()
         self.estimated = np.zeros(max(self.Q, 1), dtype=np.int32)
-        for q, (kind, idx, bt, est) in enumerate(components):
-            (self.proc_slot if kind == 'proc' else self.obs_slot)[idx] = q
+        for q, comp in enumerate(components):
+            kind, idx, bt, est = comp[:4]
+            members = comp[4] if len(comp) > 4 else None
+            slots, table = (self.proc_slot, self.proc_cac) if kind == 'proc' else (self.obs_slot, self.obs_ts)
+            if members is None:
+                slots[idx] = q
+            else:
+                slots[idx] = -2
+                table[idx, list(members)] = q
             f, s_, dur, a_, b_, mult = bt
             self.bts[q] = BackTransform(int(f), int(s_), int(dur), 0, float(a_), float(b_), float(mult))
             self.estimated[q] = 1 if est else 0
+        multi_p = bool(np.any(self.proc_slot == -2))
+        multi_o = bool(np.any(self.obs_slot == -2))
         self.desc = MifDesc(self.R, self.Q, _ptr(self.proc_slot, _ip), _ptr(self.obs_slot, _ip),
-                            C.cast(self.bts, _P(BackTransform)), _ptr(self.estimated, _ip))
+                            C.cast(self.bts, _P(BackTransform)), _ptr(self.estimated, _ip),
+                            _ptr(self.proc_cac, _ip) if multi_p else None,
+                            _ptr(self.obs_ts, _ip) if multi_o else None)
 
 
 class MifPlan(object):

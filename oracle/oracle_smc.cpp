@@ -584,16 +584,30 @@ int oracle_weight_and_resample(double* w, int J, double like_min, double U, doub
 
 namespace {
 
+// uni: parameters from the particle; a per-group one (cslot / tslot) picks
+// the component of the population / series
 struct HostMifEnv : HostEnv {
   double parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
   unsigned uni;
-  double par(int p, int cac) const { return ((uni >> p) & 1u) ? parp[p] : par_[p * M::N_CAC + cac]; }
+  const int* slot;
+  const int* cslot;
+  const double* nat;
+  double par(int p, int cac) const {
+    if (!((uni >> p) & 1u)) return par_[p * M::N_CAC + cac];
+    return slot[p] == -2 ? nat[cslot[p * M::N_CAC + cac]] : parp[p];
+  }
 };
 
 struct HostMifObsEnv : HostObsEnv {
   double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
   unsigned uni;
-  double par_ts(int p, int ts) const { return ((uni >> p) & 1u) ? obsp[p] : par_ts_[p * M::N_TS + ts]; }
+  const int* slot;
+  const int* tslot;
+  const double* nat;
+  double par_ts(int p, int ts) const {
+    if (!((uni >> p) & 1u)) return par_ts_[p * M::N_TS + ts];
+    return slot[p] == -2 ? nat[tslot[p * M::N_TS + ts]] : obsp[p];
+  }
 };
 
 template <int V, bool DRIFT>
@@ -671,13 +685,19 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
           memcpy(&bt, &mf->theta_bt[q], sizeof(bt));
           nat[q] = plomrt::back_transform<double>(th[(size_t)j * Q + q], bt);
         }
+        e.slot = mf->proc_slot;
+        e.cslot = mf->proc_cac_slot;
+        e.nat = nat;
+        oe.slot = mf->obs_slot;
+        oe.tslot = mf->obs_ts_slot;
+        oe.nat = nat;
         for (int k = 0; k < M::N_PAR_PROC; ++k) {
           e.parp[k] = mf->proc_slot[k] >= 0 ? nat[mf->proc_slot[k]] : 0.0;
-          if (mf->proc_slot[k] >= 0) e.uni |= 1u << k;
+          if (mf->proc_slot[k] >= 0 || mf->proc_slot[k] == -2) e.uni |= 1u << k;
         }
         for (int k = 0; k < M::N_PAR_OBS; ++k) {
           oe.obsp[k] = mf->obs_slot[k] >= 0 ? nat[mf->obs_slot[k]] : 0.0;
-          if (mf->obs_slot[k] >= 0) oe.uni |= 1u << k;
+          if (mf->obs_slot[k] >= 0 || mf->obs_slot[k] == -2) oe.uni |= 1u << k;
         }
         double* x = &Xn[(size_t)j * S];
         memcpy(x, &X[(size_t)j * S], sizeof(double) * S);

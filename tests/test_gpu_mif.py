@@ -13,14 +13,15 @@ pytestmark = pytest.mark.gpu
 def _setup(name, J, R, precision=64):
     eng = models.engine(name)
     p = models.make_problem(name, J=J, dt=1.0, precision=precision, seed=3)
-    sd = {'r0': 0.2, 'v': 0.1, 'rep': 0.1, 'sto': 0.3}
+    sd = {'r0': 0.2, 'v': 0.1, 'rep': 0.1, 'sto': 0.3, 'phi': 0.1}
     names = [n for n in sd if n in p.model.par_proc + p.model.par_obs]
     run = mif.Mif(eng, p, n_runs=R, names=names, sd_transf=sd, a=0.95, b=2.0)
     return eng, p, run
 
 
-@pytest.mark.parametrize('name,J,R', [('sir_short', 400, 3), ('seir3', 256, 2)])
+@pytest.mark.parametrize('name,J,R', [('sir_short', 400, 3), ('seir3', 256, 2), ('noise', 300, 2)])
 def test_mif_iteration_matches_oracle(name, J, R):
+    """noise: r0 (process) and phi (observation) are fitted per group, one component each."""
     eng, p, run = _setup(name, J, R)
     orc = models.build_oracle(name)
     rng = np.random.default_rng(1)

@@ -217,3 +217,27 @@ def test_oracle_summaries_are_consistent():
     nc, nsv = info.n_cac, info.n_par_sv * info.n_cac
     states = h[:, :nsv, 1].reshape(len(h), info.n_par_sv, nc).sum(axis=1)
     np.testing.assert_allclose(h[:, nsv:nsv + nc, 1], p.pop_size - states, rtol=1e-9)
+
+
+def test_mif_components_per_group():
+    """A parameter fitted per group gives one component per group; its slot is -2 and the
+    per-population / per-series table names the component of every member."""
+    from plomgpu import mif
+    from plomgpu.native import MifDescHolder
+    p = models.make_problem('noise', J=10, dt=1.0, precision=64)
+    comp = mif.components(p, names=['r0', 'v', 'phi'])
+    names = [(c['name'], c['g']) for c in comp]
+    assert names == [('r0', 0), ('r0', 1), ('v', 0), ('phi', 0), ('phi', 1)]
+    m = p.model
+    h = MifDescHolder(1, [(c['kind'], c['index'], c['bt'], True, c['members']) for c in comp],
+                      len(m.par_proc), len(m.par_obs), m.N_CAC, m.N_TS)
+    r0, v, phi = m.par_proc.index('r0'), m.par_proc.index('v'), m.par_obs.index('phi')
+    assert h.proc_slot[r0] == -2 and h.proc_slot[v] == 2
+    assert list(h.proc_cac[r0]) == [0, 1]
+    assert h.obs_slot[phi] == -2 and list(h.obs_ts[phi]) == [3, 4, 3, 3]
+    orc = models.build_oracle('noise')
+    import numpy as np
+    th = np.array([[c['theta0'] for c in comp]])
+    Q, T = len(comp), p.n_obs
+    ll, nf, bart, vt = orc.mif_iteration(p, h, th, np.full(Q, 0.05), np.full((T, Q), 0.01), np.zeros((T, Q)), 3)
+    assert np.isfinite(ll).all()
