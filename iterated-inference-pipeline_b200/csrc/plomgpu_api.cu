@@ -1041,10 +1041,28 @@ extern "C" int plomgpu_mif_create(const plomgpu_smc_desc* base, const plomgpu_mi
     return fail(PLOMGPU_EINVAL, "n_theta must be in [1, " + std::to_string(kMaxTheta) + "]");
   if (!m->theta_bt || !m->estimated || (M::N_PAR_PROC > 0 && !m->proc_slot) || (M::N_PAR_OBS > 0 && !m->obs_slot))
     return fail(PLOMGPU_EINVAL, "missing arrays");
-  for (int k = 0; k < M::N_PAR_PROC; ++k)
-    if (m->proc_slot[k] < -1 || m->proc_slot[k] >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad proc_slot");
-  for (int k = 0; k < M::N_PAR_OBS; ++k)
-    if (m->obs_slot[k] < -1 || m->obs_slot[k] >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad obs_slot");
+  for (int k = 0; k < M::N_PAR_PROC; ++k) {
+    const int sl = m->proc_slot[k];
+    if (sl < -2 || sl >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad proc_slot");
+    if (sl == -2) {
+      if (!m->proc_cac_slot) return fail(PLOMGPU_EINVAL, "proc_slot -2 needs proc_cac_slot");
+      for (int c = 0; c < M::N_CAC; ++c) {
+        const int q = m->proc_cac_slot[k * M::N_CAC + c];
+        if (q < 0 || q >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad proc_cac_slot");
+      }
+    }
+  }
+  for (int k = 0; k < M::N_PAR_OBS; ++k) {
+    const int sl = m->obs_slot[k];
+    if (sl < -2 || sl >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad obs_slot");
+    if (sl == -2) {
+      if (!m->obs_ts_slot) return fail(PLOMGPU_EINVAL, "obs_slot -2 needs obs_ts_slot");
+      for (int ts = 0; ts < M::N_TS; ++ts) {
+        const int q = m->obs_ts_slot[k * M::N_TS + ts];
+        if (q < 0 || q >= m->n_theta) return fail(PLOMGPU_EINVAL, "bad obs_ts_slot");
+      }
+    }
+  }
   if (base->crn_normals) return fail(PLOMGPU_EINVAL, "iterated filtering draws its own numbers");
   if ((long long)m->n_runs * base->J > (1LL << 31) - 1) return fail(PLOMGPU_EINVAL, "n_runs * J too large");
   return plan_create(base, out, false, false, false, false, m);
