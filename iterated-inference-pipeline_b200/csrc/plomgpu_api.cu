@@ -211,7 +211,7 @@ struct PropLaunch {
   explicit operator bool() const { return k != nullptr; }
 };
 
-template <class T, int V, bool DRIFT, bool CRN, bool MIF, bool PSR = false>
+template <class T, int V, bool DRIFT, bool CRN, bool MIF, bool PSR = false, bool MULTI = false>
 PropLaunch<T> pick4() {
   PropLaunch<T> l;
   if constexpr (PSR) {
@@ -226,7 +226,7 @@ PropLaunch<T> pick4() {
     l.per_block = L::PB;
     l.smem = L::bytes();
   } else {
-    l.k = &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp>;
+    l.k = &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp, false, MULTI>;
     l.bt = kBtProp;
     l.per_block = kBtProp;
     l.smem = propagate_smem_bytes<T, kSmem, kBtProp>();
@@ -234,23 +234,23 @@ PropLaunch<T> pick4() {
   return l;
 }
 
-template <class T, bool CRN, bool MIF>
+template <class T, bool CRN, bool MIF, bool MULTI = false>
 PropLaunch<T> pick_v(int v, bool drift) {
   if (drift) {
     if constexpr (M::N_DRIFT > 0) {
       switch (v) {
-        case 0: return pick4<T, 0, true, CRN, MIF>();
-        case 1: return pick4<T, 1, true, CRN, MIF>();
-        case 2: return pick4<T, 2, true, CRN, MIF>();
-        default: return pick4<T, 3, true, CRN, MIF>();
+        case 0: return pick4<T, 0, true, CRN, MIF, false, MULTI>();
+        case 1: return pick4<T, 1, true, CRN, MIF, false, MULTI>();
+        case 2: return pick4<T, 2, true, CRN, MIF, false, MULTI>();
+        default: return pick4<T, 3, true, CRN, MIF, false, MULTI>();
       }
     }
   }
   switch (v) {
-    case 0: return pick4<T, 0, false, CRN, MIF>();
-    case 1: return pick4<T, 1, false, CRN, MIF>();
-    case 2: return pick4<T, 2, false, CRN, MIF>();
-    default: return pick4<T, 3, false, CRN, MIF>();
+    case 0: return pick4<T, 0, false, CRN, MIF, false, MULTI>();
+    case 1: return pick4<T, 1, false, CRN, MIF, false, MULTI>();
+    case 2: return pick4<T, 2, false, CRN, MIF, false, MULTI>();
+    default: return pick4<T, 3, false, CRN, MIF, false, MULTI>();
   }
 }
 
@@ -267,7 +267,7 @@ PropLaunch<T> pick_psr(int noises_off) {
 }
 
 template <class T>
-PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif, bool psr = false) {
+PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif, bool psr = false, bool multi = false) {
   if (psr) {
     if (crn || mif) return PropLaunch<T>();
     return pick_psr<T>(noises_off);
@@ -276,7 +276,7 @@ PropLaunch<T> pick_prop(int noises_off, bool crn, bool mif, bool psr = false) {
   const bool d = drift_on(noises_off);
   if (mif) {
     if (crn) return PropLaunch<T>();
-    return pick_v<T, false, true>(v, d);
+    return multi ? pick_v<T, false, true, true>(v, d) : pick_v<T, false, true>(v, d);
   }
   if (crn) return pick_v<T, true, false>(v, d);
   return pick_v<T, false, false>(v, d);
@@ -328,7 +328,8 @@ int enqueue_filter(plomgpu_plan* p) {
   const int R = p->R;
   const size_t RJ = (size_t)R * J;
 
-  const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif, p->psr);
+  const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif, p->psr,
+                                        p->proc_cslot != nullptr || p->obs_tslot != nullptr);
   if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
   const size_t smem = kp.smem;
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1630,6 +1631,8 @@ void server_free(plomgpu_server* sv) {
   sv->cv.notify_all();
   if (sv->worker.joinable()) sv->worker.join();
   if (sv->ctl_h) __atomic_store_n(&sv->ctl_h->stop, 1, __ATOMIC_RELEASE);
+  for (int i = 1; i < plomgpu_server::kLoops; ++i)
+    if (sv->loop_stream[i]) cudaStreamSynchronize(sv->loop_stream[i]);
   if (sv->stream) cudaStreamSynchronize(sv->stream);
   for (auto& pp : sv->plans) {
     if (pp.plan) plan_free(pp.plan);
@@ -1643,6 +1646,10 @@ void server_free(plomgpu_server* sv) {
   if (sv->slots_h) cudaFreeHost(sv->slots_h);
   if (sv->ctl_h) cudaFreeHost(sv->ctl_h);
   if (sv->map_h) cudaFreeHost(sv->map_h);
+  for (int i = 1; i < plomgpu_server::kLoops; ++i) {
+    if (sv->loop_ev[i]) cudaEventDestroy(sv->loop_ev[i]);
+    if (sv->loop_stream[i]) cudaStreamDestroy(sv->loop_stream[i]);
+  }
   if (sv->kernel_ev) cudaEventDestroy(sv->kernel_ev);
   if (sv->stream) cudaStreamDestroy(sv->stream);
   delete sv;
@@ -1713,6 +1720,14 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->base.x0 = sv->x0_h.data();
   cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->kernel_ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) {
+    sv->loop_stream[0] = sv->stream;
+    sv->loop_ev[0] = sv->kernel_ev;
+    for (int i = 1; i < plomgpu_server::kLoops && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithFlags(&sv->loop_stream[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->loop_ev[i], cudaEventDisableTiming);
+    }
+  }
   if (e != cudaSuccess) {
     server_free(sv);
     return fail(PLOMGPU_ECUDA, std::string("stream/event: ") + cudaGetErrorString(e));

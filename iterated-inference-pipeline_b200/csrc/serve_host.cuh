@@ -121,6 +121,16 @@ struct plomgpu_server {
   cudaStream_t stream = nullptr;
   cudaEvent_t kernel_ev = nullptr;
   bool kernel_live = false;
+  // Instances of the device loop.  Each is launched with as many CTAs as
+  // requests wait for one (never more than `grid`, the CTAs the GPU holds at
+  // once), so that a loop serving a few requests leaves the other SMs to
+  // other work; a backlog beyond the live CTAs starts another instance on
+  // the next stream.  Instance 0 uses `stream` / `kernel_ev`.
+  static constexpr int kLoops = 4;
+  cudaStream_t loop_stream[kLoops] = {};
+  cudaEvent_t loop_ev[kLoops] = {};
+  int loop_grid[kLoops] = {};
+  bool loop_live[kLoops] = {};
   unsigned long long published = 0;
   std::vector<long long> slot_ticket;  // ring slot -> ticket (-1 free)
   std::vector<size_t> slot_off, slot_bytes;
@@ -198,13 +208,16 @@ ServeKernel<T> pick_serve(int noises_off) {
 }
 
 template <class T>
-int serve_launch(plomgpu_server* sv) {
+int serve_launch(plomgpu_server* sv, int inst, int grid) {
   ServeKernel<T> k = pick_serve<T>(sv->base.noises_off);
   if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
-  k<<<sv->grid, sv->bt, 0, sv->stream>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d, sv->d_head,
-                                         sv->d_pool, sv->idle_limit);
+  cudaStream_t st = sv->loop_stream[inst];
+  k<<<grid, sv->bt, 0, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d, sv->d_head, sv->d_pool,
+                             sv->idle_limit);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(sv->kernel_ev, sv->stream));
+  CK(cudaEventRecord(sv->loop_ev[inst], st));
+  sv->loop_live[inst] = true;
+  sv->loop_grid[inst] = grid;
   sv->kernel_live = true;
   sv->launches++;
   return PLOMGPU_OK;
@@ -347,14 +360,24 @@ void serve_pass(plomgpu_server* sv) {
       sv->launches++;
     }
   }
-  // (re)start the device loop when published requests are waiting for it
+  // (re)start device loops while published requests outnumber the live CTAs
   if (sv->persistent) {
-    bool waiting = false;
-    for (int i = 0; i < sv->ring && !waiting; ++i) waiting = sv->slot_ticket[i] >= 0;
-    if (sv->kernel_live && cudaEventQuery(sv->kernel_ev) == cudaSuccess) sv->kernel_live = false;
-    if (waiting && !sv->kernel_live) {
-      const int rc = (sv->precision == 64) ? serve_launch<double>(sv) : serve_launch<float>(sv);
-      if (rc) sv->last_error = g_err;
+    long long live_ctas = 0;
+    for (int i = 0; i < plomgpu_server::kLoops; ++i) {
+      if (sv->loop_live[i] && cudaEventQuery(sv->loop_ev[i]) == cudaSuccess) sv->loop_live[i] = false;
+      if (sv->loop_live[i]) live_ctas += sv->loop_grid[i];
+    }
+    sv->kernel_live = live_ctas > 0;
+    long long waiting = 0;
+    for (int i = 0; i < sv->ring; ++i) waiting += sv->slot_ticket[i] >= 0;
+    if (waiting > live_ctas && live_ctas < sv->grid) {
+      for (int i = 0; i < plomgpu_server::kLoops; ++i) {
+        if (sv->loop_live[i]) continue;
+        const int grid = (int)std::min<long long>(waiting - live_ctas, (long long)sv->grid - live_ctas);
+        const int rc = (sv->precision == 64) ? serve_launch<double>(sv, i, grid) : serve_launch<float>(sv, i, grid);
+        if (rc) sv->last_error = g_err;
+        break;
+      }
     }
   }
 }

@@ -162,17 +162,19 @@ struct StepArgs {
 };
 
 // environments with per-particle parameters (iterated filtering)
-// uni: parameters taken from the particle; multi: those of them whose
-// component depends on the population / series (one per group), looked up
-// in cslot and selected from the particle's natural values natq.
-template <class T>
+// uni: parameters taken from the particle; with MULTI, multi marks those of
+// them whose component depends on the population / series (one per group),
+// looked up in cslot and selected from the particle's natural values natq
+// (the instantiation without MULTI keeps the registers of the plain case).
+template <class T, bool MULTI>
 struct MifProcEnv : ProcEnv<T> {
   T parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
   unsigned uni, multi;
   const int* cslot;  // [N_PAR_PROC][N_CAC]
-  T natq[kMaxTheta];
+  T natq[MULTI ? kMaxTheta : 1];
   __device__ __forceinline__ T par(int p, int cac) const {
     if (!((uni >> p) & 1u)) return this->par_[p * M::N_CAC + cac];
+    if constexpr (!MULTI) return parp[p];
     if (!((multi >> p) & 1u)) return parp[p];
     const int q = __ldg(cslot + p * M::N_CAC + cac);
     T v = T(0);
@@ -183,13 +185,15 @@ struct MifProcEnv : ProcEnv<T> {
   }
 };
 
+template <bool MULTI>
 struct MifObsEnv : ObsEnv {
   double obsp[M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 1];
   unsigned uni, multi;
   const int* tslot;  // [N_PAR_OBS][N_TS]
-  double natq[kMaxTheta];
+  double natq[MULTI ? kMaxTheta : 1];
   __device__ __forceinline__ double par_ts(int p, int ts) const {
     if (!((uni >> p) & 1u)) return par_ts_[p * M::N_TS + ts];
+    if constexpr (!MULTI) return obsp[p];
     if (!((multi >> p) & 1u)) return obsp[p];
     const int q = __ldg(tslot + p * M::N_TS + ts);
     double v = 0.0;
@@ -216,7 +220,7 @@ constexpr size_t propagate_smem_bytes() {
 // PSR: the Poisson-system step (M::step_psr, the reference's default "psr"
 // implementation) instead of Euler-Maruyama; bit 1 of V turns its white
 // noise off.
-template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false>
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* s_coup = reinterpret_cast<T*>(smem_raw);
@@ -247,7 +251,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
 #pragma unroll
   for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);  // reset_inc
 
-  typedef typename std::conditional<MIF, MifProcEnv<T>, ProcEnv<T>>::type PEnv;
+  typedef typename std::conditional<MIF, MifProcEnv<T, MULTI>, ProcEnv<T>>::type PEnv;
   PEnv e;
   e.par_ = s_par;
   e.coup_ = s_coup;
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   const T dt = (T)tb.dt;
   const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id + (uint32_t)r);
 
-  typedef typename std::conditional<MIF, MifObsEnv, ObsEnv>::type OEnv;
+  typedef typename std::conditional<MIF, MifObsEnv<MULTI>, ObsEnv>::type OEnv;
   OEnv oe;
   oe.par_ts_ = tb.par_ts;
   oe.cov_ts_ = a.cov_ts;
@@ -288,8 +292,10 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     e.uni = 0u;
     e.multi = 0u;
     e.cslot = tb.proc_cslot;
+    if constexpr (MULTI) {
 #pragma unroll
-    for (int q = 0; q < kMaxTheta; ++q) e.natq[q] = (T)nat[q];
+      for (int q = 0; q < kMaxTheta; ++q) e.natq[q] = (T)nat[q];
+    }
 #pragma unroll
     for (int k = 0; k < M::N_PAR_PROC; ++k) {
       const int slot = __ldg(tb.proc_slot + k);
@@ -304,8 +310,10 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     oe.uni = 0u;
     oe.multi = 0u;
     oe.tslot = tb.obs_tslot;
+    if constexpr (MULTI) {
 #pragma unroll
-    for (int q = 0; q < kMaxTheta; ++q) oe.natq[q] = nat[q];
+      for (int q = 0; q < kMaxTheta; ++q) oe.natq[q] = nat[q];
+    }
 #pragma unroll
     for (int k = 0; k < M::N_PAR_OBS; ++k) {
       const int slot = __ldg(tb.obs_slot + k);
