@@ -121,12 +121,14 @@ struct plomgpu_server {
   cudaStream_t stream = nullptr;
   cudaEvent_t kernel_ev = nullptr;
   bool kernel_live = false;
-  // Instances of the device loop.  Each is launched with as many CTAs as
-  // requests wait for one (never more than `grid`, the CTAs the GPU holds at
-  // once), so that a loop serving a few requests leaves the other SMs to
-  // other work; a backlog beyond the live CTAs starts another instance on
-  // the next stream.  Instance 0 uses `stream` / `kernel_ev`.
-  static constexpr int kLoops = 4;
+  // Instances of the device loop.  Each is launched with about as many CTAs
+  // as requests wait for one (at least 8, and at least half the live CTAs so
+  // that a burst is met in a few launches; never more than `grid`, the CTAs
+  // the GPU holds at once), so that a loop serving a few requests leaves the
+  // other SMs to other work; a backlog beyond the live CTAs starts another
+  // instance on the next stream, and CTAs that find no work for a while
+  // return.  Instance 0 uses `stream` / `kernel_ev`.
+  static constexpr int kLoops = 8;
   cudaStream_t loop_stream[kLoops] = {};
   cudaEvent_t loop_ev[kLoops] = {};
   int loop_grid[kLoops] = {};
@@ -373,7 +375,8 @@ void serve_pass(plomgpu_server* sv) {
     if (waiting > live_ctas && live_ctas < sv->grid) {
       for (int i = 0; i < plomgpu_server::kLoops; ++i) {
         if (sv->loop_live[i]) continue;
-        const int grid = (int)std::min<long long>(waiting - live_ctas, (long long)sv->grid - live_ctas);
+        const long long want = std::max<long long>(std::max<long long>(waiting - live_ctas, (live_ctas + 1) / 2), 8);
+        const int grid = (int)std::min<long long>(want, (long long)sv->grid - live_ctas);
         const int rc = (sv->precision == 64) ? serve_launch<double>(sv, i, grid) : serve_launch<float>(sv, i, grid);
         if (rc) sv->last_error = g_err;
         break;
