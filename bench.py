@@ -149,6 +149,21 @@ def ncu_traffic(workload):
         return None
 
 
+def max_over_ranks(x, dist, device):
+    """The slowest rank's time (every rank runs an independent replica)."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(psteps_per_rank, world, ms_step):
+    """Whole-job particle-steps/s: every rank advances its own filter of psteps_per_rank
+    particle-steps in a step that lasts the slowest rank's ms_step (weak scaling)."""
+    return psteps_per_rank * world / (ms_step / 1000.0)
+
+
 def ncu_issue(workload):
     """Issue-side utilisation of the propagate kernel from the committed ncu summary (the bound that
     binds: the full-noise step is instruction-issue bound, not HBM bound)."""
@@ -488,12 +503,9 @@ def main():
     tot_prop, n_prop = plan.propagate_time()  # last launch
     res = plan.results()
     ms_step = ms_total / args.steps
-    t = torch.tensor([ms_step], device='cuda')
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_step = float(t.item())
+    ms_step = max_over_ranks(ms_step, dist, 'cuda')
     psteps = prob.J * prob.n_obs
-    value = psteps * world / (ms_step / 1000.0)
+    value = replica_throughput(psteps, world, ms_step)
     kernels_per_step = plan.kernel_count
     plan.close()
 
@@ -509,10 +521,8 @@ def main():
     h2d = sum(a.nbytes for a in h.arrays.values())
     d2h = 8 * 2 * prob.n_obs + 16
     e2e_s = statistics.median(e2e_times) if e2e_times else float('nan')
-    tt = torch.tensor([e2e_s], device='cuda')
-    if dist is not None:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    e2e_value = psteps * world / float(tt.item()) if e2e_times else None
+    e2e_max = max_over_ranks(e2e_s, dist, 'cuda')
+    e2e_value = psteps * world / e2e_max if e2e_times else None
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()

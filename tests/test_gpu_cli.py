@@ -77,6 +77,14 @@ def test_smc_cli_outputs(model_dir):
     assert len(rows) == (p.n_obs + 1) * 500 and all(len(r) == len(head) for r in rows[:1000])
     done = json.load(open(os.path.join(d, '.done_0.json')))
     assert 'parameter' in done
+    # the reference's default implementation (psr) and the deterministic skeleton (ode)
+    out = _run(d, 'smc', '-J', '300', '-s', '1', '-i', '5')
+    assert 'logV:' in out
+    head, rows = _csv(os.path.join(d, 'trace_5.csv'))
+    assert np.isfinite(float(rows[0][-1]))
+    out = _run(d, 'smc', 'ode', '-J', '1', '-i', '6')
+    head, rows = _csv(os.path.join(d, 'hat_6.csv'))
+    assert all(r[1] == r[2] == r[3] for r in rows[1:])  # one deterministic path: the interval collapses
     # -P: theta on stdout, no .done file
     out = _run(d, 'smc', 'sde', '-J', '200', '-s', '1', '-P', '-i', '4', '-b', '-e', '-d')
     assert json.loads(out)['parameter']
