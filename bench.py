@@ -29,6 +29,8 @@ sys.path.insert(0, os.path.join(ROOT, 'iterated-inference-pipeline_b200'))
 WORKLOADS = {
     # name: (model library, J, observation intervals, dt in days)
     'seir20x2': ('seir20x2', 100000, 520, 1.0),
+    # the same filter with the reference's default implementation (Poisson system with stochastic rates)
+    'seir20x2_psr': ('seir20x2', 100000, 520, 1.0),
     'sir': ('sir', 1000, 52, 1.0),
     # 4096 SIR parameter sets, J in 256..16384, T in 52..520 weeks, one persistent launch
     'sir_batch': ('sir', None, None, 1.0),
@@ -59,7 +61,8 @@ def workload_problem(name, precision=32, seed=0, J=None, nb_obs=-1):
     lib, J0, T, dt = WORKLOADS[name]
     c, p, l, th = workloads.load(lib)
     m = model.PlomModel(c, p, l)
-    return problem.Problem(m, m.settings(), th, J=J or J0, dt=dt, precision=precision, seed=seed, nb_obs=nb_obs)
+    return problem.Problem(m, m.settings(), th, J=J or J0, dt=dt, precision=precision, seed=seed, nb_obs=nb_obs,
+                           psr=name.endswith('_psr'))
 
 
 def state_words(prob):
@@ -535,7 +538,9 @@ def main():
             'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
             'config': {'workload': args.workload, 'J': prob.J, 'T': prob.n_obs, 'K': int(prob.n_sub[0]),
-                       'state_words': state_words(prob), 'noise': 'sde full (demographic + environmental)',
+                       'state_words': state_words(prob),
+                       'noise': ('psr (multinomial + Poisson + Gamma white noise)' if prob.psr else
+                                 'sde full (demographic + environmental)'),
                        'parallelism': 'replicas' if world > 1 else 'single GPU',
                        'l2': 'inputs larger than L2 (two state generations of %.0f MB)' %
                              (2 * state_words(prob) * 4 * prob.J / 1e6)},

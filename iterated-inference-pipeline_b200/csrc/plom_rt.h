@@ -133,7 +133,7 @@ PLOM_HD double finish_loglik(double ll, int floor_hits, int n_ts) { return floor
 struct U4 { uint32_t x, y, z, w; };
 
 PLOM_HD uint32_t mulhilo32(uint32_t a, uint32_t b, uint32_t* hi) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && !defined(PLOM_PHILOX_WIDE)
   *hi = __umulhi(a, b);
   return a * b;
 #else
