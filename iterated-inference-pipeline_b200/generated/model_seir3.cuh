@@ -26,6 +26,7 @@ struct Model {
   template <class T>
   struct Pre {
     T yf_I[N_CAC];
+    T tt_0;  // cos(((T(1)/T(182)))*T(3.141592653589793)*t)
     int unused;
   };
   template <int V, bool DRIFT, class T, class X, class E>
@@ -40,7 +41,7 @@ struct Model {
     PLOM_UNROLL
     for (int c2 = 0; c2 < N_CAC; ++c2) foi_I += e.coupling(cac, c2) * pre.yf_I[c2];
     const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-    const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
+    const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))*foi_I;
     const T r2 = e.par(2, cac);
     const T r3 = e.par(1, cac);
     const T r4 = e.par(5, cac);
@@ -124,6 +125,7 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     PLOM_UNROLL
     for (int c2 = 0; c2 < N_CAC; ++c2) {
       pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
@@ -168,6 +170,9 @@ struct Model {
     PLOM_UNROLL
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     for (int c2 = tm.rank; c2 < N_CAC; c2 += TM::TP) pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
+    if (tm.rank == 0) {
+      pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
+    }
     tm.sync();
     PLOM_PRAGMA_CAC
     for (int gi = tm.rank; gi < NG; gi += TM::TP) {
@@ -208,6 +213,7 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
     for (int cac = 0; cac < N_CAC; ++cac) {
       const T xo_S = x[0*N_CAC+cac];
@@ -217,7 +223,7 @@ struct Model {
       T foi_I = T(0);
       for (int c2 = 0; c2 < N_CAC; ++c2) foi_I += e.coupling(cac, c2) * pre.yf_I[c2];
       const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-      const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
+      const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))*foi_I;
       const T r2 = e.par(2, cac);
       const T r3 = e.par(1, cac);
       const T r4 = e.par(5, cac);
@@ -253,7 +259,7 @@ struct Model {
       wn_0 = plomrt::gamma(rs, ddt / (sd * sd), sd * sd) / ddt;
     }
     const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-    const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))*foi_I;
+    const T r1 = e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))*foi_I;
     const T r2 = e.par(2, cac);
     const T r3 = e.par(1, cac);
     const T r4 = e.par(5, cac);
@@ -350,6 +356,7 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
     for (int cac = 0; cac < N_CAC; ++cac) {
       plomrt::UniformStream rs;

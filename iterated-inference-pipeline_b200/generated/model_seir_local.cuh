@@ -25,6 +25,7 @@ struct Model {
   }
   template <class T>
   struct Pre {
+    T tt_0;  // cos(((T(1)/T(182)))*T(3.141592653589793)*t)
     int unused;
   };
   template <int V, bool DRIFT, class T, class X, class E>
@@ -36,7 +37,7 @@ struct Model {
     const T xo_I = x[2*N_CAC+cac];
     const T xo_R = x[3*N_CAC+cac];
     const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-    const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))/(xo_E + xo_I + xo_R + xo_S);
+    const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))/(xo_E + xo_I + xo_R + xo_S);
     const T r2 = e.par(2, cac);
     const T r3 = e.par(1, cac);
     const T r4 = e.par(5, cac);
@@ -120,6 +121,7 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     PLOM_PRAGMA_CAC
     for (int cac0 = 0; cac0 < NMAIN; cac0 += G) {
       T nz[NW * G > 0 ? NW * G : 1];
@@ -159,6 +161,10 @@ struct Model {
     T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
     PLOM_UNROLL
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    if (tm.rank == 0) {
+      pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
+    }
+    tm.sync();
     PLOM_PRAGMA_CAC
     for (int gi = tm.rank; gi < NG; gi += TM::TP) {
       const int cac0 = gi * G;
@@ -198,13 +204,14 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     for (int cac = 0; cac < N_CAC; ++cac) {
       const T xo_S = x[0*N_CAC+cac];
       const T xo_E = x[1*N_CAC+cac];
       const T xo_I = x[2*N_CAC+cac];
       const T xo_R = x[3*N_CAC+cac];
       const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-      const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))/(xo_E + xo_I + xo_R + xo_S);
+      const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))/(xo_E + xo_I + xo_R + xo_S);
       const T r2 = e.par(2, cac);
       const T r3 = e.par(1, cac);
       const T r4 = e.par(5, cac);
@@ -238,7 +245,7 @@ struct Model {
       wn_0 = plomrt::gamma(rs, ddt / (sd * sd), sd * sd) / ddt;
     }
     const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
-    const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*cos(((T(1)/T(182)))*T(3.141592653589793)*t) + T(1))/(xo_E + xo_I + xo_R + xo_S);
+    const T r1 = xo_I*e.par(0, cac)*e.par(1, cac)*(T(0.3)*pre.tt_0 + T(1))/(xo_E + xo_I + xo_R + xo_S);
     const T r2 = e.par(2, cac);
     const T r3 = e.par(1, cac);
     const T r4 = e.par(5, cac);
@@ -335,6 +342,7 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;
     Pre<T> pre;
     pre.unused = 0;
+    pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     for (int cac = 0; cac < N_CAC; ++cac) {
       plomrt::UniformStream rs;
       rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);

@@ -30,6 +30,9 @@ Differences from the reference's generated C, each one forced by the target:
   random numbers possible between the GPU and the oracle.
 """
 
+import os
+import re
+
 import sympy
 from sympy.printing.c import C99CodePrinter
 
@@ -127,6 +130,52 @@ def _sympify(expr, names, drop_correct_rate):
     return sympy.sympify(s, locals=local)
 
 
+# Calls of the rates that depend on time only (seasonal forcing such as
+# cos(2 pi t / 364)) are evaluated once per substep instead of once per cac.
+HOIST_TIME_TERMS = os.environ.get('PLOM_HOIST_TIME_TERMS', '1') != '0'
+_TIME_FUNCS = ('cos', 'sin', 'tan', 'exp', 'log', 'sqrt', 'pow', 'cosh', 'sinh', 'tanh')
+
+
+def _time_only(arg):
+    names = set(re.findall(r'[A-Za-z_][A-Za-z_0-9]*', arg))
+    return names <= {'t', 'T'} and 't' in names
+
+
+def hoist_time_terms(exprs):
+    """(expressions with time-only calls replaced by pre.tt_k, [call text of tt_k])."""
+    terms = []
+    out = []
+    for e in exprs:
+        i = 0
+        res = ''
+        while i < len(e):
+            m = re.compile(r'\b(%s)\(' % '|'.join(_TIME_FUNCS)).search(e, i)
+            if not m:
+                res += e[i:]
+                break
+            depth, j = 0, m.end() - 1
+            while j < len(e):
+                if e[j] == '(':
+                    depth += 1
+                elif e[j] == ')':
+                    depth -= 1
+                    if depth == 0:
+                        break
+                j += 1
+            call = e[m.start():j + 1]
+            arg = e[m.end():j]
+            if _time_only(arg):
+                if call not in terms:
+                    terms.append(call)
+                res += e[i:m.start()] + 'pre.tt_%d' % terms.index(call)
+                i = j + 1
+            else:
+                res += e[i:m.end()]
+                i = m.end()
+        out.append(res)
+    return out, terms
+
+
 class Emitter(object):
     """Builds the model header for one :class:`PlomModel` with context."""
 
@@ -187,6 +236,7 @@ class Emitter(object):
                 rates.append(r['rate'])
         sm = self._proc_symmap()
         caches = [self.c_expr(r, sm) for r in rates]
+        caches, self.time_terms = hoist_time_terms(caches) if HOIST_TIME_TERMS else (caches, [])
         univ = (UNIVERSE, m.remainder)
 
         def term(r):
@@ -331,6 +381,8 @@ class Emitter(object):
         a('  struct Pre {')
         for s in foi_states:
             a('    T yf_%s[N_CAC];' % s)
+        for k in range(len(self.time_terms)):
+            a('    T tt_%d;  // %s' % (k, self.time_terms[k]))
         a('    int unused;')
         a('  };')
         # one compartment-age class: rates, noises, equations, incidence
@@ -425,6 +477,8 @@ class Emitter(object):
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
+        for k, tt in enumerate(self.time_terms):
+            a('    pre.tt_%d = %s;' % (k, tt))
         for s in foi_states:
             si = m.par_sv.index(s)
             a('    PLOM_UNROLL')
@@ -488,7 +542,12 @@ class Emitter(object):
             si = m.par_sv.index(s_)
             a('    for (int c2 = tm.rank; c2 < N_CAC; c2 += TM::TP) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;'
               % (s_, si, self._npop_expr('c2')))
-        if foi_states:
+        if self.time_terms:
+            a('    if (tm.rank == 0) {')
+            for k, tt in enumerate(self.time_terms):
+                a('      pre.tt_%d = %s;' % (k, tt))
+            a('    }')
+        if foi_states or self.time_terms:
             a('    tm.sync();')
         a('    PLOM_PRAGMA_CAC')
         a('    for (int gi = tm.rank; gi < NG; gi += TM::TP) {')
@@ -537,6 +596,8 @@ class Emitter(object):
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
+        for k, tt in enumerate(self.time_terms):
+            a('    pre.tt_%d = %s;' % (k, tt))
         for s_ in foi_states:
             si = m.par_sv.index(s_)
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
@@ -718,6 +779,8 @@ class Emitter(object):
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
+        for k, tt in enumerate(self.time_terms):
+            a('    pre.tt_%d = %s;' % (k, tt))
         for s_ in foi_states:
             si = m.par_sv.index(s_)
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
