@@ -24,9 +24,39 @@
 
 #include "plom_rt.h"
 
+// The samplers are real calls on the device (one copy of their code for the
+// many call sites of a step): inlined, the step's code overflows the
+// instruction cache.
+#if defined(__CUDACC__)
+#ifndef PLOM_PSR_INLINE
+#define PLOM_SAMPLER __host__ __device__ __noinline__
+#else
+#define PLOM_SAMPLER PLOM_HD
+#endif
+#else
+#define PLOM_SAMPLER inline
+#endif
+
 namespace plomrt {
 
 enum { STREAM_PSR = 4 };
+
+// double-precision elementary functions of the samplers, called rather than
+// inlined at every use (same values; less code)
+PLOM_SAMPLER double s_log(double x) { return log(x); }
+PLOM_SAMPLER double s_exp(double x) { return exp(x); }
+PLOM_SAMPLER double s_pow(double x, double y) { return pow(x, y); }
+PLOM_SAMPLER double s_lgamma(double x) { return lgamma(x); }
+PLOM_SAMPLER double s_cos(double x) { return cos(x); }
+
+// two 53-bit uniforms of Philox block (j, n, group, STREAM_PSR + 16 block)
+PLOM_SAMPLER void psr_uniform_pair(PhiloxKey key, uint32_t j, uint32_t n, uint32_t group, uint32_t block, double* a,
+                                   double* b) {
+  const U4 c = {j, n, group, (uint32_t)STREAM_PSR + (block << 4)};
+  const U4 r = philox4x32_10(c, key.k0, key.k1);
+  *a = u01d(r.x, r.y);
+  *b = u01d(r.z, r.w);
+}
 
 // Uniforms of one (particle, interval, substep, cac) group: Philox counter
 // (x = particle slot, y = interval, z = substep * (N_CAC + 1) + cac,
@@ -52,22 +82,21 @@ struct UniformStream {
       has = false;
       return cache;
     }
-    const U4 c = {j, n, group, (uint32_t)STREAM_PSR + (block << 4)};
+    double first;
+    psr_uniform_pair(key, j, n, group, block, &first, &cache);
     ++block;
-    const U4 r = philox4x32_10(c, key.k0, key.k1);
-    cache = u01d(r.z, r.w);
     has = true;
-    return u01d(r.x, r.y);
+    return first;
   }
   PLOM_HD double normal() {
     const double u1 = next(), u2 = next();
-    return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    return sqrt(-2.0 * s_log(u1)) * s_cos(6.283185307179586 * u2);
   }
 };
 
 // log k! - Stirling's approximation of it (the correction term of BTRD)
 PLOM_HD double stirling_correction(double k) {
-  if (k < 10.0) return lgamma(k + 1.0) - ((k + 0.5) * log(k + 1.0) - (k + 1.0) + 0.9189385332046728);
+  if (k < 10.0) return s_lgamma(k + 1.0) - ((k + 0.5) * s_log(k + 1.0) - (k + 1.0) + 0.9189385332046728);
   const double r = 1.0 / (k + 1.0), r2 = r * r;
   return (1.0 / 12.0 - (1.0 / 360.0 - (1.0 / 1260.0) * r2) * r2) * r;
 }
@@ -79,7 +108,7 @@ constexpr int kMaxRejection = 1000;
 PLOM_HD double binomial_inversion(UniformStream& rs, double n, double p) {
   const double q = 1.0 - p;
   const double s = p / q, a = (n + 1.0) * s;
-  const double r0 = pow(q, n);
+  const double r0 = s_pow(q, n);
   for (int round = 0; round < kMaxRejection; ++round) {
     double u = rs.next(), r = r0, x = 0.0;
     while (u > r) {
@@ -134,15 +163,15 @@ PLOM_HD double binomial_btrd(UniformStream& rs, double n, double p) {
       continue;
     }
     // squeeze
-    v = log(v);
+    v = s_log(v);
     const double rho = (km / npq) * (((km / 3.0 + 0.625) * km + 1.0 / 6.0) / npq + 0.5);
     const double t = -km * km / (2.0 * npq);
     if (v < t - rho) return k;
     if (v > t + rho) continue;
     const double nm = n - m + 1.0;
-    const double h = (m + 0.5) * log((m + 1.0) / (r * nm)) + stirling_correction(m) + stirling_correction(n - m);
+    const double h = (m + 0.5) * s_log((m + 1.0) / (r * nm)) + stirling_correction(m) + stirling_correction(n - m);
     const double nk = n - k + 1.0;
-    if (v <= h + (n + 1.0) * log(nm / nk) + (k + 0.5) * log(nk * r / (k + 1.0)) - stirling_correction(k) -
+    if (v <= h + (n + 1.0) * s_log(nm / nk) + (k + 0.5) * s_log(nk * r / (k + 1.0)) - stirling_correction(k) -
                  stirling_correction(n - k))
       return k;
   }
@@ -150,7 +179,7 @@ PLOM_HD double binomial_btrd(UniformStream& rs, double n, double p) {
 }
 
 // Binomial(n, p), n a non-negative integer held in a double
-PLOM_HD double binomial(UniformStream& rs, double n, double p) {
+PLOM_SAMPLER double binomial(UniformStream& rs, double n, double p) {
   if (n <= 0.0 || !(p > 0.0)) return 0.0;
   if (p >= 1.0) return n;
   const bool flip = p > 0.5;  // sample the smaller tail
@@ -159,11 +188,11 @@ PLOM_HD double binomial(UniformStream& rs, double n, double p) {
   return flip ? n - x : x;
 }
 
-PLOM_HD double poisson(UniformStream& rs, double mu) {
+PLOM_SAMPLER double poisson(UniformStream& rs, double mu) {
   if (!(mu > 0.0)) return 0.0;
   if (mu < 10.0) {
     for (int round = 0; round < kMaxRejection; ++round) {
-      double u = rs.next(), p = exp(-mu), x = 0.0;
+      double u = rs.next(), p = s_exp(-mu), x = 0.0;
       while (u > p) {
         u -= p;
         x += 1.0;
@@ -179,7 +208,7 @@ PLOM_HD double poisson(UniformStream& rs, double mu) {
   const double a = -0.059 + 0.02483 * b;
   const double inv_alpha = 1.1239 + 1.1328 / (b - 3.4);
   const double vr = 0.9277 - 3.6224 / (b - 2.0);
-  const double lmu = log(mu);
+  const double lmu = s_log(mu);
   for (int round = 0; round < kMaxRejection; ++round) {
     const double u = rs.next() - 0.5;
     const double v = rs.next();
@@ -187,17 +216,17 @@ PLOM_HD double poisson(UniformStream& rs, double mu) {
     const double k = floor((2.0 * a / us + b) * u + mu + 0.43);
     if (us >= 0.07 && v <= vr) return k;
     if (k < 0.0 || (us < 0.013 && v > us)) continue;
-    if (log(v) + log(inv_alpha) - log(a / (us * us) + b) <= -mu + k * lmu - lgamma(k + 1.0)) return k;
+    if (s_log(v) + s_log(inv_alpha) - s_log(a / (us * us) + b) <= -mu + k * lmu - s_lgamma(k + 1.0)) return k;
   }
   return floor(mu);
 }
 
 // Gamma with shape a and scale theta
-PLOM_HD double gamma(UniformStream& rs, double a, double theta) {
+PLOM_SAMPLER double gamma(UniformStream& rs, double a, double theta) {
   if (!(a > 0.0) || !(theta > 0.0)) return 0.0;
   double boost = 1.0;
   if (a < 1.0) {
-    boost = pow(rs.next(), 1.0 / a);
+    boost = s_pow(rs.next(), 1.0 / a);
     a += 1.0;
   }
   const double d = a - 1.0 / 3.0, c = 1.0 / sqrt(9.0 * d);
@@ -208,7 +237,7 @@ PLOM_HD double gamma(UniformStream& rs, double a, double theta) {
     v = v * v * v;
     const double u = rs.next();
     if (u < 1.0 - 0.0331 * z * z * z * z) return d * v * theta * boost;
-    if (log(u) < 0.5 * z * z + d * (1.0 - v + log(v))) return d * v * theta * boost;
+    if (s_log(u) < 0.5 * z * z + d * (1.0 - v + s_log(v))) return d * v * theta * boost;
   }
   return d * theta * boost;
 }

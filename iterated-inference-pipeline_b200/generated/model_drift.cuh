@@ -252,7 +252,7 @@ struct Model {
       const double sum = h0 + h1;
       double p[3];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
         p[2] = 1.0 - p[0] - p[1];
@@ -271,7 +271,7 @@ struct Model {
       const double sum = h0 + h1;
       double p[3];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
         p[2] = 1.0 - p[0] - p[1];

@@ -256,7 +256,7 @@ struct Model {
       const double sum = h0 + h1;
       double p[3];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
         p[2] = 1.0 - p[0] - p[1];
@@ -275,7 +275,7 @@ struct Model {
       const double sum = h0 + h1;
       double p[3];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
         p[2] = 1.0 - p[0] - p[1];
@@ -294,7 +294,7 @@ struct Model {
       const double sum = h0 + h1;
       double p[3];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
         p[2] = 1.0 - p[0] - p[1];
@@ -312,7 +312,7 @@ struct Model {
       const double sum = h0;
       double p[2];
       if (sum > 0.0) {
-        const double ome = 1.0 - exp(-sum);
+        const double ome = 1.0 - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = 1.0 - p[0];
       } else {

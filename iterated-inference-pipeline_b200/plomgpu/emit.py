@@ -712,7 +712,7 @@ class Emitter(object):
             a('      const double sum = %s;' % ' + '.join('h%d' % q for q in range(len(exits))))
             a('      double p[%d];' % K)
             a('      if (sum > 0.0) {')
-            a('        const double ome = 1.0 - exp(-sum);')
+            a('        const double ome = 1.0 - plomrt::s_exp(-sum);')
             for q in range(len(exits)):
                 a('        p[%d] = ome * (h%d / sum);' % (q, q))
             a('        p[%d] = 1.0%s;' % (len(exits), ''.join(' - p[%d]' % q for q in range(len(exits)))))
