@@ -116,10 +116,16 @@ struct Model {
     x[3*N_CAC+cac] = (f_R < T(0)) ? T(0) : f_R;
   }
   // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)
+  // (PLOM_MAX_DRAW_GROUP caps the group of blocks of more than 2 normals, the FP32
+  // generator, leaving part of the last block of a group unused)
   static constexpr PLOM_HD int draw_group(int nw, int per_block) {
     int g = 1;
     while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;
-    return (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;
+    g = (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;
+#ifdef PLOM_MAX_DRAW_GROUP
+    if (per_block > 2 && g > PLOM_MAX_DRAW_GROUP) g = PLOM_MAX_DRAW_GROUP;
+#endif
+    return g;
   }
   template <int V, bool DRIFT, class T, class X, class E, class D>
   PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {

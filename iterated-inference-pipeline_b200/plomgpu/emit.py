@@ -462,10 +462,16 @@ class Emitter(object):
         a('  }')
         # one Euler-Maruyama substep of the whole particle
         a('  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)')
+        a('  // (PLOM_MAX_DRAW_GROUP caps the group of blocks of more than 2 normals, the FP32')
+        a('  // generator, leaving part of the last block of a group unused)')
         a('  static constexpr PLOM_HD int draw_group(int nw, int per_block) {')
         a('    int g = 1;')
         a('    while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;')
-        a('    return (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;')
+        a('    g = (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;')
+        a('#ifdef PLOM_MAX_DRAW_GROUP')
+        a('    if (per_block > 2 && g > PLOM_MAX_DRAW_GROUP) g = PLOM_MAX_DRAW_GROUP;')
+        a('#endif')
+        a('    return g;')
         a('  }')
         a('  template <int V, bool DRIFT, class T, class X, class E, class D>')
         a('  PLOM_HD static void step(X& x, const T t, const T dt, const E& e, D& draws) {')
