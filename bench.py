@@ -51,8 +51,8 @@ def parse():
     ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
-    ap.add_argument('--plan-pool', type=int, default=2, help='serve: concurrent plans of the shared-memory model '
-                    '(2 measured 1.5x faster than 8 on the SEIR 20x2 requests)')
+    ap.add_argument('--plan-pool', type=int, default=4, help='serve: concurrent plans of the shared-memory model '
+                    '(the SEIR 20x2 requests took 29.3 / 24.9 / 24.5 s with 2 / 3 / 4)')
     return ap.parse_args()
 
 
@@ -393,8 +393,9 @@ def run_serve(args, window_s=0.25, rate=2000.0):
     k = 0
 
     def harvest(block=False):
-        for tk in list(outstanding):
-            ch, cl, th = outstanding[tk]
+        for key in list(outstanding):
+            cl, tk = key
+            ch, _, th = outstanding[key]
             r = classes[cl]['server'].poll(tk) if not block else classes[cl]['server'].wait(tk, 600.0)
             if r is None:
                 continue
@@ -405,7 +406,7 @@ def run_serve(args, window_s=0.25, rate=2000.0):
             if np.log(rng.uniform()) < ll - c['ll']:
                 c['theta'], c['ll'] = th, ll
                 c['accepted'] += 1
-            del outstanding[tk]
+            del outstanding[key]
 
     with Clocks(int(os.environ.get('LOCAL_RANK', '0'))) as clk:
         while k < len(arrivals):
@@ -416,7 +417,8 @@ def run_serve(args, window_s=0.25, rate=2000.0):
                 th = c['theta'] * np.exp(0.02 * rng.standard_normal(c['theta'].shape))
                 sv = classes[c['cls']]['server']
                 tk = sv.submit(classes[c['cls']]['J'], par_cac=th, seed=int(1 + k))
-                outstanding[tk if c['cls'] == 'sir' else tk] = (ch, c['cls'], th)
+                # tickets are numbered per server: key them by class too
+                outstanding[(c['cls'], tk)] = (ch, c['cls'], th)
                 k += 1
             else:
                 harvest()

@@ -322,9 +322,9 @@ typedef struct plomgpu_server_opts {
     int max_J;              /* largest particle count of a request */
     double memory_budget;   /* bytes of HBM the requests may hold (0: 150e9) */
     int ring_slots;         /* requests in flight on the device loop (0: 1024) */
-    int plan_pool;          /* concurrent plans for models served per plan (0: 2; one SEIR 20x2 filter of
-                             * 2e4 particles nearly fills a B200, and 8 concurrent plans measured 1.5x
-                             * slower than 2) */
+    int plan_pool;          /* concurrent plans for models served per plan (0: 4; one SEIR 20x2 filter of
+                             * 2e4 particles fills half of a B200's resident slots: 2 / 3 / 4 plans run
+                             * 1.6 / 2.0 / 2.1x the filters per second of one) */
     int precision;          /* 32 or 64 */
 } plomgpu_server_opts;
 

@@ -355,6 +355,36 @@ PLOM_HD double systematic_point(const SysSeg* seg, int ns, int j) {
   return seg[lo].x0 + (double)(j - seg[lo].j0) * seg[lo].step;
 }
 
+// ---------------------------------------------------------------- incidence sums
+// The incidence terms of one substep, summed per unique incidence series in
+// cac order before they are added to the state (the order the sum of every
+// implementation keeps).  In registers a series index known only at run time
+// reaches its register through an unrolled compare chain.
+template <class T, int N>
+struct RegIncAcc {
+  T v[N > 0 ? N : 1];
+  PLOM_HD RegIncAcc() {}
+  template <class X>
+  PLOM_HD explicit RegIncAcc(X&) {}
+  PLOM_HD void zero() {
+    PLOM_UNROLL
+    for (int w = 0; w < N; ++w) v[w] = T(0);
+  }
+  PLOM_HD void add(int w, T d) {
+    PLOM_UNROLL
+    for (int ww = 0; ww < N; ++ww)
+      if (ww == w) v[ww] += d;
+  }
+  PLOM_HD T get(int w) const { return v[w]; }
+};
+
+// Accumulator of a particle store X; a store in shared memory may give the
+// sums words of their own there (one indexed load / add / store per term).
+template <class X, class T, int N>
+struct IncAccFor {
+  typedef RegIncAcc<T, N> type;
+};
+
 }  // namespace plomrt
 
 template <class T> PLOM_HD T plom_heaviside(T x) { return plomrt::heaviside_<T>(x); }

@@ -1678,7 +1678,7 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->precision = o->precision;
   sv->max_J = o->max_J;
   sv->ring = o->ring_slots > 0 ? o->ring_slots : 1024;
-  sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 2;
+  sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 4;
   sv->budget = o->memory_budget > 0 ? (size_t)o->memory_budget : (size_t)150e9;
   // keep host copies of the shared problem
   const int n = d->n_obs;

@@ -90,7 +90,7 @@ struct PooledPlan {
 
 struct plomgpu_server {
   // configuration
-  int precision = 32, max_J = 0, ring = 1024, plan_pool = 2;
+  int precision = 32, max_J = 0, ring = 1024, plan_pool = 4;
   size_t budget = 0;
   bool persistent = !kSmem;
   int bt = 256, grid = 0;

@@ -47,6 +47,55 @@ struct SmemState {
   PLOM_HD T& operator[](int i) const { return b[i * STRIDE]; }
 };
 
+// Incidence sums of a shared-memory particle in the words after its state
+// (S .. S + N_TS_INC_UNIQUE - 1 of its column): a term goes to its series by
+// an indexed shared-memory add instead of a compare chain over registers.
+template <class T, int STRIDE>
+struct SmemIncAcc {
+  T* b;
+  PLOM_HD explicit SmemIncAcc(SmemState<T, STRIDE>& x) : b(x.b + (size_t)M::S * STRIDE) {}
+  PLOM_HD void zero() {
+#pragma unroll
+    for (int w = 0; w < M::N_TS_INC_UNIQUE; ++w) b[w * STRIDE] = T(0);
+  }
+  PLOM_HD void add(int w, T d) { b[w * STRIDE] += d; }
+  PLOM_HD T get(int w) const { return b[w * STRIDE]; }
+};
+
+// the propagate kernel's shared memory: coupling matrix, per-cac parameters
+// (both read by every thread with the same address), then the state columns
+// of the block's particles when the state does not fit registers, followed by
+// their incidence sums when those words keep the blocks per SM (FP32 only:
+// FP64 states run the parity modes, with the register sums)
+constexpr int pad4(int n) { return (n + 3) & ~3; }
+constexpr int kSmemCoup = M::COUPLED ? pad4(M::N_CAC * M::N_CAC) : 0;
+constexpr int kSmemPar = pad4(M::N_PAR_PROC * M::N_CAC);
+
+template <class T, int BT>
+constexpr bool inc_in_smem() {
+#if defined(PLOM_INC_REGS)
+  return false;
+#else
+  constexpr size_t sm = 228 * 1024, per_block_resv = 1024, block_max = 227 * 1024;
+  constexpr size_t base = ((size_t)kSmemCoup + kSmemPar + (size_t)M::S * BT) * sizeof(T);
+  constexpr size_t ext = base + (size_t)M::N_TS_INC_UNIQUE * BT * sizeof(T);
+  return sizeof(T) == 4 && M::N_TS_INC_UNIQUE > 0 && ext <= block_max &&
+         sm / (ext + per_block_resv) >= sm / (base + per_block_resv);
+#endif
+}
+
+}  // namespace plomgpu
+
+namespace plomrt {
+template <class T, int STRIDE, int N>
+struct IncAccFor<plomgpu::SmemState<T, STRIDE>, T, N> {
+  typedef typename std::conditional<plomgpu::inc_in_smem<T, STRIDE>(), plomgpu::SmemIncAcc<T, STRIDE>,
+                                    RegIncAcc<T, N>>::type type;
+};
+}  // namespace plomrt
+
+namespace plomgpu {
+
 // ------------------------------------------------------------------ environments
 template <class T>
 struct ProcEnv {
@@ -205,16 +254,10 @@ struct MifObsEnv : ObsEnv {
 };
 
 // ------------------------------------------------------------------ propagate
-// shared-memory layout of k_propagate: coupling matrix, per-cac parameters
-// (both read by every thread with the same address), then the state
-// columns of the block's particles when the state does not fit registers
-constexpr int pad4(int n) { return (n + 3) & ~3; }
-constexpr int kSmemCoup = M::COUPLED ? pad4(M::N_CAC * M::N_CAC) : 0;
-constexpr int kSmemPar = pad4(M::N_PAR_PROC * M::N_CAC);
-
 template <class T, bool SMEM, int BT>
 constexpr size_t propagate_smem_bytes() {
-  return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) + (SMEM ? (size_t)M::S * BT * sizeof(T) : 0);
+  return (size_t)(kSmemCoup + kSmemPar) * sizeof(T) +
+         (SMEM ? ((size_t)M::S + (inc_in_smem<T, BT>() ? M::N_TS_INC_UNIQUE : 0)) * BT * sizeof(T) : 0);
 }
 
 // PSR: the Poisson-system step (M::step_psr, the reference's default "psr"

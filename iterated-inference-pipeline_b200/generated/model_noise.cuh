@@ -27,9 +27,9 @@ struct Model {
   struct Pre {
     int unused;
   };
-  template <int V, bool DRIFT, class T, class X, class E>
+  template <int V, bool DRIFT, class T, class X, class E, class IA>
   PLOM_HD static void cac_body(X& x, const int cac, const T* nz, const T t, const T dt, const E& e,
-                               T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
+                               IA& inc_acc, const Pre<T>& pre) {
     (void)t; (void)nz; (void)pre;
     const T xo_S = x[0*N_CAC+cac];
     const T xo_I = x[1*N_CAC+cac];
@@ -79,13 +79,8 @@ struct Model {
       const int l = inc_link(cac, k);
       if (l < 0) break;
       const int o = l >> 10, w = l & 1023;
-      PLOM_UNROLL
-      for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {
-        if (ww == w) {
-          if (o == 0) inc_acc[ww] += incterm_0;
-          if (o == 1) inc_acc[ww] += incterm_1;
-        }
-      }
+      if (o == 0) inc_acc.add(w, incterm_0);
+      if (o == 1) inc_acc.add(w, incterm_1);
     }
     x[0*N_CAC+cac] = (f_S < T(0)) ? T(0) : f_S;
     x[1*N_CAC+cac] = (f_I < T(0)) ? T(0) : f_I;
@@ -111,9 +106,8 @@ struct Model {
     constexpr int NW = draws_per_cac(V);
     constexpr int G = draw_group(NW, D::PER_BLOCK);
     constexpr int NMAIN = N_CAC - (N_CAC % G);
-    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-    PLOM_UNROLL
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    typename plomrt::IncAccFor<X, T, N_TS_INC_UNIQUE>::type inc_acc(x);
+    inc_acc.zero();
     Pre<T> pre;
     pre.unused = 0;
     PLOM_PRAGMA_CAC
@@ -131,7 +125,7 @@ struct Model {
     }
     PLOM_UNROLL
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {
-      const T f = x[OFF_INC+w] + inc_acc[w];
+      const T f = x[OFF_INC+w] + inc_acc.get(w);
       x[OFF_INC+w] = (f < T(0)) ? T(0) : f;
     }
     if (DRIFT) {
@@ -152,9 +146,8 @@ struct Model {
     constexpr int G = draw_group(NW, D::PER_BLOCK);
     constexpr int NG = N_CAC / G;
     constexpr int NMAIN = NG * G;
-    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-    PLOM_UNROLL
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    plomrt::RegIncAcc<T, N_TS_INC_UNIQUE> inc_acc;
+    inc_acc.zero();
     PLOM_PRAGMA_CAC
     for (int gi = tm.rank; gi < NG; gi += TM::TP) {
       const int cac0 = gi * G;
@@ -169,12 +162,12 @@ struct Model {
       cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);
     }
     PLOM_UNROLL
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = tm.sum(inc_acc[w]);
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc.v[w] = tm.sum(inc_acc.v[w]);
     tm.sync();
     if (tm.rank == 0) {
       PLOM_UNROLL
       for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {
-        const T f = x[OFF_INC+w] + inc_acc[w];
+        const T f = x[OFF_INC+w] + inc_acc.v[w];
         x[OFF_INC+w] = (f < T(0)) ? T(0) : f;
       }
     }

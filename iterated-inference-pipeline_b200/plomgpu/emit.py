@@ -386,9 +386,9 @@ class Emitter(object):
         a('    int unused;')
         a('  };')
         # one compartment-age class: rates, noises, equations, incidence
-        a('  template <int V, bool DRIFT, class T, class X, class E>')
+        a('  template <int V, bool DRIFT, class T, class X, class E, class IA>')
         a('  PLOM_HD static void cac_body(X& x, const int cac, const T* nz, const T t, const T dt, const E& e,')
-        a('                               T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
+        a('                               IA& inc_acc, const Pre<T>& pre) {')
         a('    (void)t; (void)nz; (void)pre;')
         for i, s in enumerate(m.par_sv):
             a('    const T xo_%s = x[%d*N_CAC+cac];' % (s, i))
@@ -449,13 +449,8 @@ class Emitter(object):
             a('      const int l = inc_link(cac, k);')
             a('      if (l < 0) break;')
             a('      const int o = l >> 10, w = l & 1023;')
-            a('      PLOM_UNROLL')
-            a('      for (int ww = 0; ww < N_TS_INC_UNIQUE; ++ww) {')
-            a('        if (ww == w) {')
             for o in range(len(inc)):
-                a('          if (o == %d) inc_acc[ww] += incterm_%d;' % (o, o))
-            a('        }')
-            a('      }')
+                a('      if (o == %d) inc_acc.add(w, incterm_%d);' % (o, o))
             a('    }')
         for i, s in enumerate(m.par_sv):
             a('    x[%d*N_CAC+cac] = (f_%s < T(0)) ? T(0) : f_%s;' % (i, s, s))
@@ -482,9 +477,8 @@ class Emitter(object):
         a('    constexpr int NW = draws_per_cac(V);')
         a('    constexpr int G = draw_group(NW, D::PER_BLOCK);')
         a('    constexpr int NMAIN = N_CAC - (N_CAC % G);')
-        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
-        a('    PLOM_UNROLL')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        a('    typename plomrt::IncAccFor<X, T, N_TS_INC_UNIQUE>::type inc_acc(x);')
+        a('    inc_acc.zero();')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
         for k, tt in enumerate(self.time_terms):
@@ -510,7 +504,7 @@ class Emitter(object):
         a('    }')
         a('    PLOM_UNROLL')
         a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {')
-        a('      const T f = x[OFF_INC+w] + inc_acc[w];')
+        a('      const T f = x[OFF_INC+w] + inc_acc.get(w);')
         a('      x[OFF_INC+w] = (f < T(0)) ? T(0) : f;')
         a('    }')
         a('    if (DRIFT) {')
@@ -545,9 +539,8 @@ class Emitter(object):
         a('    constexpr int G = draw_group(NW, D::PER_BLOCK);')
         a('    constexpr int NG = N_CAC / G;')
         a('    constexpr int NMAIN = NG * G;')
-        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
-        a('    PLOM_UNROLL')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        a('    plomrt::RegIncAcc<T, N_TS_INC_UNIQUE> inc_acc;')
+        a('    inc_acc.zero();')
         for s_ in foi_states:
             si = m.par_sv.index(s_)
             a('    for (int c2 = tm.rank; c2 < N_CAC; c2 += TM::TP) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;'
@@ -573,12 +566,12 @@ class Emitter(object):
         a('      cac_body<V, DRIFT, T>(x, cac, nz, t, dt, e, inc_acc, pre);')
         a('    }')
         a('    PLOM_UNROLL')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = tm.sum(inc_acc[w]);')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc.v[w] = tm.sum(inc_acc.v[w]);')
         a('    tm.sync();')
         a('    if (tm.rank == 0) {')
         a('      PLOM_UNROLL')
         a('      for (int w = 0; w < N_TS_INC_UNIQUE; ++w) {')
-        a('        const T f = x[OFF_INC+w] + inc_acc[w];')
+        a('        const T f = x[OFF_INC+w] + inc_acc.v[w];')
         a('        x[OFF_INC+w] = (f < T(0)) ? T(0) : f;')
         a('      }')
         a('    }')
