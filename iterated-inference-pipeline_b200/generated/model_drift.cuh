@@ -3,6 +3,12 @@
 #include "plom_rt.h"
 #include "psr_samplers.h"
 namespace plomgen {
+// incidence links of each cac (obs * 1024 + word, -1 after its last), read with a run-time
+// cac: from constant memory on the device
+#if defined(__CUDACC__)
+__constant__ int kIncLinkDev[4] = {0,-1,0,1025};
+#endif
+static const int kIncLinkHost[4] = {0,-1,0,1025};
 struct Model {
   static constexpr const char* NAME = "drift";
   static constexpr int N_PAR_SV = 2, N_C = 2, N_AC = 1, N_CAC = 2;
@@ -20,8 +26,11 @@ struct Model {
   static constexpr int N_INC_LINKS = 3;
   static constexpr int INC_PER_CAC = 2;
   PLOM_HD static int inc_link(int cac, int k) {
-    constexpr int tab[N_CAC][INC_PER_CAC] = {{0,-1},{0,1025}};
-    return tab[cac][k];
+#if defined(__CUDA_ARCH__)
+    return kIncLinkDev[cac * INC_PER_CAC + k];
+#else
+    return kIncLinkHost[cac * INC_PER_CAC + k];
+#endif
   }
   template <class T>
   struct Pre {

@@ -3,6 +3,12 @@
 #include "plom_rt.h"
 #include "psr_samplers.h"
 namespace plomgen {
+// incidence links of each cac (obs * 1024 + word, -1 after its last), read with a run-time
+// cac: from constant memory on the device
+#if defined(__CUDACC__)
+__constant__ int kIncLinkDev[6] = {0,0,1,1,2,2};
+#endif
+static const int kIncLinkHost[6] = {0,0,1,1,2,2};
 struct Model {
   static constexpr const char* NAME = "seir_local";
   static constexpr int N_PAR_SV = 4, N_C = 3, N_AC = 2, N_CAC = 6;
@@ -20,8 +26,11 @@ struct Model {
   static constexpr int N_INC_LINKS = 6;
   static constexpr int INC_PER_CAC = 1;
   PLOM_HD static int inc_link(int cac, int k) {
-    constexpr int tab[N_CAC][INC_PER_CAC] = {{0},{0},{1},{1},{2},{2}};
-    return tab[cac][k];
+#if defined(__CUDA_ARCH__)
+    return kIncLinkDev[cac * INC_PER_CAC + k];
+#else
+    return kIncLinkHost[cac * INC_PER_CAC + k];
+#endif
   }
   template <class T>
   struct Pre {

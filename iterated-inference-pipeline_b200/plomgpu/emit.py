@@ -309,6 +309,7 @@ class Emitter(object):
         a('#include "plom_rt.h"')
         a('#include "psr_samplers.h"')
         a('namespace plomgen {')
+        self._emit_inc_link_table(a)
         a('struct Model {')
         a('  static constexpr const char* NAME = "%s";' % name)
         a('  static constexpr int N_PAR_SV = %d, N_C = %d, N_AC = %d, N_CAC = %d;' % (nsv, m.N_C, m.N_AC, m.N_CAC))
@@ -354,7 +355,8 @@ class Emitter(object):
     def _n_inc_links(self):
         return sum(len(c) for (_, _, c) in self._inc_words())
 
-    def _emit_inc_tables(self, a):
+    def _inc_link_rows(self):
+        """(links per cac, flat [N_CAC * links] table of obs * 1024 + word, -1 after a cac's last)."""
         m = self.m
         words = self._inc_words()
         # per cac, the (obs, word) pairs it feeds, in word order
@@ -363,14 +365,32 @@ class Emitter(object):
             for c in cacs:
                 per[c].append((o, w))
         nmax = max([len(p) for p in per] + [1])
-        a('  static constexpr int INC_PER_CAC = %d;' % nmax)
-        rows = []
+        flat = []
         for p in per:
-            ent = ['%d' % (o * 1024 + w) for (o, w) in p] + ['-1'] * (nmax - len(p))
-            rows.append('{' + ','.join(ent) + '}')
+            flat += [o * 1024 + w for (o, w) in p] + [-1] * (nmax - len(p))
+        return nmax, flat
+
+    def _emit_inc_link_table(self, a):
+        """The links at namespace scope: the step reads them with a run-time cac, and a
+        table local to the function would be rebuilt on the stack at every call."""
+        _, flat = self._inc_link_rows()
+        vals = ','.join('%d' % v for v in flat)
+        a('// incidence links of each cac (obs * 1024 + word, -1 after its last), read with a run-time')
+        a('// cac: from constant memory on the device')
+        a('#if defined(__CUDACC__)')
+        a('__constant__ int kIncLinkDev[%d] = {%s};' % (len(flat), vals))
+        a('#endif')
+        a('static const int kIncLinkHost[%d] = {%s};' % (len(flat), vals))
+
+    def _emit_inc_tables(self, a):
+        nmax, _ = self._inc_link_rows()
+        a('  static constexpr int INC_PER_CAC = %d;' % nmax)
         a('  PLOM_HD static int inc_link(int cac, int k) {')
-        a('    constexpr int tab[N_CAC][INC_PER_CAC] = {%s};' % ','.join(rows))
-        a('    return tab[cac][k];')
+        a('#if defined(__CUDA_ARCH__)')
+        a('    return kIncLinkDev[cac * INC_PER_CAC + k];')
+        a('#else')
+        a('    return kIncLinkHost[cac * INC_PER_CAC + k];')
+        a('#endif')
         a('  }')
 
     def _emit_step(self, a, caches, ode, inc):
