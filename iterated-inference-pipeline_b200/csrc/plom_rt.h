@@ -14,6 +14,7 @@
 
 #include <stdint.h>
 #include <math.h>
+#include <string.h>
 
 #if defined(__CUDACC__)
 #define PLOM_HD __host__ __device__ __forceinline__
@@ -170,8 +171,16 @@ PLOM_HD U4 philox4x32_10(U4 c, uint32_t k0, uint32_t k1) {
   return c;
 }
 
-// uniform in (0, 1) with 24-bit resolution (Box-Muller angle)
-PLOM_HD float u01f(uint32_t u) { return ((float)(u >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+// uniform in (0, 1) with 23-bit resolution (Box-Muller angle): the high 23 bits
+// as the mantissa of a float in [1, 2), minus 1 - 2^-24 (exact by Sterbenz), i.e.
+// (k + 1/2) 2^-23; integer and logic instructions instead of a conversion on the
+// special-function pipe
+PLOM_HD float u01f(uint32_t u) {
+  const uint32_t b = 0x3f800000u | (u >> 9);
+  float f;
+  memcpy(&f, &b, sizeof f);
+  return f - 0.99999994039535522f;
+}
 // uniform in (0, 1] from all 32 bits, fine near 0 (Box-Muller radius: tails to 6.7 sd)
 PLOM_HD float u01f_radius(uint32_t u) { return (float)u * 2.3283064365386963e-10f + 1.1641532182693481e-10f; }
 // uniform in (0, 1) from 64 bits with 53-bit resolution

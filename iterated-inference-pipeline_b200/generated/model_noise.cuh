@@ -94,19 +94,16 @@ struct Model {
     x[0*N_CAC+cac] = (f_S < T(0)) ? T(0) : f_S;
     x[1*N_CAC+cac] = (f_I < T(0)) ? T(0) : f_I;
   }
-  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)
-  // For generators of more than 2 normals per block (FP32) the group is capped at
-  // PLOM_MAX_DRAW_GROUP (default 1 when the state lives in shared memory), leaving part
-  // of the last block of a group unused: the shorter loop body measured 18 % faster on
-  // SEIR 20x2 than whole blocks over 4 cacs, for 33 % more Philox blocks.
+  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block);
+  // for generators of more than 2 normals per block (FP32) PLOM_MAX_DRAW_GROUP caps the
+  // group, leaving part of the last block of a group unused (SEIR 20x2: 4 cacs = 9 whole
+  // blocks measured 10 % faster than 1 cac = 3 blocks with 3 of their 12 normals unused)
   static constexpr PLOM_HD int draw_group(int nw, int per_block) {
     int g = 1;
     while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;
     g = (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;
 #if defined(PLOM_MAX_DRAW_GROUP)
     if (per_block > 2 && g > PLOM_MAX_DRAW_GROUP) g = PLOM_MAX_DRAW_GROUP;
-#elif defined(PLOM_SMEM_STATE) && PLOM_SMEM_STATE
-    if (per_block > 2) g = 1;
 #endif
     return g;
   }

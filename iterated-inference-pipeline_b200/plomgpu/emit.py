@@ -476,19 +476,16 @@ class Emitter(object):
             a('    x[%d*N_CAC+cac] = (f_%s < T(0)) ? T(0) : f_%s;' % (i, s, s))
         a('  }')
         # one Euler-Maruyama substep of the whole particle
-        a('  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block)')
-        a('  // For generators of more than 2 normals per block (FP32) the group is capped at')
-        a('  // PLOM_MAX_DRAW_GROUP (default 1 when the state lives in shared memory), leaving part')
-        a('  // of the last block of a group unused: the shorter loop body measured 18 % faster on')
-        a('  // SEIR 20x2 than whole blocks over 4 cacs, for 33 % more Philox blocks.')
+        a('  // cacs drawn together so that whole draw blocks are used (PER_BLOCK normals per block);')
+        a('  // for generators of more than 2 normals per block (FP32) PLOM_MAX_DRAW_GROUP caps the')
+        a('  // group, leaving part of the last block of a group unused (SEIR 20x2: 4 cacs = 9 whole')
+        a('  // blocks measured 10 % faster than 1 cac = 3 blocks with 3 of their 12 normals unused)')
         a('  static constexpr PLOM_HD int draw_group(int nw, int per_block) {')
         a('    int g = 1;')
         a('    while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;')
         a('    g = (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;')
         a('#if defined(PLOM_MAX_DRAW_GROUP)')
         a('    if (per_block > 2 && g > PLOM_MAX_DRAW_GROUP) g = PLOM_MAX_DRAW_GROUP;')
-        a('#elif defined(PLOM_SMEM_STATE) && PLOM_SMEM_STATE')
-        a('    if (per_block > 2) g = 1;')
         a('#endif')
         a('    return g;')
         a('  }')
