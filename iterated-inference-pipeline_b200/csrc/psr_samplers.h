@@ -19,7 +19,9 @@
 // * multinomial: sequential conditional binomials (plom_ran_multinomial,
 //   model_builder/C/core/prediction_util.c:327-345).
 //
-// Everything is computed in double whatever the state precision.
+// FP64 particle states (the parity modes, and the oracle) draw in double;
+// FP32 states draw with the single-precision versions at the end of this
+// file, which keep double where magnitudes cancel.
 #pragma once
 
 #include "plom_rt.h"
@@ -257,6 +259,225 @@ PLOM_HD void multinomial(UniformStream& rs, double N, const double (&p)[K], doub
     sum_n += out[k];
   }
   out[K - 1] = (p[K - 1] > 0.0) ? N - sum_n : 0.0;
+}
+
+// ---------------------------------------------------------------- single precision
+// The same samplers for FP32 particle states, in float where the magnitudes
+// allow it: four 24-bit uniforms per Philox block instead of two 53-bit ones,
+// float elementary functions.  Three quantities keep double: the location
+// n p + 1/2 (or mu + 0.43) added last when a count is formed, the mode of
+// BTRD, and the final acceptance tests of BTRD and PTRS, whose terms are of
+// the order of the count (k log mu, log k!) and cancel to O(1).  Counts are
+// exact in float below 2^24, the range of an FP32 state's integers.
+PLOM_SAMPLER float s_log(float x) { return logf(x); }
+PLOM_SAMPLER float s_exp(float x) { return expf(x); }
+PLOM_SAMPLER float s_pow(float x, float y) { return powf(x, y); }
+PLOM_SAMPLER float s_log1p(float x) { return log1pf(x); }
+
+// Philox block (j, n, group, STREAM_PSR + 16 block) as four uniforms in (0, 1)
+PLOM_SAMPLER void psr_uniform_quad(PhiloxKey key, uint32_t j, uint32_t n, uint32_t group, uint32_t block, float* u) {
+  const U4 c = {j, n, group, (uint32_t)STREAM_PSR + (block << 4)};
+  const U4 r = philox4x32_10(c, key.k0, key.k1);
+  const float s = 1.0f / 16777216.0f;
+  u[0] = ((float)(r.x >> 8) + 0.5f) * s;
+  u[1] = ((float)(r.y >> 8) + 0.5f) * s;
+  u[2] = ((float)(r.z >> 8) + 0.5f) * s;
+  u[3] = ((float)(r.w >> 8) + 0.5f) * s;
+}
+
+struct UniformStreamF {
+  PhiloxKey key;
+  uint32_t j, n, group;
+  uint32_t block;
+  float cache[4];
+  int used;  // uniforms of the cached block already returned (4: none left)
+  PLOM_HD void init(PhiloxKey k, uint32_t j_, uint32_t n_, uint32_t group_) {
+    key = k;
+    j = j_;
+    n = n_;
+    group = group_;
+    block = 0;
+    used = 4;
+  }
+  PLOM_HD float next() {
+    if (used == 4) {
+      psr_uniform_quad(key, j, n, group, block, cache);
+      ++block;
+      used = 0;
+    }
+    return cache[used++];
+  }
+  PLOM_HD float normal() {
+    const float u1 = next(), u2 = next();
+    return sqrtf(-2.0f * s_log(u1)) * cosf(6.2831853071795865f * u2);
+  }
+};
+
+// stream type of a particle precision
+template <class T> struct PsrStream { typedef UniformStream type; };
+template <> struct PsrStream<float> { typedef UniformStreamF type; };
+
+// Inversion for n p < 14.  The float partial sums of the probabilities may
+// stop short of a uniform near 1; the search therefore ends at x = 110 (the
+// probability of more is below 1e-40 for a mean below 14) and the round
+// redraws, instead of walking up to n through probabilities that underflow.
+constexpr float kInversionMaxF = 110.0f;
+
+PLOM_HD float binomial_inversion(UniformStreamF& rs, float n, float p) {
+  const float q = 1.0f - p;
+  const float s = p / q, a = (n + 1.0f) * s;
+  const float r0 = s_exp(n * s_log1p(-p));  // q^n, accurate for small p
+  const float xmax = fminf(n, kInversionMaxF);
+  for (int round = 0; round < kMaxRejection; ++round) {
+    float u = rs.next(), r = r0, x = 0.0f;
+    while (u > r) {
+      u -= r;
+      x += 1.0f;
+      if (x > xmax) break;
+      r *= (a / x - s);
+    }
+    if (x <= xmax) return x;
+  }
+  return floorf(n * p);
+}
+
+// the last BTRD test, log f(k) / f(m) against the scaled hat value log v
+PLOM_SAMPLER bool btrd_accept(double n, double m, double k, double r, double v) {
+  const double nm = n - m + 1.0;
+  const double h = (m + 0.5) * s_log((m + 1.0) / (r * nm)) + stirling_correction(m) + stirling_correction(n - m);
+  const double nk = n - k + 1.0;
+  return v <= h + (n + 1.0) * s_log(nm / nk) + (k + 0.5) * s_log(nk * r / (k + 1.0)) - stirling_correction(k) -
+                  stirling_correction(n - k);
+}
+
+PLOM_HD float binomial_btrd(UniformStreamF& rs, float n, float p) {
+  const float q = 1.0f - p;
+  const float spq = sqrtf(n * p * q);
+  const float b = 1.15f + 2.53f * spq;
+  const float a = -0.0873f + 0.0248f * b + 0.01f * p;
+  const double c = (double)n * (double)p + 0.5;
+  const float vr = 0.92f - 4.2f / b;
+  const float alpha = (2.83f + 5.1f / b) * spq;
+  const double md = floor(((double)n + 1.0) * (double)p);
+  const float m = (float)md;
+  const float r = p / q, nr = (n + 1.0f) * r, npq = n * p * q;
+  for (int round = 0; round < kMaxRejection; ++round) {
+    float v = rs.next();
+    float u;
+    if (v <= 0.86f * vr) {
+      u = v / vr - 0.43f;
+      return (float)floor((double)((2.0f * a / (0.5f - fabsf(u)) + b) * u) + c);
+    }
+    if (v >= vr) {
+      u = rs.next() - 0.5f;
+    } else {
+      u = v / vr - 0.93f;
+      u = ((u > 0.0f) ? 0.5f : -0.5f) - u;
+      v = rs.next() * vr;
+    }
+    const float us = 0.5f - fabsf(u);
+    const float k = (float)floor((double)((2.0f * a / us + b) * u) + c);
+    if (k < 0.0f || k > n) continue;
+    v = v * alpha / (a / (us * us) + b);
+    const float km = fabsf(k - m);
+    if (km <= 15.0f) {
+      // integer steps: a float counter would stop moving above 2^24
+      const int steps = (int)km;
+      float f = 1.0f;
+      if (m < k) {
+        for (int d = 1; d <= steps; ++d) f *= (nr / (m + (float)d) - r);
+      } else if (m > k) {
+        for (int d = 1; d <= steps; ++d) v *= (nr / (k + (float)d) - r);
+      }
+      if (v <= f) return k;
+      continue;
+    }
+    v = s_log(v);
+    const float rho = (km / npq) * (((km / 3.0f + 0.625f) * km + 1.0f / 6.0f) / npq + 0.5f);
+    const float t = -km * km / (2.0f * npq);
+    if (v < t - rho) return k;
+    if (v > t + rho) continue;
+    if (btrd_accept((double)n, md, (double)k, (double)p / (double)q, (double)v)) return k;
+  }
+  return m;
+}
+
+PLOM_SAMPLER float binomial(UniformStreamF& rs, float n, float p) {
+  if (n <= 0.0f || !(p > 0.0f)) return 0.0f;
+  if (p >= 1.0f) return n;
+  const bool flip = p > 0.5f;
+  const float pp = flip ? 1.0f - p : p;
+  const float x = (n * pp < 14.0f) ? binomial_inversion(rs, n, pp) : binomial_btrd(rs, n, pp);
+  return flip ? n - x : x;
+}
+
+// the last PTRS test
+PLOM_SAMPLER bool ptrs_accept(double mu, double k, double v, double us, double a, double b, double inv_alpha) {
+  return s_log(v) + s_log(inv_alpha) - s_log(a / (us * us) + b) <= -mu + k * s_log(mu) - s_lgamma(k + 1.0);
+}
+
+PLOM_SAMPLER float poisson(UniformStreamF& rs, float mu) {
+  if (!(mu > 0.0f)) return 0.0f;
+  if (mu < 10.0f) {
+    for (int round = 0; round < kMaxRejection; ++round) {
+      float u = rs.next(), p = s_exp(-mu), x = 0.0f;
+      while (u > p) {
+        u -= p;
+        x += 1.0f;
+        p *= mu / x;
+        if (x > kInversionMaxF) break;
+      }
+      if (x <= kInversionMaxF) return x;
+    }
+    return floorf(mu);
+  }
+  const float smu = sqrtf(mu);
+  const float b = 0.931f + 2.53f * smu;
+  const float a = -0.059f + 0.02483f * b;
+  const float inv_alpha = 1.1239f + 1.1328f / (b - 3.4f);
+  const float vr = 0.9277f - 3.6224f / (b - 2.0f);
+  const double loc = (double)mu + 0.43;
+  for (int round = 0; round < kMaxRejection; ++round) {
+    const float u = rs.next() - 0.5f;
+    const float v = rs.next();
+    const float us = 0.5f - fabsf(u);
+    const float k = (float)floor((double)((2.0f * a / us + b) * u) + loc);
+    if (us >= 0.07f && v <= vr) return k;
+    if (k < 0.0f || (us < 0.013f && v > us)) continue;
+    if (ptrs_accept((double)mu, (double)k, (double)v, (double)us, (double)a, (double)b, (double)inv_alpha)) return k;
+  }
+  return floorf(mu);
+}
+
+PLOM_SAMPLER float gamma(UniformStreamF& rs, float a, float theta) {
+  if (!(a > 0.0f) || !(theta > 0.0f)) return 0.0f;
+  float boost = 1.0f;
+  if (a < 1.0f) {
+    boost = s_pow(rs.next(), 1.0f / a);
+    a += 1.0f;
+  }
+  const float d = a - 1.0f / 3.0f, c = 1.0f / sqrtf(9.0f * d);
+  for (int round = 0; round < kMaxRejection; ++round) {
+    const float z = rs.normal();
+    float v = 1.0f + c * z;
+    if (v <= 0.0f) continue;
+    v = v * v * v;
+    const float u = rs.next();
+    if (u < 1.0f - 0.0331f * z * z * z * z) return d * v * theta * boost;
+    if (s_log(u) < 0.5f * z * z + d * (1.0f - v + s_log(v))) return d * v * theta * boost;
+  }
+  return d * theta * boost;
+}
+
+template <int K>
+PLOM_HD void multinomial(UniformStreamF& rs, float N, const float (&p)[K], float (&out)[K]) {
+  float sum_p = 0.0f, sum_n = 0.0f;
+  for (int k = 0; k < K - 1; ++k) {
+    out[k] = (p[k] > 0.0f) ? binomial(rs, N - sum_n, p[k] / (1.0f - sum_p)) : 0.0f;
+    sum_p += p[k];
+    sum_n += out[k];
+  }
+  out[K - 1] = (p[K - 1] > 0.0f) ? N - sum_n : 0.0f;
 }
 
 }  // namespace plomrt

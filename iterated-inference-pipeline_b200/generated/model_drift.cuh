@@ -230,10 +230,11 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];
   }
   template <bool DRIFT, bool NOENV, class T, class X, class E>
-  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e, plomrt::UniformStream& rs,
-                              double (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
+  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e,
+                              typename plomrt::PsrStream<T>::type& rs,
+                              T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
     (void)t; (void)pre;
-    const double ddt = (double)dt;
+    const T ddt = dt;
     const T xo_S = x[0*N_CAC+cac];
     const T xo_I = x[1*N_CAC+cac];
     T drift_0;
@@ -254,46 +255,46 @@ struct Model {
     const T r1 = xo_I*drift_0*e.par(1, cac)/e.cov(0, cac);
     const T r2 = e.par(1, cac);
     const T r3 = e.cov(2, cac);
-    double inc_S[3];
+    T inc_S[3];
     {
-      const double h0 = (double)r1 * ddt;
-      const double h1 = (double)r3 * ddt;
-      const double sum = h0 + h1;
-      double p[3];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r1 * ddt;
+      const T h1 = r3 * ddt;
+      const T sum = h0 + h1;
+      T p[3];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
-        p[2] = 1.0 - p[0] - p[1];
+        p[2] = T(1) - p[0] - p[1];
       } else {
-        p[0] = 0.0;
-        p[1] = 0.0;
-        p[2] = 1.0;
+        p[0] = T(0);
+        p[1] = T(0);
+        p[2] = T(1);
       }
-      const double xs = (double)xo_S;
-      plomrt::multinomial<3>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_S);
+      const T xs = xo_S;
+      plomrt::multinomial<3>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_S);
     }
-    double inc_I[3];
+    T inc_I[3];
     {
-      const double h0 = (double)r2 * ddt;
-      const double h1 = (double)r3 * ddt;
-      const double sum = h0 + h1;
-      double p[3];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r2 * ddt;
+      const T h1 = r3 * ddt;
+      const T sum = h0 + h1;
+      T p[3];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
-        p[2] = 1.0 - p[0] - p[1];
+        p[2] = T(1) - p[0] - p[1];
       } else {
-        p[0] = 0.0;
-        p[1] = 0.0;
-        p[2] = 1.0;
+        p[0] = T(0);
+        p[1] = T(0);
+        p[2] = T(1);
       }
-      const double xs = (double)xo_I;
-      plomrt::multinomial<3>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_I);
+      const T xs = xo_I;
+      plomrt::multinomial<3>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_I);
     }
-    double inc_U[1];
-    inc_U[0] = plomrt::poisson(rs, (double)r0 * ddt);
+    T inc_U[1];
+    inc_U[0] = plomrt::poisson(rs, r0 * ddt);
     x[0*N_CAC+cac] = (T)(inc_S[2] + inc_U[0]);
     x[1*N_CAC+cac] = (T)(inc_I[2] + inc_S[0]);
     for (int k = 0; k < INC_PER_CAC; ++k) {
@@ -307,16 +308,16 @@ struct Model {
   template <bool DRIFT, bool NOENV, class T, class X, class E, class D>
   PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,
                                const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {
-    double inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
     for (int cac = 0; cac < N_CAC; ++cac) {
-      plomrt::UniformStream rs;
+      typename plomrt::PsrStream<T>::type rs;
       rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);
       psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);
     }
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = (T)((double)x[OFF_INC+w] + inc_acc[w]);
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc[w];
     if (DRIFT) {
       // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)
       for (int i = 0; i < N_DRIFT; ++i) {

@@ -240,17 +240,18 @@ struct Model {
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];
   }
   template <bool DRIFT, bool NOENV, class T, class X, class E>
-  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e, plomrt::UniformStream& rs,
-                              double (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
+  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e,
+                              typename plomrt::PsrStream<T>::type& rs,
+                              T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
     (void)t; (void)pre;
-    const double ddt = (double)dt;
+    const T ddt = dt;
     const T xo_S = x[0*N_CAC+cac];
     const T xo_E = x[1*N_CAC+cac];
     const T xo_I = x[2*N_CAC+cac];
     const T xo_R = x[3*N_CAC+cac];
-    double wn_0 = 1.0;
+    T wn_0 = T(1);
     if (!NOENV) {
-      const double sd = (double)(e.par(3, cac));
+      const T sd = (T)(e.par(3, cac));
       wn_0 = plomrt::gamma(rs, ddt / (sd * sd), sd * sd) / ddt;
     }
     const T r0 = e.par(4, cac)*(xo_E + xo_I + xo_R + xo_S);
@@ -258,81 +259,81 @@ struct Model {
     const T r2 = e.par(2, cac);
     const T r3 = e.par(1, cac);
     const T r4 = e.par(5, cac);
-    double inc_S[3];
+    T inc_S[3];
     {
-      const double h0 = (double)r1*wn_0 * ddt;
-      const double h1 = (double)r4 * ddt;
-      const double sum = h0 + h1;
-      double p[3];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r1*wn_0 * ddt;
+      const T h1 = r4 * ddt;
+      const T sum = h0 + h1;
+      T p[3];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
-        p[2] = 1.0 - p[0] - p[1];
+        p[2] = T(1) - p[0] - p[1];
       } else {
-        p[0] = 0.0;
-        p[1] = 0.0;
-        p[2] = 1.0;
+        p[0] = T(0);
+        p[1] = T(0);
+        p[2] = T(1);
       }
-      const double xs = (double)xo_S;
-      plomrt::multinomial<3>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_S);
+      const T xs = xo_S;
+      plomrt::multinomial<3>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_S);
     }
-    double inc_E[3];
+    T inc_E[3];
     {
-      const double h0 = (double)r2 * ddt;
-      const double h1 = (double)r4 * ddt;
-      const double sum = h0 + h1;
-      double p[3];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r2 * ddt;
+      const T h1 = r4 * ddt;
+      const T sum = h0 + h1;
+      T p[3];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
-        p[2] = 1.0 - p[0] - p[1];
+        p[2] = T(1) - p[0] - p[1];
       } else {
-        p[0] = 0.0;
-        p[1] = 0.0;
-        p[2] = 1.0;
+        p[0] = T(0);
+        p[1] = T(0);
+        p[2] = T(1);
       }
-      const double xs = (double)xo_E;
-      plomrt::multinomial<3>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_E);
+      const T xs = xo_E;
+      plomrt::multinomial<3>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_E);
     }
-    double inc_I[3];
+    T inc_I[3];
     {
-      const double h0 = (double)r3 * ddt;
-      const double h1 = (double)r4 * ddt;
-      const double sum = h0 + h1;
-      double p[3];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r3 * ddt;
+      const T h1 = r4 * ddt;
+      const T sum = h0 + h1;
+      T p[3];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
         p[1] = ome * (h1 / sum);
-        p[2] = 1.0 - p[0] - p[1];
+        p[2] = T(1) - p[0] - p[1];
       } else {
-        p[0] = 0.0;
-        p[1] = 0.0;
-        p[2] = 1.0;
+        p[0] = T(0);
+        p[1] = T(0);
+        p[2] = T(1);
       }
-      const double xs = (double)xo_I;
-      plomrt::multinomial<3>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_I);
+      const T xs = xo_I;
+      plomrt::multinomial<3>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_I);
     }
-    double inc_R[2];
+    T inc_R[2];
     {
-      const double h0 = (double)r4 * ddt;
-      const double sum = h0;
-      double p[2];
-      if (sum > 0.0) {
-        const double ome = 1.0 - plomrt::s_exp(-sum);
+      const T h0 = r4 * ddt;
+      const T sum = h0;
+      T p[2];
+      if (sum > T(0)) {
+        const T ome = T(1) - plomrt::s_exp(-sum);
         p[0] = ome * (h0 / sum);
-        p[1] = 1.0 - p[0];
+        p[1] = T(1) - p[0];
       } else {
-        p[0] = 0.0;
-        p[1] = 1.0;
+        p[0] = T(0);
+        p[1] = T(1);
       }
-      const double xs = (double)xo_R;
-      plomrt::multinomial<2>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_R);
+      const T xs = xo_R;
+      plomrt::multinomial<2>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_R);
     }
-    double inc_U[1];
-    inc_U[0] = plomrt::poisson(rs, (double)r0 * ddt);
+    T inc_U[1];
+    inc_U[0] = plomrt::poisson(rs, r0 * ddt);
     x[0*N_CAC+cac] = (T)(inc_S[2] + inc_U[0]);
     x[1*N_CAC+cac] = (T)(inc_E[2] + inc_S[0]);
     x[2*N_CAC+cac] = (T)(inc_I[2] + inc_E[0]);
@@ -347,17 +348,17 @@ struct Model {
   template <bool DRIFT, bool NOENV, class T, class X, class E, class D>
   PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,
                                const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {
-    double inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;
+    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
     Pre<T> pre;
     pre.unused = 0;
     pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
     for (int cac = 0; cac < N_CAC; ++cac) {
-      plomrt::UniformStream rs;
+      typename plomrt::PsrStream<T>::type rs;
       rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);
       psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);
     }
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = (T)((double)x[OFF_INC+w] + inc_acc[w]);
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc[w];
     if (DRIFT) {
       // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)
       for (int i = 0; i < N_DRIFT; ++i) {

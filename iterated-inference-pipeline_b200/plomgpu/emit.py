@@ -677,17 +677,18 @@ class Emitter(object):
 
         def rate_expr(r):
             k = rates.index(r['rate'])
-            e = '(double)r%d' % k
+            e = 'r%d' % k
             wn = r.get('white_noise')
             if wn:
                 e = '%s*wn_%d' % (e, [n for n, _ in noises].index(wn['name']))
             return e
 
         a('  template <bool DRIFT, bool NOENV, class T, class X, class E>')
-        a('  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e, plomrt::UniformStream& rs,')
-        a('                              double (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
+        a('  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e,')
+        a('                              typename plomrt::PsrStream<T>::type& rs,')
+        a('                              T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
         a('    (void)t; (void)pre;')
-        a('    const double ddt = (double)dt;')
+        a('    const T ddt = dt;')
         for i, s_ in enumerate(m.par_sv):
             a('    const T xo_%s = x[%d*N_CAC+cac];' % (s_, i))
         for k, p_ in enumerate(self.drift):
@@ -711,9 +712,9 @@ class Emitter(object):
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * pre.yf_%s[c2];' % (s_, s_))
         # 1: white noises
         for j, (name, sd) in enumerate(noises):
-            a('    double wn_%d = 1.0;' % j)
+            a('    T wn_%d = T(1);' % j)
             a('    if (!NOENV) {')
-            a('      const double sd = (double)(%s);' % sd)
+            a('      const T sd = (T)(%s);' % sd)
             a('      wn_%d = plomrt::gamma(rs, ddt / (sd * sd), sd * sd) / ddt;' % j)
             a('    }')
         # 2: rates
@@ -725,24 +726,24 @@ class Emitter(object):
             if not exits:
                 continue
             K = len(exits) + 1
-            a('    double inc_%s[%d];' % (s_, K))
+            a('    T inc_%s[%d];' % (s_, K))
             a('    {')
             for q, r in enumerate(exits):
-                a('      const double h%d = %s * ddt;' % (q, rate_expr(r)))
-            a('      const double sum = %s;' % ' + '.join('h%d' % q for q in range(len(exits))))
-            a('      double p[%d];' % K)
-            a('      if (sum > 0.0) {')
-            a('        const double ome = 1.0 - plomrt::s_exp(-sum);')
+                a('      const T h%d = %s * ddt;' % (q, rate_expr(r)))
+            a('      const T sum = %s;' % ' + '.join('h%d' % q for q in range(len(exits))))
+            a('      T p[%d];' % K)
+            a('      if (sum > T(0)) {')
+            a('        const T ome = T(1) - plomrt::s_exp(-sum);')
             for q in range(len(exits)):
                 a('        p[%d] = ome * (h%d / sum);' % (q, q))
-            a('        p[%d] = 1.0%s;' % (len(exits), ''.join(' - p[%d]' % q for q in range(len(exits)))))
+            a('        p[%d] = T(1)%s;' % (len(exits), ''.join(' - p[%d]' % q for q in range(len(exits)))))
             a('      } else {')
             for q in range(len(exits)):
-                a('        p[%d] = 0.0;' % q)
-            a('        p[%d] = 1.0;' % len(exits))
+                a('        p[%d] = T(0);' % q)
+            a('        p[%d] = T(1);' % len(exits))
             a('      }')
-            a('      const double xs = (double)xo_%s;' % s_)
-            a('      plomrt::multinomial<%d>(rs, xs > 0.0 ? floor(xs) : 0.0, p, inc_%s);' % (K, s_))
+            a('      const T xs = xo_%s;' % s_)
+            a('      plomrt::multinomial<%d>(rs, xs > T(0) ? floor(xs) : T(0), p, inc_%s);' % (K, s_))
             a('    }')
         # 4: arrivals from outside
         for src in univ:
@@ -751,13 +752,13 @@ class Emitter(object):
             arr = [r for r in m.proc_model if r['from'] == src]
             if not arr:
                 continue
-            a('    double inc_%s[%d];' % (self._univ_name(src), len(arr)))
+            a('    T inc_%s[%d];' % (self._univ_name(src), len(arr)))
             for q, r in enumerate(arr):
                 a('    inc_%s[%d] = plomrt::poisson(rs, %s * ddt);' % (self._univ_name(src), q, rate_expr(r)))
         # 5: new contents
         for i, s_ in enumerate(m.par_sv):
             exits = [r for r in m.proc_model if r['from'] == s_]
-            terms = ['inc_%s[%d]' % (s_, len(exits))] if exits else ['(double)xo_%s' % s_]
+            terms = ['inc_%s[%d]' % (s_, len(exits))] if exits else ['xo_%s' % s_]
             for s2 in m.par_sv:
                 for q, r in enumerate([r for r in m.proc_model if r['from'] == s2]):
                     if r['to'] == s_:
@@ -782,7 +783,7 @@ class Emitter(object):
                         same = [x for x in m.proc_model if x['from'] == src]
                         name = self._univ_name(src) if src in univ else src
                         t_.append('inc_%s[%d]' % (name, same.index(r)))
-            inc_terms.append(' + '.join(t_) or '0.0')
+            inc_terms.append(' + '.join(t_) or 'T(0)')
         if inc_terms:
             a('    for (int k = 0; k < INC_PER_CAC; ++k) {')
             a('      const int l = inc_link(cac, k);')
@@ -795,8 +796,8 @@ class Emitter(object):
         a('  template <bool DRIFT, bool NOENV, class T, class X, class E, class D>')
         a('  PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,')
         a('                               const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {')
-        a('    double inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = 0.0;')
+        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
         for k, tt in enumerate(self.time_terms):
@@ -805,11 +806,11 @@ class Emitter(object):
             si = m.par_sv.index(s_)
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
         a('    for (int cac = 0; cac < N_CAC; ++cac) {')
-        a('      plomrt::UniformStream rs;')
+        a('      typename plomrt::PsrStream<T>::type rs;')
         a('      rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);')
         a('      psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);')
         a('    }')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = (T)((double)x[OFF_INC+w] + inc_acc[w]);')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc[w];')
         a('    if (DRIFT) {')
         a('      // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)')
         a('      for (int i = 0; i < N_DRIFT; ++i) {')

@@ -44,6 +44,8 @@ class Oracle(object):
                                            _dp, C.POINTER(C.c_int), _dp, _dp]
         L.oracle_psr_samples.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, _dp]
         L.oracle_psr_samples.restype = None
+        L.oracle_psr_samples_f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, _dp]
+        L.oracle_psr_samples_f.restype = None
         L.oracle_ci95.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
         L.oracle_ci95.restype = None
         L.oracle_proj2obs.argtypes = [_dp, _dp]
@@ -138,9 +140,11 @@ class Oracle(object):
                              C.byref(lo), C.byref(hi))
         return lo.value, hi.value
 
-    def psr_samples(self, kind, a, b=0.0, seed=1, count=10000):
-        """Draws of the psr samplers: 'binomial' (n=a, p=b), 'poisson' (mu=a), 'gamma' (shape a, scale b)."""
+    def psr_samples(self, kind, a, b=0.0, seed=1, count=10000, precision=64):
+        """Draws of the psr samplers: 'binomial' (n=a, p=b), 'poisson' (mu=a), 'gamma' (shape a, scale b);
+        precision 32: the single-precision samplers of FP32 particle states."""
         out = np.zeros(count)
         k = {'binomial': 0, 'poisson': 1, 'gamma': 2}[kind]
-        self.lib.oracle_psr_samples(k, float(a), float(b), int(seed), int(count), out.ctypes.data_as(_dp))
+        fn = self.lib.oracle_psr_samples if precision == 64 else self.lib.oracle_psr_samples_f
+        fn(k, float(a), float(b), int(seed), int(count), out.ctypes.data_as(_dp))
         return out

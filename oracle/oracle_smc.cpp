@@ -460,6 +460,18 @@ void oracle_psr_samples(int kind, double a, double b, uint64_t seed, int count, 
   }
 }
 
+// The same draws with the single-precision samplers of FP32 particle states
+// (host build of the device code's algorithm).
+void oracle_psr_samples_f(int kind, double a, double b, uint64_t seed, int count, double* out) {
+  plomrt::UniformStreamF rs;
+  rs.init(plomrt::make_key(seed, 0u), 0u, 0u, 0u);
+  for (int i = 0; i < count; ++i) {
+    if (kind == 0) out[i] = plomrt::binomial(rs, (float)a, (float)b);
+    else if (kind == 1) out[i] = plomrt::poisson(rs, (float)a);
+    else out[i] = plomrt::gamma(rs, (float)a, (float)b);
+  }
+}
+
 // get_CI95 on given values and weights (null: 1/J), known-answer tests.
 void oracle_ci95(const double* v, const double* w, int J, double* lo, double* hi) {
   std::vector<double> vv(v, v + J);

@@ -36,14 +36,14 @@ def _norm_ref_update(line, par_sv, remainder):
 
 
 def _norm_mine_update(line, par_sv):
-    # x[0*N_CAC+cac] = (T)(inc_S[2] + inc_U[0]);
+    # x[0*N_CAC+cac] = (T)(inc_S[2] + inc_U[0]);  or  (T)(xo_R + inc_I[0]);
     i = int(re.search(r'x\[(\d+)\*N_CAC\+cac\]', line).group(1))
     rhs = line.split('=', 1)[1]
     terms = []
     for t in re.findall(r'inc_(\w+?)\[(\d+)\]', rhs):
         name = t[0][4:] if t[0].startswith('rem_') else t[0]
         terms.append((name, int(t[1])))
-    for t in re.findall(r'\(double\)xo_(\w+)', rhs):
+    for t in re.findall(r'\bxo_(\w+)', rhs):
         terms.append((t, 'x'))
     return par_sv[i], sorted(terms, key=str)
 
@@ -55,7 +55,7 @@ def test_psr_structure_matches_reference_generator(name):
     m = models.plom_model(name)
     code = _emitted_psr(name)
     # multinomial splits: one per compartment with exits, exits + stay categories
-    mine_multi = re.findall(r'plomrt::multinomial<(\d+)>\(rs, xs > 0\.0 \? floor\(xs\) : 0\.0, p, inc_(\w+)\)', code)
+    mine_multi = re.findall(r'plomrt::multinomial<(\d+)>\(rs, xs > T\(0\) \? floor\(xs\) : T\(0\), p, inc_(\w+)\)', code)
     assert sorted((s, int(k)) for k, s in mine_multi) == sorted((d['state'], d['nb_exit']) for d in ref['multinomial'])
     # Poisson arrivals: as many as the reference draws, from the same sources
     ref_pois = [re.search(r'inc\[ORDER_(\w+)\]\[cac\]\[(\d+)\]', p_).groups() for p_ in ref['poisson']]
@@ -75,10 +75,12 @@ def test_psr_structure_matches_reference_generator(name):
     assert mine_inc == ref_inc
 
 
-@pytest.mark.parametrize('n,p', [(7, 0.3), (40, 0.2), (1000, 0.05), (100000, 0.3), (2_000_000, 0.9), (50, 0.97)])
-def test_binomial_sampler(n, p):
+@pytest.mark.parametrize('precision', [64, 32])
+@pytest.mark.parametrize('n,p', [(7, 0.3), (40, 0.2), (1000, 0.05), (100000, 0.3), (2_000_000, 0.9), (50, 0.97),
+                                 (10_000_000, 1e-6), (10_000_000, 2e-6), (8_000_000, 1e-3)])
+def test_binomial_sampler(n, p, precision):
     orc = models.build_oracle('sir')
-    x = orc.psr_samples('binomial', n, p, seed=n, count=40000)
+    x = orc.psr_samples('binomial', n, p, seed=n, count=40000, precision=precision)
     assert np.all(x == np.floor(x)) and x.min() >= 0 and x.max() <= n
     mu, var = n * p, n * p * (1 - p)
     assert abs(x.mean() - mu) < 5 * math.sqrt(var / len(x))
@@ -92,10 +94,11 @@ def test_binomial_sampler(n, p):
         assert stats.chi2.sf(chi, keep.sum() - 1) > 1e-4
 
 
-@pytest.mark.parametrize('mu', [0.3, 4.0, 9.99, 10.0, 37.5, 2e4])
-def test_poisson_sampler(mu):
+@pytest.mark.parametrize('precision', [64, 32])
+@pytest.mark.parametrize('mu', [0.3, 4.0, 9.99, 10.0, 37.5, 2e4, 3e6])
+def test_poisson_sampler(mu, precision):
     orc = models.build_oracle('sir')
-    x = orc.psr_samples('poisson', mu, seed=int(mu * 100) + 1, count=40000)
+    x = orc.psr_samples('poisson', mu, seed=int(mu * 100) + 1, count=40000, precision=precision)
     assert np.all(x == np.floor(x)) and x.min() >= 0
     assert abs(x.mean() - mu) < 5 * math.sqrt(mu / len(x))
     assert abs(x.var() / mu - 1.0) < 0.05
@@ -108,10 +111,11 @@ def test_poisson_sampler(mu):
         assert stats.chi2.sf(chi, keep.sum() - 1) > 1e-4
 
 
+@pytest.mark.parametrize('precision', [64, 32])
 @pytest.mark.parametrize('a,theta', [(0.3, 2.0), (1.0, 1.0), (100.0, 0.01), (7.0, 3.0)])
-def test_gamma_sampler(a, theta):
+def test_gamma_sampler(a, theta, precision):
     orc = models.build_oracle('sir')
-    x = orc.psr_samples('gamma', a, theta, seed=int(a * 10) + 3, count=40000)
+    x = orc.psr_samples('gamma', a, theta, seed=int(a * 10) + 3, count=40000, precision=precision)
     assert x.min() > 0
     ks = stats.kstest(x, stats.gamma(a, scale=theta).cdf)
     assert ks.pvalue > 1e-4
@@ -151,14 +155,15 @@ def test_psr_gpu_matches_oracle(name, noises_off):
 
 
 @pytest.mark.gpu
-def test_psr_gpu_fp32_statistics():
-    """FP32 state: the psr log-likelihood estimator over replicates has the FP64 oracle's mean."""
-    eng = models.engine('sir')
-    orc = models.build_oracle('sir')
-    R = 40
-    g = [eng.smc(models.make_problem('sir', J=1000, dt=1.0, precision=32, seed=100 + r, psr=True)).loglik
+@pytest.mark.parametrize('name,J,R', [('sir', 1000, 40), ('seir3', 500, 24)])
+def test_psr_gpu_fp32_statistics(name, J, R):
+    """FP32 state (single-precision samplers): the psr log-likelihood estimator over replicates has the FP64
+    oracle's mean."""
+    eng = models.engine(name)
+    orc = models.build_oracle(name)
+    g = [eng.smc(models.make_problem(name, J=J, dt=1.0, precision=32, seed=100 + r, psr=True)).loglik
          for r in range(R)]
-    o = [orc.smc(models.make_problem('sir', J=1000, dt=1.0, precision=64, seed=500 + r, psr=True)).loglik
+    o = [orc.smc(models.make_problem(name, J=J, dt=1.0, precision=64, seed=500 + r, psr=True)).loglik
          for r in range(R)]
     se = math.sqrt(np.var(g) / R + np.var(o) / R)
     assert abs(np.mean(g) - np.mean(o)) < 4 * se + 0.5
