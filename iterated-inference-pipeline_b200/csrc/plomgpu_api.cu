@@ -114,6 +114,12 @@ struct plomgpu_plan {
   FilterAcc* acc_h = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  // one-shot filters (plomgpu_smc_run) enqueue the time loop on the stream
+  // instead of capturing it, and read the accumulator through pageable
+  // memory: a graph that runs once, and a pinned page read once, cost more
+  // than they save (SIR J = 1000, T = 52: 2.6 against 3.3 ms per call; SEIR
+  // 20x2 J = 1e5, T = 520: 319 against 322 ms)
+  bool direct = false;
   // optional timing events around every propagate launch (event record nodes of the graph)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // [2 * n_obs]: before / after propagate n
@@ -511,7 +517,10 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
   CK(cudaMalloc((void**)&p->tstat, (size_t)p->R * p->ntiles * sizeof(TileStatus)));
   CK(cudaMemsetAsync(p->tstat, 0, (size_t)p->R * p->ntiles * sizeof(TileStatus), s));
-  CK(cudaMallocHost((void**)&p->acc_h, sizeof(FilterAcc)));
+  // a reused plan reads its accumulator through pinned memory; a one-shot
+  // filter reads it once, and pinning a page costs more than the copy
+  if (p->direct) p->acc_h = new FilterAcc();
+  else CK(cudaMallocHost((void**)&p->acc_h, sizeof(FilterAcc)));
 
   const size_t n_par = (size_t)M::N_PAR_PROC * M::N_CAC;
   if (n_par > 0) {
@@ -615,6 +624,7 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
     for (auto& e : p->ev) CK(cudaEventCreate(&e));
   }
   CK(cudaStreamSynchronize(s));
+  if (p->direct) return PLOMGPU_OK;
 
   // capture the time loop
   CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -645,7 +655,10 @@ void plan_free(plomgpu_plan* p) {
                   p->traj_j, p->traj_n, p->traj_x};
   for (void* b : bufs)
     if (b) cudaFree(b);
-  if (p->acc_h) cudaFreeHost(p->acc_h);
+  if (p->acc_h) {
+    if (p->direct) delete p->acc_h;
+    else cudaFreeHost(p->acc_h);
+  }
   for (cudaEvent_t e : p->ev)
     if (e) cudaEventDestroy(e);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -668,7 +681,8 @@ int mif_group_tables(const plomgpu_mif_desc* mif, plomgpu_plan* p) {
 }
 
 int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bool want_xpred, bool want_final,
-                bool timing = false, const plomgpu_mif_desc* mif = nullptr, bool want_hat = false) {
+                bool timing = false, const plomgpu_mif_desc* mif = nullptr, bool want_hat = false,
+                bool direct = false) {
   *out = nullptr;
   int rc = check_desc(d);
   if (rc) return rc;
@@ -685,6 +699,7 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->want_xpred = want_xpred;
   p->timing = timing;
   p->want_hat = want_hat;
+  p->direct = direct;
   p->ode = d->ode != 0;
   p->psr = d->psr != 0;
   if (p->psr && (p->ode || p->crn || mif)) {
@@ -928,6 +943,7 @@ int plomgpu_plan_update_drift(plomgpu_plan* p, const double* drift_vol) {
 
 int plomgpu_plan_launch(plomgpu_plan* p) {
   if (!p) return fail(PLOMGPU_EINVAL, "null plan");
+  if (p->direct) return (p->tsize == sizeof(double)) ? enqueue_filter<double>(p) : enqueue_filter<float>(p);
   CK(cudaGraphLaunch(p->exec, p->stream));
   return PLOMGPU_OK;
 }
@@ -947,7 +963,7 @@ int plomgpu_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r) {
   if (!r) return fail(PLOMGPU_EINVAL, "null result");
   plomgpu_plan* p = nullptr;
   int rc = plan_create(d, &p, r->ancestors != nullptr, r->x_pred != nullptr, r->x_final != nullptr, false, nullptr,
-                       r->hat != nullptr || r->pred_res != nullptr);
+                       r->hat != nullptr || r->pred_res != nullptr, /*direct=*/true);
   if (rc) {
     r->status = rc;
     return rc;
