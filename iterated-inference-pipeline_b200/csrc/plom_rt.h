@@ -122,6 +122,55 @@ PLOM_HD double log_like_term(double y, double mu, double var, double like_min, i
   return log(l);
 }
 
+// The same term for FP32 particle states, in single precision.  The
+// differences y -/+ 1/2 - mu are taken in double (counts and means reach
+// 1e7, whose float spacing would shift the bounds), the rest in float
+// arranged so that no difference of nearly equal floats decides the value:
+// * 1/sd <= 1/20: the interval is narrow, and the probability is the density
+//   at its midpoint m times its width d with the next two terms of the
+//   expansion of Phi(m + d/2) - Phi(m - d/2), phi(m) d (1 + (m^2 - 1) d^2 / 24
+//   + (m^4 - 6 m^2 + 3) d^4 / 1920), whose first omitted term is
+//   He6(m) d^6 / 161280 relative (He6 the sixth Hermite polynomial; below
+//   3e-8 wherever the density is above LIKE_MIN = 1e-17, |m| < 8.4);
+// * otherwise: upper tails by erfc when the interval lies above the mean,
+//   lower tails when below, and 1 minus both tails when it straddles it.
+// Clamping, the floor count and the log are those of the double version;
+// the sum over series stays double.
+PLOM_HD double log_like_term_f(double y, double mu, double var, double like_min, int* floor_hits) {
+  const float k = 0.70710678118654752f;  // 1/sqrt(2)
+  const float inv = 1.0f / sqrtf((float)var);
+  float like;
+  if (y > 0.0) {
+    const float lo = (float)(y - 0.5 - mu) * inv, hi = (float)(y + 0.5 - mu) * inv;
+    if (inv <= 0.05f) {
+      const float m = 0.5f * (lo + hi), m2 = m * m, d2 = inv * inv;
+      like = 0.39894228040143268f * expf(-0.5f * m2) * inv *
+             (1.0f + (m2 - 1.0f) * d2 * (1.0f / 24.0f) + ((m2 - 6.0f) * m2 + 3.0f) * (d2 * d2) * (1.0f / 1920.0f));
+    } else if (lo >= 0.0f) {
+      like = 0.5f * (erfcf(lo * k) - erfcf(hi * k));
+    } else if (hi <= 0.0f) {
+      like = 0.5f * (erfcf(-hi * k) - erfcf(-lo * k));
+    } else {
+      like = 1.0f - 0.5f * (erfcf(hi * k) + erfcf(-lo * k));
+    }
+  } else {
+    like = 0.5f * erfcf(-(float)(y + 0.5 - mu) * inv * k);
+  }
+  if (!(like > (float)like_min) || isinf(like)) {
+    ++*floor_hits;
+    return log(like_min);
+  }
+  return (double)logf(like);
+}
+
+// the term of a particle precision: FP64 states (the parity modes) keep the
+// double version
+template <class T>
+PLOM_HD double log_like_term_p(double y, double mu, double var, double like_min, int* floor_hits) {
+  if constexpr (sizeof(T) == sizeof(float)) return log_like_term_f(y, mu, var, like_min, floor_hits);
+  else return log_like_term(y, mu, var, like_min, floor_hits);
+}
+
 // A particle's log-weight.  The reference fails a particle when
 // exp(loglik) <= LIKE_MIN^N_TS (smc.c:44); since every density is at least
 // LIKE_MIN, that holds in exact arithmetic exactly when all N_TS series are on

@@ -234,7 +234,7 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
           if (isnan(yy)) continue;
           const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
           const double var = M::obs_var(obs[ts], ts, t_obs, oe);
-          ll += plomrt::log_like_term(yy, mu, var, a.like_min, &fl);
+          ll += plomrt::log_like_term_p<T>(yy, mu, var, a.like_min, &fl);
         }
         const T l = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
         ws.lw[j] = l;

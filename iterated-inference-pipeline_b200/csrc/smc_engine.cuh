@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       if (isnan(y)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += plomrt::log_like_term(y, mu, var, tb.like_min, &fl);
+      ll += plomrt::log_like_term_p<T>(y, mu, var, tb.like_min, &fl);
     }
     ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
   }
@@ -566,7 +566,7 @@ __global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(con
       if (isnan(y)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += plomrt::log_like_term(y, mu, var, tb.like_min, &fl);
+      ll += plomrt::log_like_term_p<T>(y, mu, var, tb.like_min, &fl);
     }
     ll = tm.sum(ll);
     fl = tm.sum(fl);
@@ -1075,7 +1075,7 @@ __global__ void __launch_bounds__(BT) k_propagate_ode(const Tables<T> tb, const 
       if (isnan(yy)) continue;
       const double mu = M::obs_mean(obs[ts], ts, a.t_obs, oe);
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
-      ll += plomrt::log_like_term(yy, mu, var, tb.like_min, &fl);
+      ll += plomrt::log_like_term_p<T>(yy, mu, var, tb.like_min, &fl);
     }
     ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
   }

@@ -38,6 +38,9 @@ class Oracle(object):
         L.oracle_obs_moments.restype = None
         L.oracle_like.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double]
         L.oracle_like.restype = C.c_double
+        L.oracle_log_like_terms.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double, _dp, _dp, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_int)]
+        L.oracle_log_like_terms.restype = None
         L.oracle_weight_and_resample.argtypes = [_dp, C.c_int, C.c_double, C.c_double, _dp, _dp,
                                                  C.POINTER(C.c_uint32)]
         L.oracle_mif_iteration.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.MifDesc), _dp, _dp, _dp, _dp,
@@ -124,6 +127,18 @@ class Oracle(object):
 
     def like(self, y, mu, var, like_min):
         return self.lib.oracle_like(y, mu, var, like_min)
+
+    def log_like_terms(self, y, mu, var, like_min):
+        """(log term in double, in single precision, floor flags of each) for arrays y, mu, var."""
+        y, mu, var = (np.ascontiguousarray(a, dtype=np.float64) for a in (y, mu, var))
+        n = len(y)
+        o64, o32 = np.zeros(n), np.zeros(n)
+        f64, f32 = np.zeros(n, dtype=np.int32), np.zeros(n, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        self.lib.oracle_log_like_terms(n, y.ctypes.data_as(_dp), mu.ctypes.data_as(_dp), var.ctypes.data_as(_dp),
+                                       like_min, o64.ctypes.data_as(_dp), o32.ctypes.data_as(_dp),
+                                       f64.ctypes.data_as(ip), f32.ctypes.data_as(ip))
+        return o64, o32, f64, f32
 
     def proj2obs(self, x):
         x = np.ascontiguousarray(x, dtype=np.float64)

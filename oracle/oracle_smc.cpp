@@ -843,6 +843,18 @@ void oracle_obs_moments(double x, int ts, double t, const plomgpu_smc_desc* d, d
   *var = M::obs_var(x, ts, t, oe);
 }
 
+// One series' log-density term in both precisions (the single-precision
+// version is that of FP32 particle states), with their floor counts.
+void oracle_log_like_terms(int n, const double* y, const double* mu, const double* var, double like_min,
+                           double* out64, double* out32, int* floor64, int* floor32) {
+  for (int i = 0; i < n; ++i) {
+    floor64[i] = 0;
+    floor32[i] = 0;
+    out64[i] = plomrt::log_like_term(y[i], mu[i], var[i], like_min, floor64 + i);
+    out32[i] = plomrt::log_like_term_f(y[i], mu[i], var[i], like_min, floor32 + i);
+  }
+}
+
 double oracle_like(double y, double mu, double var, double like_min) {
   return plomrt::disc_normal_like(y, mu, var, like_min);
 }

@@ -241,3 +241,39 @@ def test_mif_components_per_group():
     Q, T = len(comp), p.n_obs
     ll, nf, bart, vt = orc.mif_iteration(p, h, th, np.full(Q, 0.05), np.full((T, Q), 0.01), np.zeros((T, Q)), 3)
     assert np.isfinite(ll).all()
+
+
+def test_single_precision_log_density_matches_double():
+    """The FP32 particle states' discretised-normal log-density: narrow intervals (sd >= 20) by the midpoint
+    expansion, wide ones by tail-aware erfc; counts and means up to 1e7.  Against tail-accurate values (the
+    double version, a difference of two CDFs like the reference's, loses the upper tail to cancellation below
+    about 1e-12) and against the double version where that one is accurate."""
+    from scipy import stats
+    orc = models.build_oracle('sir')
+    like_min = 1e-17
+    y, mu, var = [], [], []
+    for yy in [0.0, 1.0, 3.0, 17.0, 250.0, 4.0e3, 1.0e5, 2.5e6, 1.0e7]:
+        for sd in [0.3, 0.7, 1.0, 2.5, 7.0, 19.9, 20.0, 20.1, 55.0, 300.0, 4.0e3, 1.5e5]:
+            for k in np.linspace(-9.0, 9.0, 37):
+                m = yy + k * sd
+                if m < 0.0:
+                    continue
+                y.append(yy)
+                mu.append(m)
+                var.append(sd * sd)
+    y, mu, var = np.array(y), np.array(mu), np.array(var)
+    o64, o32, f64, f32 = orc.log_like_terms(y, mu, var, like_min)
+    sd = np.sqrt(var)
+    lo, hi = (y - 0.5 - mu) / sd, (y + 0.5 - mu) / sd
+    truth = np.where(y > 0, np.where(lo >= 0, stats.norm.sf(lo) - stats.norm.sf(hi),
+                                     stats.norm.cdf(hi) - stats.norm.cdf(lo)), stats.norm.cdf(hi))
+    ok = truth > 10 * like_min
+    assert ok.sum() > 2500
+    assert np.all(f32[ok] == 0)
+    assert np.abs(o32[ok] - np.log(truth[ok])).max() < 5e-5
+    accurate = ok & (o64 > math.log(1e-12))
+    assert accurate.sum() > 2000
+    assert np.abs(o32[accurate] - o64[accurate]).max() < 5e-5
+    # below the floor both clamp to it
+    under = truth < 0.1 * like_min
+    assert np.all(f32[under] == 1) and np.all(o32[under] == math.log(like_min))
