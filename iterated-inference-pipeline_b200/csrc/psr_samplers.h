@@ -269,10 +269,12 @@ PLOM_HD void multinomial(UniformStream& rs, double N, const double (&p)[K], doub
 // BTRD, and the final acceptance tests of BTRD and PTRS, whose terms are of
 // the order of the count (k log mu, log k!) and cancel to O(1).  Counts are
 // exact in float below 2^24, the range of an FP32 state's integers.
-PLOM_SAMPLER float s_log(float x) { return logf(x); }
-PLOM_SAMPLER float s_exp(float x) { return expf(x); }
-PLOM_SAMPLER float s_pow(float x, float y) { return powf(x, y); }
-PLOM_SAMPLER float s_log1p(float x) { return log1pf(x); }
+// float elementary functions inline (short; as calls the psr step of SEIR
+// 20x2 took 19.5 against 16.8 ms per interval), the samplers still calls
+PLOM_HD float s_log(float x) { return logf(x); }
+PLOM_HD float s_exp(float x) { return expf(x); }
+PLOM_HD float s_pow(float x, float y) { return powf(x, y); }
+PLOM_HD float s_log1p(float x) { return log1pf(x); }
 
 // Philox block (j, n, group, STREAM_PSR + 16 block) as four uniforms in (0, 1)
 PLOM_SAMPLER void psr_uniform_quad(PhiloxKey key, uint32_t j, uint32_t n, uint32_t group, uint32_t block, float* u) {
@@ -317,11 +319,16 @@ struct UniformStreamF {
 template <class T> struct PsrStream { typedef UniformStream type; };
 template <> struct PsrStream<float> { typedef UniformStreamF type; };
 
-// Inversion for n p < 14.  The float partial sums of the probabilities may
-// stop short of a uniform near 1; the search therefore ends at x = 110 (the
-// probability of more is below 1e-40 for a mean below 14) and the round
+// Inversion for n p < 40 (the double samplers switch to BTRD at 14; in
+// float the inversion loop is the cheaper of the two up to a mean of about
+// 60: SEIR 20x2 psr 16.7 / 14.7 / 13.7 / 13.2 ms per interval with the switch
+// at 14 / 30 / 40 / 60, and q^n = (1 - p)^n stays a normal float, above
+// 2^-80, below 40).  The float partial sums of the probabilities may stop
+// short of a uniform near 1; the search therefore ends at x = 200 (the
+// probability of more is below 1e-40 for a mean below 40) and the round
 // redraws, instead of walking up to n through probabilities that underflow.
-constexpr float kInversionMaxF = 110.0f;
+constexpr float kInversionMaxF = 200.0f;
+constexpr float kInversionMeanF = 40.0f;
 
 PLOM_HD float binomial_inversion(UniformStreamF& rs, float n, float p) {
   const float q = 1.0f - p;
@@ -407,7 +414,7 @@ PLOM_SAMPLER float binomial(UniformStreamF& rs, float n, float p) {
   if (p >= 1.0f) return n;
   const bool flip = p > 0.5f;
   const float pp = flip ? 1.0f - p : p;
-  const float x = (n * pp < 14.0f) ? binomial_inversion(rs, n, pp) : binomial_btrd(rs, n, pp);
+  const float x = (n * pp < kInversionMeanF) ? binomial_inversion(rs, n, pp) : binomial_btrd(rs, n, pp);
   return flip ? n - x : x;
 }
 

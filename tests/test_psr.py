@@ -76,7 +76,8 @@ def test_psr_structure_matches_reference_generator(name):
 
 
 @pytest.mark.parametrize('precision', [64, 32])
-@pytest.mark.parametrize('n,p', [(7, 0.3), (40, 0.2), (1000, 0.05), (100000, 0.3), (2_000_000, 0.9), (50, 0.97),
+@pytest.mark.parametrize('n,p', [(7, 0.3), (40, 0.2), (100, 0.3), (1000, 0.035), (1000, 0.05), (100000, 0.3),
+                                 (2_000_000, 0.9), (50, 0.97), (80, 0.5),
                                  (10_000_000, 1e-6), (10_000_000, 2e-6), (8_000_000, 1e-3)])
 def test_binomial_sampler(n, p, precision):
     orc = models.build_oracle('sir')
