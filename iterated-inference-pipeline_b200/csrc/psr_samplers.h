@@ -323,7 +323,8 @@ template <> struct PsrStream<float> { typedef UniformStreamF type; };
 // float the inversion loop is the cheaper of the two up to a mean of about
 // 60: SEIR 20x2 psr 16.7 / 14.7 / 13.7 / 13.2 ms per interval with the switch
 // at 14 / 30 / 40 / 60, and q^n = (1 - p)^n stays a normal float, above
-// 2^-80, below 40).  The float partial sums of the probabilities may stop
+// 2^-80, below 40); likewise Poisson counts below a mean of 40 (PTRS above;
+// 13.7 / 12.8 / 12.4 ms with the switch at 10 / 20 / 40).  The float partial sums of the probabilities may stop
 // short of a uniform near 1; the search therefore ends at x = 200 (the
 // probability of more is below 1e-40 for a mean below 40) and the round
 // redraws, instead of walking up to n through probabilities that underflow.
@@ -425,7 +426,7 @@ PLOM_SAMPLER bool ptrs_accept(double mu, double k, double v, double us, double a
 
 PLOM_SAMPLER float poisson(UniformStreamF& rs, float mu) {
   if (!(mu > 0.0f)) return 0.0f;
-  if (mu < 10.0f) {
+  if (mu < kInversionMeanF) {  // e^-mu stays a normal float; PTRS above
     for (int round = 0; round < kMaxRejection; ++round) {
       float u = rs.next(), p = s_exp(-mu), x = 0.0f;
       while (u > p) {

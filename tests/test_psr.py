@@ -96,7 +96,7 @@ def test_binomial_sampler(n, p, precision):
 
 
 @pytest.mark.parametrize('precision', [64, 32])
-@pytest.mark.parametrize('mu', [0.3, 4.0, 9.99, 10.0, 37.5, 2e4, 3e6])
+@pytest.mark.parametrize('mu', [0.3, 4.0, 9.99, 10.0, 37.5, 39.9, 40.0, 55.0, 2e4, 3e6])
 def test_poisson_sampler(mu, precision):
     orc = models.build_oracle('sir')
     x = orc.psr_samples('poisson', mu, seed=int(mu * 100) + 1, count=40000, precision=precision)
