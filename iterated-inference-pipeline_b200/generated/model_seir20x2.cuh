@@ -257,10 +257,9 @@ struct Model {
     for (int w = OFF_DRIFT; w < OFF_INC; ++w) f[w] = T(0);
     for (int w = 0; w < N_TS_INC_UNIQUE; ++w) f[OFF_INC+w] = inc_acc[w];
   }
-  template <bool DRIFT, bool NOENV, class T, class X, class E>
+  template <bool DRIFT, bool NOENV, class T, class X, class E, class IA>
   PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e,
-                              typename plomrt::PsrStream<T>::type& rs,
-                              T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {
+                              typename plomrt::PsrStream<T>::type& rs, IA& inc_acc, const Pre<T>& pre) {
     (void)t; (void)pre;
     const T ddt = dt;
     const T xo_S = x[0*N_CAC+cac];
@@ -268,6 +267,7 @@ struct Model {
     const T xo_I = x[2*N_CAC+cac];
     const T xo_R = x[3*N_CAC+cac];
     T foi_I = T(0);
+    PLOM_UNROLL
     for (int c2 = 0; c2 < N_CAC; ++c2) foi_I += e.coupling(cac, c2) * pre.yf_I[c2];
     T wn_0 = T(1);
     if (!NOENV) {
@@ -362,24 +362,26 @@ struct Model {
       const int l = inc_link(cac, k);
       if (l < 0) break;
       const int o = l >> 10, w = l & 1023;
-      if (o == 0) inc_acc[w] += inc_I[0];
+      if (o == 0) inc_acc.add(w, inc_I[0]);
     }
   }
   template <bool DRIFT, bool NOENV, class T, class X, class E, class D>
   PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,
                                const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {
-    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);
+    typename plomrt::IncAccFor<X, T, N_TS_INC_UNIQUE>::type inc_acc(x);
+    inc_acc.zero();
     Pre<T> pre;
     pre.unused = 0;
     pre.tt_0 = cos(((T(1)/T(182)))*T(3.141592653589793)*t);
+    PLOM_UNROLL
     for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_I[c2] = x[2*N_CAC+c2] / (x[0*N_CAC+c2]+x[1*N_CAC+c2]+x[2*N_CAC+c2]+x[3*N_CAC+c2]);
     for (int cac = 0; cac < N_CAC; ++cac) {
       typename plomrt::PsrStream<T>::type rs;
       rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);
       psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);
     }
-    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc[w];
+    PLOM_UNROLL
+    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc.get(w);
     if (DRIFT) {
       // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)
       for (int i = 0; i < N_DRIFT; ++i) {

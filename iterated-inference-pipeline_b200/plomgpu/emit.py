@@ -683,10 +683,9 @@ class Emitter(object):
                 e = '%s*wn_%d' % (e, [n for n, _ in noises].index(wn['name']))
             return e
 
-        a('  template <bool DRIFT, bool NOENV, class T, class X, class E>')
+        a('  template <bool DRIFT, bool NOENV, class T, class X, class E, class IA>')
         a('  PLOM_HD static void psr_cac(X& x, const int cac, const T t, const T dt, const E& e,')
-        a('                              typename plomrt::PsrStream<T>::type& rs,')
-        a('                              T (&inc_acc)[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1], const Pre<T>& pre) {')
+        a('                              typename plomrt::PsrStream<T>::type& rs, IA& inc_acc, const Pre<T>& pre) {')
         a('    (void)t; (void)pre;')
         a('    const T ddt = dt;')
         for i, s_ in enumerate(m.par_sv):
@@ -709,6 +708,7 @@ class Emitter(object):
             a('    }')
         for s_ in foi_states:
             a('    T foi_%s = T(0);' % s_)
+            a('    PLOM_UNROLL')
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) foi_%s += e.coupling(cac, c2) * pre.yf_%s[c2];' % (s_, s_))
         # 1: white noises
         for j, (name, sd) in enumerate(noises):
@@ -790,27 +790,29 @@ class Emitter(object):
             a('      if (l < 0) break;')
             a('      const int o = l >> 10, w = l & 1023;')
             for o, t_ in enumerate(inc_terms):
-                a('      if (o == %d) inc_acc[w] += %s;' % (o, t_))
+                a('      if (o == %d) inc_acc.add(w, %s);' % (o, t_))
             a('    }')
         a('  }')
         a('  template <bool DRIFT, bool NOENV, class T, class X, class E, class D>')
         a('  PLOM_HD static void step_psr(X& x, const T t, const T dt, const E& e, const plomrt::PhiloxKey key,')
         a('                               const uint32_t j, const uint32_t n, const uint32_t sub, D& draws) {')
-        a('    T inc_acc[N_TS_INC_UNIQUE > 0 ? N_TS_INC_UNIQUE : 1];')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) inc_acc[w] = T(0);')
+        a('    typename plomrt::IncAccFor<X, T, N_TS_INC_UNIQUE>::type inc_acc(x);')
+        a('    inc_acc.zero();')
         a('    Pre<T> pre;')
         a('    pre.unused = 0;')
         for k, tt in enumerate(self.time_terms):
             a('    pre.tt_%d = %s;' % (k, tt))
         for s_ in foi_states:
             si = m.par_sv.index(s_)
+            a('    PLOM_UNROLL')
             a('    for (int c2 = 0; c2 < N_CAC; ++c2) pre.yf_%s[c2] = x[%d*N_CAC+c2] / %s;' % (s_, si, self._npop_expr('c2')))
         a('    for (int cac = 0; cac < N_CAC; ++cac) {')
         a('      typename plomrt::PsrStream<T>::type rs;')
         a('      rs.init(key, j, n, sub * (uint32_t)(N_CAC + 1) + (uint32_t)cac);')
         a('      psr_cac<DRIFT, NOENV, T>(x, cac, t, dt, e, rs, inc_acc, pre);')
         a('    }')
-        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc[w];')
+        a('    PLOM_UNROLL')
+        a('    for (int w = 0; w < N_TS_INC_UNIQUE; ++w) x[OFF_INC+w] = x[OFF_INC+w] + inc_acc.get(w);')
         a('    if (DRIFT) {')
         a('      // Brownian walk of the drifted parameters (model_builder/C/core/drift.c:27-41)')
         a('      for (int i = 0; i < N_DRIFT; ++i) {')

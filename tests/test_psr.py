@@ -70,7 +70,7 @@ def test_psr_structure_matches_reference_generator(name):
     ref_inc = [sorted(re.findall(r'inc\[ORDER_(\w+)\]\[cac\]\[(\d+)\]', d['right_hand_side'])) for d in ref['obs_inc']]
     mine_inc = []
     for o in range(len(ref_inc)):
-        mm = re.search(r'if \(o == %d\) inc_acc\[w\] \+= (.*);' % o, code)
+        mm = re.search(r'if \(o == %d\) inc_acc\.add\(w, (.*)\);' % o, code)
         mine_inc.append(sorted((norm(a), b) for a, b in re.findall(r'inc_(\w+?)\[(\d+)\]', mm.group(1))))
     assert mine_inc == ref_inc
 
