@@ -67,10 +67,14 @@ def _stamp(name, extra):
 
 def nvcc_command(name, S, out=None, verbose_ptxas=False):
     smem = 1 if S > SMEM_STATE_WORDS else 0
-    # single precision: flush denormals, hardware-rate sqrt and division (the
-    # FP32 path is judged statistically; FP64 arithmetic is unaffected)
+    # single precision: flush denormals, hardware-rate sqrt and division, and the
+    # special-function-unit forms of exp / log / sin / cos / pow (the FP32 path
+    # is judged statistically; its quantities that cancel are computed in
+    # double, and FP64 arithmetic is unaffected).  The approximate forms took
+    # the SEIR 20x2 sde step from 0.529 to 0.514 ms and its psr step from 12.4
+    # to 11.1 ms per interval.
     cmd = [NVCC] + ARCH + ['-lineinfo', '-O3', '-std=c++17', '--expt-relaxed-constexpr',
-                           '-ftz=true', '-prec-div=false', '-prec-sqrt=false',
+                           '--use_fast_math', '-ftz=true', '-prec-div=false', '-prec-sqrt=false',
                            '-Xcompiler', '-fPIC', '-shared',
                            '-DPLOM_MODEL_HEADER="model_%s.cuh"' % name, '-DPLOM_SMEM_STATE=%d' % smem,
                            '-I', CSRC, '-I', GEN, '-I', INCLUDE,
@@ -86,10 +90,11 @@ def build_model(model, name, force=False, verbose=False, out=None):
     out = out or lib_path(name)
     os.makedirs(os.path.dirname(out), exist_ok=True)
     stamp_file = out + '.stamp'
-    stamp = _stamp(name, {'S': S, 'arch': ARCH})
+    cmd = nvcc_command(name, S, out=out)
+    # the compile line (flags included, output path excluded) is part of the stamp
+    stamp = _stamp(name, {'S': S, 'arch': ARCH, 'cmd': [c for c in cmd if c != out]})
     if not force and os.path.exists(out) and os.path.exists(stamp_file) and open(stamp_file).read() == stamp:
         return out
-    cmd = nvcc_command(name, S, out=out)
     if verbose:
         print(' '.join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
