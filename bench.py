@@ -31,7 +31,13 @@ WORKLOADS = {
     'seir20x2': ('seir20x2', 100000, 520, 1.0),
     # the same filter with the reference's default implementation (Poisson system with stochastic rates)
     'seir20x2_psr': ('seir20x2', 100000, 520, 1.0),
+    # the same filter without demographic noise (--no_dem_sto: environmental noise only)
+    'seir20x2_nodem': ('seir20x2', 100000, 520, 1.0),
+    # the deterministic Euler skeleton of the same filter (--no_dem_sto --no_white_noise)
+    'seir20x2_skel': ('seir20x2', 100000, 520, 1.0),
     'sir': ('sir', 1000, 52, 1.0),
+    # the SIR filter's Euler skeleton with 2^24 particles (4 state words: the HBM-bound case)
+    'sir_skel_large': ('sir', 1 << 24, 52, 1.0),
     # 4096 SIR parameter sets, J in 256..16384, T in 52..520 weeks, one persistent launch
     'sir_batch': ('sir', None, None, 1.0),
     # 64 iterated-filtering runs of the SEIR 20x2 model, J = 20000 each (per-iteration timing)
@@ -40,6 +46,10 @@ WORKLOADS = {
     'serve': (None, None, None, 1.0),
 }
 METRIC = 'particle-steps/s at matched loglik error'
+# noises_off of the workloads that turn noise terms off (bit 0: demographic, bit 1: environmental)
+NOISES_OFF = {'seir20x2_nodem': 1, 'seir20x2_skel': 3, 'sir_skel_large': 3}
+NOISE_TEXT = {0: 'sde full (demographic + environmental)', 1: 'sde without demographic noise (--no_dem_sto)',
+              3: 'Euler skeleton (--no_dem_sto --no_white_noise)'}
 
 
 def parse():
@@ -51,6 +61,7 @@ def parse():
     ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
+    ap.add_argument('--error-seeds', type=int, default=4, help='paired FP32 / FP64 filters for loglik_error (0: skip)')
     ap.add_argument('--plan-pool', type=int, default=4, help='serve: concurrent plans of the shared-memory model '
                     '(the SEIR 20x2 requests took 29.3 / 24.9 / 24.5 s with 2 / 3 / 4)')
     return ap.parse_args()
@@ -62,7 +73,7 @@ def workload_problem(name, precision=32, seed=0, J=None, nb_obs=-1):
     c, p, l, th = workloads.load(lib)
     m = model.PlomModel(c, p, l)
     return problem.Problem(m, m.settings(), th, J=J or J0, dt=dt, precision=precision, seed=seed, nb_obs=nb_obs,
-                           psr=name.endswith('_psr'))
+                           psr=name.endswith('_psr'), noises_off=NOISES_OFF.get(name, 0))
 
 
 def state_words(prob):
@@ -142,14 +153,37 @@ def measured_peak_hbm():
 
 
 def ncu_traffic(workload):
-    """Per-launch DRAM bytes of the propagate kernel from the committed ncu summary, scaled to J."""
+    """Per-launch DRAM bytes of the propagate kernel from the committed ncu summary, scaled to J, and
+    where they come from (the summary file and the date of its capture)."""
     path = os.path.join(ROOT, 'profiles', 'k_propagate_%s.json' % workload)
     try:
         with open(path) as f:
             d = json.load(f)
-        return float(d['dram_bytes_per_particle']) * WORKLOADS[workload][1]
+        src = 'profiles/k_propagate_%s.json (ncu capture of %s, not this run)' % (workload, d.get('captured', '?'))
+        return float(d['dram_bytes_per_particle']) * WORKLOADS[workload][1], src
     except (OSError, KeyError, ValueError):
+        return None, None
+
+
+def loglik_error(eng, workload, seeds):
+    """Precision error of the production arithmetic at the workload's size: whole FP32 filters against the
+    FP64 filters of the same seeds with paired draws (the FP32 filter consumes the FP64 filter's normals
+    and resampling uniforms, rounded), so that the difference is due to precision alone."""
+    if workload.endswith('_psr') or not seeds:
         return None
+    d = []
+    for s in seeds:
+        p = workload_problem(workload, precision=32, seed=s)
+        p.paired_draws = True
+        d.append(eng.smc(p, precision=32).loglik - eng.smc(p, precision=64).loglik)
+    d = [float(x) for x in d]
+    n = len(d)
+    mean = statistics.mean(d)
+    se = statistics.stdev(d) / math.sqrt(n) if n > 1 else None
+    return {'fp32_minus_fp64_mean': mean, 'se': se, 'mean_abs': statistics.mean(abs(x) for x in d), 'filters': n,
+            'unit': 'nats per filter', 'gate': 0.5,
+            'method': 'paired draws: FP32 state / FP64 reductions against FP64 everywhere, same normals and '
+                      'resampling uniforms, whole filters at the benchmark size'}
 
 
 def max_over_ranks(x, dist, device):
@@ -285,20 +319,15 @@ def run_batch(args):
     ms_single = e0.elapsed_time(e1) / reps
     plan.close()
     single_value = single.J * single.n_obs / (ms_single / 1000.0)
-    # log-likelihood error of the FP32 arithmetic against the FP64 path on a sample of
-    # sets, with common random numbers (same injected normals and uniforms): the
-    # difference is due to precision alone
-    sample = list(range(0, 4096, 256))
+    # log-likelihood error of the FP32 arithmetic against the FP64 path on every 16th
+    # set (256 sets), with paired draws (the FP32 filter consumes the FP64 filter's
+    # normals and resampling uniforms): the difference is due to precision alone
+    sample = list(range(0, 4096, 16))
     errs = []
-    rng = np.random.Generator(np.random.Philox(99))
     for i in sample:
-        p32 = bp.single(i, precision=32)
-        D = eng.draws_per_substep(p32.noises_off)
-        z = rng.standard_normal(int(p32.J) * int(np.sum(p32.n_sub)) * D)
-        u = rng.uniform(size=p32.n_obs)
-        a32 = eng.smc(p32, crn_normals=z, crn_uniforms=u).loglik
-        a64 = eng.smc(bp.single(i, precision=64), crn_normals=z, crn_uniforms=u).loglik
-        errs.append(a32 - a64)
+        p = bp.single(i)
+        p.paired_draws = True
+        errs.append(eng.smc(p, precision=32).loglik - eng.smc(p, precision=64).loglik)
     line = {'metric': METRIC, 'value': value, 'unit': 'particle-steps/s', 'n_gpus': 1, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
@@ -307,10 +336,12 @@ def run_batch(args):
             'plain_single_filter': {'value': single_value, 'ms_per_filter': ms_single, 'J': single.J,
                                     'T': single.n_obs},
             'batched_over_plain': value / single_value,
-            'loglik_error_fp32_vs_fp64_common_draws': {
-                'bias_mean': float(np.mean(errs)), 'bias_se': float(np.std(errs, ddof=1) / math.sqrt(len(errs))),
-                'mean_abs': float(np.mean(np.abs(errs))), 'sets': len(sample),
-                'note': 'paths split after an ancestor flips at the last bits of a weight; the bias is the error'},
+            'loglik_error': {
+                'fp32_minus_fp64_mean': float(np.mean(errs)), 'se': float(np.std(errs, ddof=1) / math.sqrt(len(errs))),
+                'mean_abs': float(np.mean(np.abs(errs))), 'max_abs': float(np.max(np.abs(errs))),
+                'filters': len(sample), 'unit': 'nats per filter', 'gate': 0.5,
+                'method': 'paired draws, plain one-shot filters of every 16th set (the batched kernel equals '
+                          'them per filter: tests/test_gpu_batch.py)'},
             'clocks': clk.summary(), 'gpu_launches': args.steps}
     print(json.dumps(line))
     return 0
@@ -534,7 +565,8 @@ def main():
         B = bytes_per_particle_step(prob, 4)
         avg_prop_ms = tot_prop / max(n_prop, 1)
         achieved = B * prob.J / (avg_prop_ms / 1000.0) / 1e9
-        traffic = ncu_traffic(args.workload)
+        traffic, traffic_src = ncu_traffic(args.workload)
+        err = loglik_error(eng, args.workload, [7000 + i for i in range(args.error_seeds)])
         line = {
             'metric': METRIC, 'value': value, 'unit': 'particle-steps/s', 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',
@@ -542,15 +574,18 @@ def main():
             'config': {'workload': args.workload, 'J': prob.J, 'T': prob.n_obs, 'K': int(prob.n_sub[0]),
                        'state_words': state_words(prob),
                        'noise': ('psr (multinomial + Poisson + Gamma white noise)' if prob.psr else
-                                 'sde full (demographic + environmental)'),
+                                 NOISE_TEXT[prob.noises_off]),
                        'parallelism': 'replicas' if world > 1 else 'single GPU',
                        'l2': 'inputs larger than L2 (two state generations of %.0f MB)' %
                              (2 * state_words(prob) * 4 * prob.J / 1e6)},
             'loglik': res.loglik,
+            'loglik_error': err,
             'euler_substeps_per_s': value * float(np.mean(prob.n_sub)),
             'gpu_launches': kernels_per_step * args.steps,
             'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                         'frac': achieved / peak, 'traffic': traffic,
+                         'frac': achieved / peak, 'traffic': traffic, 'traffic_source': traffic_src,
+                         'step_achieved': B * prob.J * prob.n_obs / (ms_step / 1000.0) / 1e9,
+                         'step_frac': B * prob.J * prob.n_obs / (ms_step / 1000.0) / 1e9 / peak,
                          'kernel': 'k_propagate', 'bytes_per_particle_step': B,
                          'avg_launch_ms': avg_prop_ms, 'peak_kind': peak_kind,
                          'propagate_share': tot_prop / (ms_total / args.steps),

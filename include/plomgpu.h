@@ -129,6 +129,16 @@ typedef struct plomgpu_smc_desc {
      * arrivals, Gamma white noise (off with PLOMGPU_NO_ENV_STO; the
      * demographic flag has no effect).  Philox draws only. */
     int psr;
+    /* Paired draws, for measuring the precision error (no counterpart in the
+     * reference): 1 makes a filter without crn_normals consume the normals
+     * of the precision-64 Philox filter of the same seed, rounded to the
+     * state precision, and its resampling uniforms, so that an FP32 filter
+     * and the FP64 filter of one seed see the same draws.  sde only. */
+    int paired_draws;
+    /* Optional initial particles, one per particle: [off_inc][J] (FP64),
+     * used instead of x0 replicated (x0 must still be given).  Plain filters
+     * only (no iterated filtering). */
+    const double *x0_particles;
 } plomgpu_smc_desc;
 
 typedef struct plomgpu_smc_result {
@@ -213,6 +223,17 @@ void plomgpu_plan_destroy(plomgpu_plan *plan);
 /* Test hook: the first J systematic-resampling points of offset U computed by
  * the device-side closed form (GPU) into out[J]. */
 int plomgpu_debug_systematic_points(double U, int J, double *out);
+
+/* Test hook: draws of the library's own generators on the device, as the
+ * filters compile them (single precision with the special-function-unit
+ * elementary functions), for distribution tests.  streams independent
+ * Philox streams (the particle slot of the counter) of per_stream draws each
+ * into out[streams * per_stream] (host).  kind 0: normals of the sde step
+ * (Box-Muller); 1: binomial(n = a, p = b); 2: Poisson(mean a); 3: Gamma
+ * (shape a, scale b); 4: normals of the psr uniform stream.  precision 32 or
+ * 64 picks the generators of FP32 or FP64 particle states. */
+int plomgpu_debug_draws(int kind, int precision, double a, double b, uint64_t seed, int streams, int per_stream,
+                        double *out);
 
 /* ------------------------------------------------------------------------
  * Iterated filtering (mif, model_builder/C/mif/mif.c:21-247): R independent
@@ -370,8 +391,10 @@ void plomgpu_server_destroy(plomgpu_server *server);
  * GPU that loads the library until exit), so J is limited to 262144
  * (PLOMGPU_EINVAL beyond).  Calls that overlap on the GPU, on any stream of
  * the same device, race on that array and must be serialised by the caller.
- * The first call on each device looks up the array's device address: make it
- * before any stream capture on that device. */
+ * Every call looks up the array's device address in the CUDA context current
+ * at the call, so the address is valid for that context only; the first call
+ * in a context also loads the library's device code there: make it before
+ * any stream capture on that device. */
 int plomgpu_resample_noalloc(const void *log_weights, int precision, int J, double like_min, double u,
                              uint32_t *ancestors, double *out, void *stream);
 

@@ -308,16 +308,21 @@ template <> struct NormalGen<float> {
 };
 
 template <> struct NormalGen<double> {
-  // 2 normals per Philox block (53-bit uniforms)
+  // the two normals of one Philox block (53-bit uniforms)
+  PLOM_HD static void block(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk, uint32_t tag, double* z0,
+                            double* z1) {
+    U4 c = {j, n, blk, tag};
+    const U4 r = philox4x32_10(c, k.k0, k.k1);
+    box_muller_d(u01d(r.x, r.y), u01d(r.z, r.w), z0, z1);
+  }
+  // 2 normals per Philox block
   template <int N>
   PLOM_HD static void fill(PhiloxKey k, uint32_t j, uint32_t n, uint32_t blk0, double* out,
                            uint32_t tag = STREAM_PROCESS) {
 #pragma unroll
     for (int b = 0; b < (N + 1) / 2; ++b) {
-      U4 c = {j, n, blk0 + (uint32_t)b, tag};
-      const U4 r = philox4x32_10(c, k.k0, k.k1);
       double z0, z1;
-      box_muller_d(u01d(r.x, r.y), u01d(r.z, r.w), &z0, &z1);
+      block(k, j, n, blk0 + (uint32_t)b, tag, &z0, &z1);
       if (2 * b + 0 < N) out[2 * b + 0] = z0;
       if (2 * b + 1 < N) out[2 * b + 1] = z1;
     }

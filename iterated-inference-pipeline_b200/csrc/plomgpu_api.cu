@@ -73,6 +73,8 @@ int draws_per_substep(int noises_off) {
 struct plomgpu_plan {
   int J = 0, n_obs = 0, sub_total = 0, precision = 32, noises_off = 0, filter = 1;
   bool crn = false, want_anc = false, want_xpred = false, want_llike = true;
+  bool paired = false;           // CRN kernels on the FP64 Philox draws (no table)
+  double* x0_cloud = nullptr;    // optional [OFF_INC][J] initial particles
   double dt = 1.0, like_min = 1e-17, thresh = 0.0, log_like_min = 0.0;
   std::vector<int> n_sub, sub0;
   std::vector<double> t_obs, crn_u;
@@ -350,7 +352,8 @@ int enqueue_filter(plomgpu_plan* p) {
   {
     const size_t total = (size_t)M::OFF_INC * RJ;
     const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
-    k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, (int)RJ, (T*)p->X[0]);
+    if (p->x0_cloud) k_init_cloud<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0_cloud, (int)RJ, (T*)p->X[0]);
+    else k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, (int)RJ, (T*)p->X[0]);
     ++kernels;
   }
   // summaries of the initial particles (time 0, incidences reset, equal weights)
@@ -380,7 +383,7 @@ int enqueue_filter(plomgpu_plan* p) {
     a.X_next = p->X[cur ^ 1];
     a.anc = anc_cur >= 0 ? p->anc[anc_cur] : nullptr;
     a.lw = p->lw;
-    a.crn = p->crn ? p->crn_tab + crn_off : nullptr;
+    a.crn = p->crn_tab ? p->crn_tab + crn_off : nullptr;
     a.crn_d = D;
     a.x_hist = p->x_hist ? p->x_hist + (size_t)n * M::S * RJ : nullptr;
     a.write_inc = ((p->x_final != nullptr && n == p->n_obs - 1) || p->want_hat) ? 1 : 0;
@@ -411,7 +414,7 @@ int enqueue_filter(plomgpu_plan* p) {
     if (p->mif) th_cur ^= 1;
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
-      const double Uc = p->crn ? p->crn_u[n] : -1.0;
+      const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
       k_weight<T, kBtWeight><<<dim3(p->nblk_weight, R), kBtWeight, 0, s>>>(
           (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->st, p->acc, p->tstat, p->ntiles, n, Uc,
           p->seed, 0u, p->llike, p->ess, p->n_obs);
@@ -453,6 +456,40 @@ int enqueue_filter(plomgpu_plan* p) {
   return PLOMGPU_OK;
 }
 
+// Draws of the production generators as this library compiles them (the
+// fast-math build of the FP32 path), for distribution tests: stream s is the
+// particle slot of the Philox counter, per_stream draws each.  kind 0: the
+// normals of the sde step (NormalGen<T>, Box-Muller); 1 / 2 / 3: the psr
+// samplers binomial(a, b), Poisson(a), Gamma(shape a, scale b) of precision T;
+// 4: the normals of the psr uniform stream (Gamma white noise).
+template <class T>
+__global__ void k_debug_draws(int kind, double a, double b, uint64_t seed, int streams, int per_stream,
+                              double* __restrict__ out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= streams) return;
+  const plomrt::PhiloxKey key = plomrt::make_key(seed, 0u);
+  double* o = out + (size_t)s * per_stream;
+  if (kind == 0) {
+    constexpr int P = plomrt::NormalGen<T>::per_block();
+    for (int i = 0; i < per_stream; i += P) {
+      T z[P];
+      plomrt::NormalGen<T>::template fill<P>(key, (uint32_t)s, 0u, (uint32_t)(i / P), z);
+      for (int q = 0; q < P && i + q < per_stream; ++q) o[i + q] = (double)z[q];
+    }
+    return;
+  }
+  typename plomrt::PsrStream<T>::type rs;
+  rs.init(key, (uint32_t)s, 0u, 0u);
+  for (int i = 0; i < per_stream; ++i) {
+    double v;
+    if (kind == 1) v = (double)plomrt::binomial(rs, (T)a, (T)b);
+    else if (kind == 2) v = (double)plomrt::poisson(rs, (T)a);
+    else if (kind == 3) v = (double)plomrt::gamma(rs, (T)a, (T)b);
+    else v = (double)rs.normal();
+    o[i] = v;
+  }
+}
+
 int check_desc(const plomgpu_smc_desc* d) {
   if (!d) return fail(PLOMGPU_EINVAL, "null descriptor");
   if (d->J < 1) return fail(PLOMGPU_EINVAL, "J must be >= 1");
@@ -466,6 +503,8 @@ int check_desc(const plomgpu_smc_desc* d) {
   if (drift_on(d->noises_off) && (!d->drift_group || !d->drift_ngroups || !d->drift_bt || !d->drift_vol))
     return fail(PLOMGPU_EINVAL, "drift tables missing");
   if (d->crn_normals && !d->crn_uniforms) return fail(PLOMGPU_EINVAL, "crn_uniforms missing");
+  if (d->paired_draws && (d->crn_normals || d->psr || d->ode))
+    return fail(PLOMGPU_EINVAL, "paired draws replace the Philox draws of the sde implementation only");
   if (!(d->dt > 0.0)) return fail(PLOMGPU_EINVAL, "dt must be > 0");
   if (!(d->like_min > 0.0)) return fail(PLOMGPU_EINVAL, "like_min must be > 0");
   long long sub_total = 0;
@@ -550,6 +589,7 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
     CK(cudaStreamSynchronize(s));
   }
   if ((rc = upload<double>(d->x0, (size_t)M::S, &p->x0, s))) return rc;
+  if (d->x0_particles && (rc = upload<double>(d->x0_particles, (size_t)M::OFF_INC * J, &p->x0_cloud, s))) return rc;
   if (p->ode && M::N_COV_CAC > 0) {
     if ((rc = upload<int>(d->cov_spline_meta, (size_t)3 * M::N_COV_CAC * M::N_CAC, &p->sp_meta, s))) return rc;
     if ((rc = upload<double>(d->cov_spline_x, (size_t)d->cov_spline_knots, &p->sp_x, s))) return rc;
@@ -652,7 +692,7 @@ void plan_free(plomgpu_plan* p) {
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
                   p->obs_slot, p->proc_cslot, p->obs_tslot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->sp_meta, p->sp_x, p->sp_y, p->sp_m2, p->data_idx, p->traj_t,
-                  p->traj_j, p->traj_n, p->traj_x};
+                  p->traj_j, p->traj_n, p->traj_x, p->x0_cloud};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (p->acc_h) {
@@ -694,7 +734,8 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->precision = d->precision;
   p->noises_off = d->noises_off;
   p->filter = d->filter;
-  p->crn = d->crn_normals != nullptr;
+  p->paired = d->paired_draws != 0;
+  p->crn = d->crn_normals != nullptr || p->paired;
   p->want_anc = want_anc;
   p->want_xpred = want_xpred;
   p->timing = timing;
@@ -750,7 +791,11 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   p->t_start.resize(d->n_obs);
   for (int n = 0; n < d->n_obs; ++n) p->t_start[n] = d->n_sub[n] > 0 ? d->t_sub[p->sub0[n]] : d->t_obs[n];
   p->sub_total = tot;
-  if (p->crn) p->crn_u.assign(d->crn_uniforms, d->crn_uniforms + d->n_obs);
+  if (d->crn_normals) p->crn_u.assign(d->crn_uniforms, d->crn_uniforms + d->n_obs);
+  if (d->x0_particles && mif) {
+    delete p;
+    return fail(PLOMGPU_EINVAL, "initial particles one by one are for plain filters");
+  }
   cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete p;
@@ -995,6 +1040,24 @@ int plomgpu_debug_systematic_points(double U, int J, double* out) {
   return PLOMGPU_OK;
 }
 
+int plomgpu_debug_draws(int kind, int precision, double a, double b, uint64_t seed, int streams, int per_stream,
+                        double* out) {
+  if (kind < 0 || kind > 4 || streams < 1 || per_stream < 1 || !out) return fail(PLOMGPU_EINVAL, "bad arguments");
+  if (precision != 32 && precision != 64) return fail(PLOMGPU_EINVAL, "precision must be 32 or 64");
+  if ((long long)streams * per_stream > (1LL << 28)) return fail(PLOMGPU_EINVAL, "too many draws");
+  const size_t n = (size_t)streams * per_stream;
+  double* d = nullptr;
+  CK(cudaMalloc((void**)&d, n * sizeof(double)));
+  const int g = (streams + 127) / 128;
+  if (precision == 32) k_debug_draws<float><<<g, 128>>>(kind, a, b, seed, streams, per_stream, d);
+  else k_debug_draws<double><<<g, 128>>>(kind, a, b, seed, streams, per_stream, d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out, d, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(PLOMGPU_ECUDA, std::string("debug draws: ") + cudaGetErrorString(e));
+  return PLOMGPU_OK;
+}
+
 int plomgpu_particle_values(const plomgpu_smc_desc* d, const double* X, int P, const int* rows, double* out) {
   if (!d || !X || !rows || !out || P < 1) return fail(PLOMGPU_EINVAL, "bad arguments");
   for (int i = 0; i < P; ++i)
@@ -1143,11 +1206,10 @@ struct NoAllocScratch {
 };
 
 // Shared by every call on a device and held by every GPU that loads this
-// library until the process exits (about 2.1 MB).
+// library until the process exits (about 2.1 MB).  Host code only knows its
+// name; the device address belongs to the CUDA context that loaded the
+// module, so it is looked up in the context current at every call.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
-
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {nullptr};
 
 __global__ void k_noalloc_out(const StepState* st, const FilterAcc* acc, double* out) {
   out[2] = (double)st->all_fail;
@@ -1186,21 +1248,15 @@ extern "C" int plomgpu_resample_noalloc(const void* log_weights, int precision, 
                                     std::to_string(kNoAllocMaxJ) + " particles");
   if (!(like_min > 0.0)) return fail(PLOMGPU_EINVAL, "like_min must be > 0");
   if (!(u >= 0.0 && u < 1.0)) return fail(PLOMGPU_EINVAL, "u must be in [0, 1)");
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return fail(PLOMGPU_EINVAL, "device index out of range");
+  // the scratch array's address in the context current now (the host-side
+  // name is not a device address).  Looked up at every call rather than
+  // cached per device index: a host runtime may make another context current
+  // or reset the device between calls, and an address kept from an earlier
+  // context would point at memory that is not this array.  The first call in
+  // a context loads this library's device code there.
   void* base = nullptr;
-  {
-    // set-up, once per device, with that device current: the symbol's
-    // address on this device (the host-side name is not a device address)
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-      void* p = nullptr;
-      CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-      g_noalloc_ptr[dev] = p;
-    }
-    base = g_noalloc_ptr[dev];
-  }
+  CK(cudaGetSymbolAddress(&base, g_noalloc_scratch));
+  if (!base) return fail(PLOMGPU_ECUDA, "no device address for the no-allocation scratch");
   NoAllocScratch* sc = reinterpret_cast<NoAllocScratch*>(base);
   cudaStream_t s = (cudaStream_t)stream;
   if (precision == 64) return noalloc_run<double>((const double*)log_weights, J, like_min, u, ancestors, out, s, sc);
@@ -1684,6 +1740,8 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   chk.J = o->max_J;
   chk.crn_normals = nullptr;
   chk.crn_uniforms = nullptr;
+  chk.paired_draws = 0;
+  chk.x0_particles = nullptr;
   chk.precision = o->precision;
   int rc = check_desc(&chk);
   if (rc) return rc;
@@ -1720,6 +1778,8 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->base.precision = o->precision;
   sv->base.crn_normals = nullptr;
   sv->base.crn_uniforms = nullptr;
+  sv->base.paired_draws = 0;
+  sv->base.x0_particles = nullptr;
   sv->base.n_sub = sv->n_sub_h.data();
   sv->base.t_sub = sv->t_sub_h.data();
   sv->base.t_obs = sv->t_obs_h.data();

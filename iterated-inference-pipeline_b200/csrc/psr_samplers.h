@@ -309,9 +309,12 @@ struct UniformStreamF {
     }
     return cache[used++];
   }
+  // Box-Muller with the angle in [-pi, pi): the special-function-unit cosine
+  // of the fast-math build is accurate on that range only; cos(a - pi) =
+  // -cos(a) flips the sign of the draw, not its distribution
   PLOM_HD float normal() {
     const float u1 = next(), u2 = next();
-    return sqrtf(-2.0f * s_log(u1)) * cosf(6.2831853071795865f * u2);
+    return sqrtf(-2.0f * s_log(u1)) * cosf(6.2831853071795865f * (u2 - 0.5f));
   }
 };
 

@@ -145,17 +145,50 @@ struct PhiloxDraws {
   }
 };
 
+// Common random numbers, one cac at a time: from an injected table, or,
+// without a table (paired draws), the normals that the FP64 filter of the
+// same seed draws for this (particle, interval, substep, cac), rounded to T.
+// Paired draws let an FP32 filter consume exactly the FP64 filter's normals,
+// so that the difference of their log-likelihoods is the precision error.
 template <class T, int V>
 struct TableDraws {
   static constexpr int PER_BLOCK = 1;
-  const double* p;  // draws of this particle and substep
+  const double* p;  // draws of this particle and substep, NULL: paired Philox draws
+  plomrt::PhiloxKey key;
+  uint32_t j, n, sub;
   template <int N>
   __device__ __forceinline__ void normals(int cac, T* out) const {
+    if (p) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) out[i] = (T)__ldg(p + cac * N + i);
+      for (int i = 0; i < N; ++i) out[i] = (T)__ldg(p + cac * N + i);
+      return;
+    }
+    // the FP64 step draws groups of G64 cacs from consecutive Philox blocks
+    // (whole blocks of 2 normals), the cacs after the last whole group one by one
+    constexpr int G64 = M::draw_group(N, plomrt::NormalGen<double>::per_block());
+    constexpr int NMAIN64 = M::N_CAC - (M::N_CAC % G64);
+    const int c0 = (cac < NMAIN64) ? cac - cac % G64 : cac;
+    const uint32_t blk0 = (sub * (uint32_t)(M::N_CAC + 1) + (uint32_t)c0) << 12;
+    const int i0 = (cac - c0) * N;
+    double z[2] = {0.0, 0.0};
+    int have = -1;
+    for (int q = 0; q < N; ++q) {
+      const int i = i0 + q;
+      if ((i >> 1) != have) {
+        have = i >> 1;
+        plomrt::NormalGen<double>::block(key, j, n, blk0 + (uint32_t)have, (uint32_t)plomrt::STREAM_PROCESS, &z[0],
+                                         &z[1]);
+      }
+      out[q] = (T)z[i & 1];
+    }
   }
   __device__ __forceinline__ T drift_normal(int i, int g) const {
-    return (T)__ldg(p + M::N_CAC * M::draws_per_cac(V) + i * M::N_CAC + g);
+    if (p) return (T)__ldg(p + M::N_CAC * M::draws_per_cac(V) + i * M::N_CAC + g);
+    double z0, z1;
+    plomrt::NormalGen<double>::block(
+        key, j, n, ((sub * (uint32_t)(M::N_CAC + 1) + (uint32_t)M::N_CAC) << 12) + (uint32_t)(i * M::N_CAC + g),
+        (uint32_t)plomrt::STREAM_PROCESS, &z0, &z1);
+    return (T)z0;
   }
 };
 
@@ -303,7 +336,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   e.dbt_ = tb.drift_bt;
   e.dvol_ = tb.drift_vol;
   const T dt = (T)tb.dt;
-  const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id + (uint32_t)r);
+  const plomrt::PhiloxKey key = plomrt::make_key(*tb.seed, tb.filter_id + (uint32_t)r);
 
   typedef typename std::conditional<MIF, MifObsEnv<MULTI>, ObsEnv>::type OEnv;
   OEnv oe;
@@ -383,7 +416,11 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       M::template step_psr<DRIFT, (V & 2) != 0, T>(x, t, dt, e, key, (uint32_t)j, (uint32_t)a.n, (uint32_t)k, d);
     } else if constexpr (CRN) {
       TableDraws<T, V> d;
-      d.p = a.crn + ((size_t)g * a.n_sub + k) * a.crn_d;
+      d.p = a.crn ? a.crn + ((size_t)g * a.n_sub + k) * a.crn_d : nullptr;
+      d.key = key;
+      d.j = (uint32_t)j;
+      d.n = (uint32_t)a.n;
+      d.sub = (uint32_t)k;
       M::template step<V, DRIFT, T>(x, t, dt, e, d);
     } else {
       PhiloxDraws<T, V> d;
@@ -528,14 +565,18 @@ __global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(con
   e.dbt_ = tb.drift_bt;
   e.dvol_ = tb.drift_vol;
   const T dt = (T)tb.dt;
-  const plomrt::PhiloxKey key = plomrt::make_key(CRN ? 0ull : *tb.seed, tb.filter_id + (uint32_t)r);
+  const plomrt::PhiloxKey key = plomrt::make_key(*tb.seed, tb.filter_id + (uint32_t)r);
   for (int k = 0; k < a.n_sub; ++k) {
     const int sub = a.sub0 + k;
     e.cov_ = tb.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
     const T t = (T)__ldg(tb.t_sub + sub);
     if constexpr (CRN) {
       TableDraws<T, V> d;
-      d.p = a.crn + ((size_t)g * a.n_sub + k) * a.crn_d;
+      d.p = a.crn ? a.crn + ((size_t)g * a.n_sub + k) * a.crn_d : nullptr;
+      d.key = key;
+      d.j = (uint32_t)j;
+      d.n = (uint32_t)a.n;
+      d.sub = (uint32_t)k;
       M::template step_team<V, DRIFT, T>(x, t, dt, e, d, tm, s_pre[lp]);
     } else {
       PhiloxDraws<T, V> d;
@@ -886,6 +927,14 @@ __global__ void k_init_state(const double* __restrict__ x0, int J, T* __restrict
     const int w = (int)(i / J);
     X[i] = (T)x0[w];
   }
+}
+
+// initial particles given one by one: cloud [OFF_INC][J] (FP64)
+template <class T>
+__global__ void k_init_cloud(const double* __restrict__ cloud, int J, T* __restrict__ X) {
+  const size_t total = (size_t)M::OFF_INC * J;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
+    X[i] = (T)cloud[i];
 }
 
 template <class T>

@@ -45,7 +45,7 @@ class SmcDesc(C.Structure):
                 ('crn_normals', _dp), ('crn_uniforms', _dp), ('pop_size', _dp), ('cov_ts0', _dp),
                 ('ode', C.c_int), ('eps_abs', C.c_double), ('eps_rel', C.c_double), ('cov_spline_meta', _ip),
                 ('cov_spline_x', _dp), ('cov_spline_y', _dp), ('cov_spline_m2', _dp), ('cov_spline_knots', C.c_int),
-                ('psr', C.c_int)]
+                ('psr', C.c_int), ('paired_draws', C.c_int), ('x0_particles', _dp)]
 
 
 class BatchDesc(C.Structure):
@@ -88,7 +88,7 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
                'plomgpu_server_create', 'plomgpu_server_submit', 'plomgpu_server_poll', 'plomgpu_server_wait',
                'plomgpu_server_get_stats', 'plomgpu_server_destroy', 'plomgpu_particle_values',
-               'plomgpu_plan_sample_traj', 'plomgpu_plan_update_drift']
+               'plomgpu_plan_sample_traj', 'plomgpu_plan_update_drift', 'plomgpu_debug_draws']
 
 
 def _ptr(a, t):
@@ -145,6 +145,12 @@ class DescHolder(object):
             crn_normals=_ptr(crn, _dp), crn_uniforms=_ptr(crnu, _dp), pop_size=_ptr(pop, _dp),
             cov_ts0=_ptr(cts0, _dp))
         self.desc.psr = 1 if getattr(p, 'psr', False) else 0
+        self.desc.paired_draws = 1 if getattr(p, 'paired_draws', False) else 0
+        if getattr(p, 'x0_particles', None) is not None:
+            xp = keep('x0_particles', p.x0_particles, np.float64)
+            if xp.shape != (self.model_off_inc(p), p.J):
+                raise ValueError('x0_particles must be [off_inc][J]')
+            self.desc.x0_particles = _ptr(xp, _dp)
         if getattr(p, 'ode', False):
             meta, xs, ys, m2 = p.spline_tables()
             meta = keep('sp_meta', meta if meta.size else np.zeros(3, np.int32), np.int32)
@@ -160,6 +166,12 @@ class DescHolder(object):
             d.cov_spline_y = _ptr(ys, _dp)
             d.cov_spline_m2 = _ptr(m2, _dp)
             d.cov_spline_knots = int(xs.size)
+
+
+    @staticmethod
+    def model_off_inc(p):
+        m = p.model
+        return len(m.par_sv) * m.N_CAC + len(m.drift_par_proc) * m.N_CAC
 
 
 class Outputs(object):
@@ -202,6 +214,7 @@ def _declare(lib):
     lib.plomgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_plan_destroy.restype = None
     lib.plomgpu_debug_systematic_points.argtypes = [C.c_double, C.c_int, _dp]
+    lib.plomgpu_debug_draws.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, _dp]
     lib.plomgpu_resample_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                              C.c_void_p, C.c_void_p, C.c_void_p]
     lib.plomgpu_last_error.restype = C.c_char_p
@@ -290,6 +303,16 @@ class Engine(object):
     def systematic_points(self, U, J):
         out = np.zeros(J)
         check(self.lib, self.lib.plomgpu_debug_systematic_points(U, J, _ptr(out, _dp)))
+        return out
+
+    DRAW_KINDS = {'normal': 0, 'binomial': 1, 'poisson': 2, 'gamma': 3, 'psr_normal': 4}
+
+    def draws(self, kind, a=0.0, b=0.0, seed=1, streams=1024, per_stream=64, precision=32):
+        """Draws of the device generators (test hook plomgpu_debug_draws): [streams * per_stream],
+        stream-major."""
+        out = np.zeros(int(streams) * int(per_stream))
+        check(self.lib, self.lib.plomgpu_debug_draws(self.DRAW_KINDS[kind], int(precision), float(a), float(b),
+                                                     int(seed), int(streams), int(per_stream), _ptr(out, _dp)))
         return out
 
 

@@ -94,7 +94,7 @@ class Problem(object):
 
     def __init__(self, model, settings, theta, J=1000, dt=1.0, nb_obs=-1, like_min=1e-17,
                  noises_off=0, filter=True, seed=2, precision=32, u_data='D', freeze_forcing=-1.0,
-                 ode=False, eps_abs=1e-6, eps_rel=1e-3, psr=False):
+                 ode=False, eps_abs=1e-6, eps_rel=1e-3, psr=False, paired_draws=False):
         if not isinstance(model, PlomModel):
             raise TypeError('model must be a PlomModel')
         m = self.model = model
@@ -114,6 +114,10 @@ class Problem(object):
             self.noises_off = 7
         # Poisson system with stochastic rates (the "psr" implementation)
         self.psr = bool(psr)
+        # draws of the FP64 filter of the same seed in any precision (precision-error measurement)
+        self.paired_draws = bool(paired_draws)
+        # optional initial particles one by one, [off_inc][J]
+        self.x0_particles = None
         if self.psr and self.ode:
             raise ValueError('psr and ode exclude each other')
         data = settings['data']
@@ -200,6 +204,29 @@ class Problem(object):
         self.par_ts = self.params.par_ts()
         self.x0 = self.params.x0(self.pop_size_t0)
         (self.drift_group, self.drift_ngroups, self.drift_bt, self.drift_vol, _) = self.params.drift_tables()
+
+    def interval_problem(self, n, x0_particles=None):
+        """The one-interval filter of observation interval n: its substeps, covariates and data row,
+        started from the particles x0_particles ([off_inc][J], FP64) when given."""
+        import copy
+        if not 0 <= n < self.n_obs:
+            raise ValueError('interval %d outside [0, %d)' % (n, self.n_obs))
+        q = copy.copy(self)
+        sub0 = int(np.sum(self.n_sub[:n]))
+        k = int(self.n_sub[n])
+        q.n_obs = 1
+        q.n_sub = self.n_sub[n:n + 1].copy()
+        q.t_sub = self.t_sub[sub0:sub0 + k].copy()
+        q.t_obs = self.t_obs[n:n + 1].copy()
+        q.data = self.data[n:n + 1].copy()
+        q.cov_cac = self.cov_cac[sub0:sub0 + k].copy()
+        q.cov_ts = self.cov_ts[n:n + 1].copy()
+        if n > 0:
+            q.cov_ts0 = self.cov_ts[n - 1].copy()
+        if self.pop_size is not None:
+            q.pop_size = self.pop_size[n:n + 2].copy()
+        q.x0_particles = None if x0_particles is None else np.ascontiguousarray(x0_particles, dtype=float)
+        return q
 
     @property
     def particle_steps(self):

@@ -493,7 +493,8 @@ int oracle_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r, int n_threa
   // AoS particles: proj[S] per particle, two generations
   std::vector<double> X((size_t)J * S), Xn((size_t)J * S);
   for (int j = 0; j < J; ++j)
-    for (int w = 0; w < S; ++w) X[(size_t)j * S + w] = (w < M::OFF_INC) ? d->x0[w] : 0.0;
+    for (int w = 0; w < S; ++w)
+      X[(size_t)j * S + w] = (w < M::OFF_INC) ? (d->x0_particles ? d->x0_particles[(size_t)w * J + j] : d->x0[w]) : 0.0;
   std::vector<double> wts(J);
   std::vector<uint32_t> select(J);
   if (r->hat) compute_hat(X, J, nullptr, d, d->cov_ts0, d->pop_size, 0.0, r->hat);

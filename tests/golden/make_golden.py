@@ -270,4 +270,6 @@ if __name__ == '__main__':
     # string hash so that the fixture is reproducible
     if os.environ.get('PYTHONHASHSEED') != '0':
         os.execve(sys.executable, [sys.executable] + sys.argv, dict(os.environ, PYTHONHASHSEED='0'))
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit('usage: python tests/golden/make_golden.py /path/to/reference')
+    main(sys.argv[1])

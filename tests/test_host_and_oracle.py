@@ -277,3 +277,40 @@ def test_single_precision_log_density_matches_double():
     # below the floor both clamp to it
     under = truth < 0.1 * like_min
     assert np.all(f32[under] == 1) and np.all(o32[under] == math.log(like_min))
+
+
+def test_oracle_interval_from_cloud_equals_interval_in_filter():
+    """One interval run alone from the resampled particles of the interval
+    before (x0_particles) equals the same interval inside the whole filter,
+    with the same CRN draws: the basis of the conditional precision-error
+    measurement."""
+    orc = models.build_oracle('seir3')
+    p = models.make_problem('seir3', J=200, dt=1.0, precision=64, seed=3, nb_obs=6)
+    D = orc.draws_per_substep(0)
+    rng = np.random.Generator(np.random.Philox(78))
+    z = rng.standard_normal(p.J * int(p.n_sub.sum()) * D)
+    u = rng.uniform(size=p.n_obs)
+    full = orc.smc(p, crn_normals=z, crn_uniforms=u, ancestors=True, x_pred=True)
+    off_inc = orc.info.off_inc
+    for n in (1, 3, 5):
+        cloud = full.x_pred[n - 1][:off_inc, full.ancestors[n - 1]]
+        sub0 = int(p.n_sub[:n].sum())
+        zn = z[p.J * sub0 * D:p.J * (sub0 + int(p.n_sub[n])) * D]
+        o = orc.smc(p.interval_problem(n, cloud), crn_normals=zn, crn_uniforms=u[n:n + 1], ancestors=True)
+        assert o.llike_n[0] == full.llike_n[n]
+        np.testing.assert_array_equal(o.ancestors[0], full.ancestors[n])
+    # the replicated cloud is the plain initial particle
+    rep = np.repeat(p.x0[:off_inc, None], p.J, axis=1)
+    q = p.interval_problem(0, rep)
+    zn = z[:p.J * int(p.n_sub[0]) * D]
+    a = orc.smc(q, crn_normals=zn, crn_uniforms=u[:1])
+    assert a.llike_n[0] == full.llike_n[0]
+
+
+def test_interval_problem_rejects_bad_cloud():
+    p = models.make_problem('sir', J=16, dt=1.0, nb_obs=4)
+    q = p.interval_problem(2, np.zeros((2, 16)))
+    with pytest.raises(ValueError):
+        native.DescHolder(q)
+    with pytest.raises(ValueError):
+        p.interval_problem(4)

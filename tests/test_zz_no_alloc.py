@@ -37,14 +37,14 @@ def _reference_interval(J, seed):
     return eng, g, lw, float(u[0])
 
 
-def _noalloc(eng, lw, u, like_min=1e-17):
+def _noalloc(eng, lw, u, like_min=1e-17, precision=64):
     import torch
     J = len(lw)
-    d_lw = torch.tensor(lw, dtype=torch.float64, device='cuda')
+    d_lw = torch.tensor(lw, dtype=torch.float64 if precision == 64 else torch.float32, device='cuda')
     d_anc = torch.full((J,), -1, dtype=torch.int32, device='cuda')
     d_out = torch.full((4,), -7.0, dtype=torch.float64, device='cuda')
     stream = torch.cuda.current_stream()
-    rc = eng.lib.plomgpu_resample_noalloc(ctypes.c_void_p(d_lw.data_ptr()), 64, J, like_min, u,
+    rc = eng.lib.plomgpu_resample_noalloc(ctypes.c_void_p(d_lw.data_ptr()), precision, J, like_min, u,
                                           ctypes.c_void_p(d_anc.data_ptr()), ctypes.c_void_p(d_out.data_ptr()),
                                           ctypes.c_void_p(stream.cuda_stream))
     native.check(eng.lib, rc)
@@ -72,6 +72,31 @@ def test_noalloc_matches_smc_run_twice_in_a_row():
     eng, g, lw, u = _reference_interval(4097, seed=42)
     anc3, out3 = _noalloc(eng, lw, u)
     _check(g, anc3, out3)
+
+
+def test_noalloc_single_precision_log_weights():
+    """FP32 log-weights (the production precision): the weights are read as
+    float and reduced in double, so the ancestors equal those of the same
+    values widened to double, and the oracle's weight() + systematic_sampling()
+    on their linear likelihoods; two calls in a row agree."""
+    eng, g, lw, u = _reference_interval(5000, seed=43)
+    lw32 = lw.astype(np.float32)
+    wide = lw32.astype(np.float64)
+    anc32, out32 = _noalloc(eng, lw32, u, precision=32)
+    anc64, out64 = _noalloc(eng, wide, u, precision=64)
+    np.testing.assert_array_equal(anc32, anc64)
+    assert np.array_equal(out32, out64)
+    orc = models.build_oracle('sir_short')
+    J = len(lw)
+    _, sel, ll, ess, fail = orc.weight_and_resample(np.exp(wide), (1.0 / J) * u)
+    assert not fail
+    np.testing.assert_array_equal(anc32, sel)
+    assert out32[0] == pytest.approx(ll, rel=1e-9)
+    assert out32[1] == pytest.approx(ess, rel=1e-8)
+    assert out32[2] == 0.0 and out32[3] == 0.0
+    anc32b, out32b = _noalloc(eng, lw32, u, precision=32)
+    np.testing.assert_array_equal(anc32, anc32b)
+    assert np.array_equal(out32, out32b)
 
 
 def test_noalloc_rejects_sizes_beyond_its_scratch():
