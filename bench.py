@@ -14,6 +14,7 @@ collective in the data path); time is the max over ranks.
 """
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -61,7 +62,8 @@ def parse():
     ap.add_argument('--workload', default='seir20x2', choices=sorted(WORKLOADS))
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
-    ap.add_argument('--error-seeds', type=int, default=4, help='paired FP32 / FP64 filters for loglik_error (0: skip)')
+    ap.add_argument('--error-samples', type=int, default=26,
+                    help='intervals sampled for loglik_error (0: skip)')
     ap.add_argument('--plan-pool', type=int, default=4, help='serve: concurrent plans of the shared-memory model '
                     '(the SEIR 20x2 requests took 29.3 / 24.9 / 24.5 s with 2 / 3 / 4)')
     return ap.parse_args()
@@ -165,25 +167,23 @@ def ncu_traffic(workload):
         return None, None
 
 
-def loglik_error(eng, workload, seeds):
-    """Precision error of the production arithmetic at the workload's size: whole FP32 filters against the
-    FP64 filters of the same seeds with paired draws (the FP32 filter consumes the FP64 filter's normals
-    and resampling uniforms, rounded), so that the difference is due to precision alone."""
-    if workload.endswith('_psr') or not seeds:
+def loglik_error(eng, prob, samples):
+    """Precision error of the production arithmetic at the workload's size, one interval at a time:
+    the same FP64 particle cloud advanced over one interval by the FP32 and the FP64 filter with paired
+    draws (the FP32 filter consumes the FP64 filter's normals and resampling uniforms), at ``samples``
+    intervals spread over an FP64 filter path (plomgpu.precision)."""
+    from plomgpu import precision
+    if prob.psr or samples <= 0:
         return None
-    d = []
-    for s in seeds:
-        p = workload_problem(workload, precision=32, seed=s)
-        p.paired_draws = True
-        d.append(eng.smc(p, precision=32).loglik - eng.smc(p, precision=64).loglik)
-    d = [float(x) for x in d]
-    n = len(d)
-    mean = statistics.mean(d)
-    se = statistics.stdev(d) / math.sqrt(n) if n > 1 else None
-    return {'fp32_minus_fp64_mean': mean, 'se': se, 'mean_abs': statistics.mean(abs(x) for x in d), 'filters': n,
-            'unit': 'nats per filter', 'gate': 0.5,
-            'method': 'paired draws: FP32 state / FP64 reductions against FP64 everywhere, same normals and '
-                      'resampling uniforms, whole filters at the benchmark size'}
+    p = copy.copy(prob)
+    stride = max(1, p.n_obs // samples)
+    n, d = precision.conditional_interval_errors(eng, p, stride=stride, seed=7000)
+    out = precision.summary(p, n, d)
+    out['method'] = ('conditional per interval: the same FP64 cloud advanced one interval in FP32 state / FP64 '
+                     'reductions and in FP64 everywhere with the same normals and uniforms, every %d-th interval '
+                     'of an FP64 filter path at the benchmark size; implied_filter_bias = T x the per-interval '
+                     'mean' % stride)
+    return out
 
 
 def max_over_ranks(x, dist, device):
@@ -566,7 +566,7 @@ def main():
         avg_prop_ms = tot_prop / max(n_prop, 1)
         achieved = B * prob.J / (avg_prop_ms / 1000.0) / 1e9
         traffic, traffic_src = ncu_traffic(args.workload)
-        err = loglik_error(eng, args.workload, [7000 + i for i in range(args.error_seeds)])
+        err = loglik_error(eng, prob, args.error_samples)
         line = {
             'metric': METRIC, 'value': value, 'unit': 'particle-steps/s', 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'weak',

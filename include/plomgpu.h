@@ -259,6 +259,30 @@ typedef struct plomgpu_mif_desc {
      * no slot is -2. */
     const int *proc_cac_slot;
     const int *obs_ts_slot;
+    /* Fixed-lag smoothing of the initial conditions and drift start values
+     * (update_fixed_lag_smoothing, model_builder/C/mif/methods.c:370-392) and
+     * the --prior patch (patch_likelihood_prior, methods.c:469-520); every
+     * field below is optional (NULL / 0: off). */
+    const int *fls;          /* [n_theta] 1: component fitted by fixed-lag smoothing: proposed
+                                with the others at the start of an iteration, resampled, never
+                                perturbed by the random walk */
+    const int *x0_slot;      /* [off_inc] component giving each initial state word, -1: the
+                                descriptor's x0.  Compartment words take the component's
+                                natural value (a proportion) times pop0 of their cac, drift
+                                words its transformed value (theta_driftIC2Xdrift) */
+    const double *pop0;      /* [n_cac] population size at t = 0 (with x0_slot) */
+    const int *vol_slot;     /* [n_drift][n_cac] component giving the volatility of drift i,
+                                group g; -1: the descriptor's drift_vol */
+    int lag;                 /* L: the fixed-lag means are the weighted means of the
+                                resampled components at interval L (L >= n_obs: none) */
+    int prior;               /* 1: weights times prior^(1/n_obs) for the random-walk
+                                components, prior^(1/lag) for the fixed-lag ones while
+                                n < lag (before the failure test and the normalisation) */
+    const int *prior_kind;   /* [n_theta] 0 flat on [lo, hi), 1 normal of mean (lo+hi)/2 and
+                                sd (hi-lo)/4, 2 pseudo-uniform (metropolis_hastings_prior.c) */
+    const double *prior_lo;  /* [n_theta] */
+    const double *prior_hi;  /* [n_theta] */
+    const plomgpu_back_transform *prior_finv; /* [n_theta] transformed -> scale of the prior */
 } plomgpu_mif_desc;
 
 typedef struct plomgpu_plan plomgpu_mif;
@@ -276,6 +300,10 @@ int plomgpu_mif_create(const plomgpu_smc_desc *base, const plomgpu_mif_desc *mif
 int plomgpu_mif_iteration(plomgpu_mif *mif, const double *theta_hat, const double *sd_init, const double *sd_mut,
                           const double *vt_add, uint64_t seed, double *loglik, int *n_all_fail, double *bart,
                           double *vt);
+/* Fixed-lag means [n_runs][n_theta] of the last iteration (NaN for the
+ * components not fitted by fixed-lag smoothing); *updated = 0 when the
+ * filter never reached interval L (L >= n_obs). */
+int plomgpu_mif_fls_means(plomgpu_mif *mif, double *out, int *updated);
 void plomgpu_mif_destroy(plomgpu_mif *mif);
 
 /* ------------------------------------------------------------------------

@@ -441,6 +441,36 @@ struct RegIncAcc {
   PLOM_HD T get(int w) const { return v[w]; }
 };
 
+// Priors of the natural-scale parameters (normal_prior, pseudo_unif_prior,
+// model_builder/C/core/metropolis_hastings_prior.c:95-133; the flat prior is
+// gsl_ran_flat_pdf): kind 0 flat on [lo, hi), 1 normal, 2 pseudo-uniform.
+PLOM_HD double prior_density(int kind, double x, double lo, double hi) {
+  if (kind == 1) {
+    const double mean = (hi + lo) / 2.0, sd = (hi - lo) / 4.0;
+    const double z = (x - mean) / sd;
+    return exp(-0.5 * z * z) / (2.5066282746310002 * sd);
+  }
+  if (kind == 2) {
+    const double delta = 0.01 * (hi - lo);
+    const double alpha = 1.0 / (hi - lo - 2.0 / 3.0 * delta);
+    const double a = -alpha / (delta * delta);
+    const double b = -2.0 * (lo + delta) * a;
+    const double c = alpha + a * (lo + delta) * (lo + delta);
+    if (x <= lo || x >= hi) return 0.0;
+    if (x < lo + delta) return a * x * x + b * x + c;
+    if (x < hi - delta) return alpha;
+    const double y = x - (hi - lo - 2.0 * delta);
+    return a * y * y + b * y + c;
+  }
+  return (x >= lo && x < hi) ? 1.0 / (hi - lo) : 0.0;
+}
+
+// log of a density floored at like_min (sanitize_likelihood, likelihood.c:77-92)
+PLOM_HD double log_sanitized(double p, double like_min) {
+  if (isnan(p) || isinf(p) || p < 0.0) return log(like_min);
+  return log(p <= like_min ? like_min : p);
+}
+
 // Accumulator of a particle store X; a store in shared memory may give the
 // sums words of their own there (one indexed load / add / store per term).
 template <class X, class T, int N>

@@ -60,6 +60,10 @@ constexpr int kIptScan = 8;
 constexpr int kTile = kBtScan * kIptScan;
 constexpr int kBtSearch = 256;
 constexpr int kMaxWeightBlocks = 592;
+// tiles of the filters' weighting / resampling (k_weight_tiles, k_resample)
+constexpr int kBtRes = 256;
+constexpr int kIptRes = 4;
+constexpr int kTileRes = kBtRes * kIptRes;
 
 int variant_of(int noises_off) { return noises_off & 3; }
 bool drift_on(int noises_off) { return M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT); }
@@ -79,19 +83,18 @@ struct plomgpu_plan {
   std::vector<int> n_sub, sub0;
   std::vector<double> t_obs, crn_u;
   std::vector<char> weigh;
-  int nblk_weight = 1, ntiles = 1;
+  int ntiles = 1;
   int kernels = 0;
   size_t tsize = 4;
   cudaStream_t stream = nullptr;
   // device buffers
   void* X[2] = {nullptr, nullptr};
   void* lw = nullptr;
-  double* C = nullptr;
+  double* P = nullptr;            // [R][ntiles + 1] tile prefixes of the normalised weights
   uint32_t* anc[2] = {nullptr, nullptr};
-  LseAcc* part = nullptr;
+  LseAcc* part = nullptr;         // [R][ntiles] tile partials
   StepState* st = nullptr;
   FilterAcc* acc = nullptr;
-  TileStatus* tstat = nullptr;
   void* par_cac = nullptr;        // T
   double* par_cac_d = nullptr;    // double staging
   void* cov_cac = nullptr;        // T
@@ -152,6 +155,15 @@ struct plomgpu_plan {
   bool psr = false;  // Poisson system with stochastic rates
   int* proc_cslot = nullptr;  // iterated filtering, per-group components
   int* obs_tslot = nullptr;
+  // iterated filtering: fixed-lag smoothing and the --prior patch
+  unsigned mut_mask = 0u;     // components perturbed by the random walk
+  unsigned fls_mask = 0u;     // components fitted by fixed-lag smoothing
+  int fls_n = -2;             // interval whose weights give the fixed-lag means (-1: initial proposal, -2: none)
+  MifTables* mx = nullptr;    // device
+  int* vol_slot = nullptr;    // device [N_DRIFT][N_CAC]
+  int* x0_slot = nullptr;     // device [OFF_INC]
+  double* pop0 = nullptr;     // device [N_CAC]
+  double* fls_out = nullptr;  // device [R][Q]
   // deterministic skeleton
   bool ode = false;
   double eps_abs = 1e-6, eps_rel = 1e-3;
@@ -333,11 +345,14 @@ int enqueue_filter(plomgpu_plan* p) {
   tb.obs_slot = p->obs_slot;
   tb.proc_cslot = p->proc_cslot;
   tb.obs_tslot = p->obs_tslot;
+  tb.mut_mask = p->mut_mask;
+  tb.vol_slot = p->vol_slot;
+  tb.mx = p->mx;
   const int R = p->R;
   const size_t RJ = (size_t)R * J;
 
   const PropLaunch<T> kp = pick_prop<T>(p->noises_off, p->crn, p->mif, p->psr,
-                                        p->proc_cslot != nullptr || p->obs_tslot != nullptr);
+                                        p->proc_cslot != nullptr || p->obs_tslot != nullptr || p->vol_slot != nullptr);
   if (!kp) return fail(PLOMGPU_EINVAL, "no propagate kernel for these options");
   const size_t smem = kp.smem;
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kp.k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -362,8 +377,13 @@ int enqueue_filter(plomgpu_plan* p) {
   if (p->mif) {
     const int g = (int)((RJ + 255) / 256 < 4096 ? (RJ + 255) / 256 : 4096);
     k_mif_init<T><<<g, 256, 0, s>>>(p->theta_hat, p->sd_init, p->Q, p->est_mask, R, J, p->seed, 0u,
-                                    (T*)p->theta[0]);
+                                    (T*)p->theta[0], p->x0_slot, p->pop0, p->x0, p->theta_bt, (T*)p->X[0], p->acc);
     ++kernels;
+    if (p->fls_n == -1) {
+      k_mif_fls<T, 256><<<dim3(p->Q, R), 256, 0, s>>>(nullptr, (const T*)p->theta[0], nullptr, J, R, p->thresh, p->st,
+                                                      p->fls_mask, p->Q, p->fls_out);
+      ++kernels;
+    }
   }
   const int D = p->crn ? draws_per_substep(p->noises_off) : 0;
   size_t crn_off = 0;
@@ -415,9 +435,9 @@ int enqueue_filter(plomgpu_plan* p) {
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
       const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
-      k_weight<T, kBtWeight><<<dim3(p->nblk_weight, R), kBtWeight, 0, s>>>(
-          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->st, p->acc, p->tstat, p->ntiles, n, Uc,
-          p->seed, 0u, p->llike, p->ess, p->n_obs);
+      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u, p->llike,
+          p->ess, p->n_obs);
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
                                                             p->thresh, p->st, p->theta_hat, p->vt_add, p->Q, n,
@@ -425,13 +445,17 @@ int enqueue_filter(plomgpu_plan* p) {
         ++kernels;
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
-      k_scan<T, kBtScan, kIptScan><<<dim3(p->ntiles, R), kBtScan, 0, s>>>((const T*)p->lw, J, p->thresh, p->st,
-                                                                         p->tstat, p->acc, p->C);
-      k_search<kBtSearch><<<dim3((J + kBtSearch - 1) / kBtSearch, R), kBtSearch, 0, s>>>(
-          p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
-      kernels += 3;
+      k_resample<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->thresh, p->part, p->P, p->st, p->anc[nxt],
+          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+      kernels += 2;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
+        ++kernels;
+      }
+      if (p->mif && n == p->fls_n) {
+        k_mif_fls<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], p->anc[nxt], J, R,
+                                                        p->thresh, p->st, p->fls_mask, p->Q, p->fls_out);
         ++kernels;
       }
       anc_cur = nxt;
@@ -539,23 +563,18 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(cudaMalloc(&p->X[0], (size_t)M::S * RJ * sizeof(T)));
   CK(cudaMalloc(&p->X[1], (size_t)M::S * RJ * sizeof(T)));
   CK(cudaMalloc(&p->lw, RJ * sizeof(T)));
-  CK(cudaMalloc((void**)&p->C, RJ * sizeof(double)));
   CK(cudaMalloc((void**)&p->anc[0], RJ * sizeof(uint32_t)));
   CK(cudaMalloc((void**)&p->anc[1], RJ * sizeof(uint32_t)));
   if (p->mif) {
     CK(cudaMalloc(&p->theta[0], (size_t)p->Q * RJ * sizeof(T)));
     CK(cudaMalloc(&p->theta[1], (size_t)p->Q * RJ * sizeof(T)));
   }
-  p->nblk_weight = (J + kBtWeight * 4 - 1) / (kBtWeight * 4);
-  if (p->nblk_weight > kMaxWeightBlocks) p->nblk_weight = kMaxWeightBlocks;
-  if (p->nblk_weight < 1) p->nblk_weight = 1;
-  p->ntiles = (J + kTile - 1) / kTile;
-  CK(cudaMalloc((void**)&p->part, (size_t)p->R * p->nblk_weight * sizeof(LseAcc)));
+  p->ntiles = (J + kTileRes - 1) / kTileRes;
+  CK(cudaMalloc((void**)&p->part, (size_t)p->R * p->ntiles * sizeof(LseAcc)));
+  CK(cudaMalloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
   CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
   CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
   CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
-  CK(cudaMalloc((void**)&p->tstat, (size_t)p->R * p->ntiles * sizeof(TileStatus)));
-  CK(cudaMemsetAsync(p->tstat, 0, (size_t)p->R * p->ntiles * sizeof(TileStatus), s));
   // a reused plan reads its accumulator through pinned memory; a one-shot
   // filter reads it once, and pinning a page costs more than the copy
   if (p->direct) p->acc_h = new FilterAcc();
@@ -686,13 +705,14 @@ void plan_free(plomgpu_plan* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  void* bufs[] = {p->X[0], p->X[1], p->lw, p->C, p->anc[0], p->anc[1], p->part, p->st, p->acc, p->tstat,
+  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->anc[0], p->anc[1], p->part, p->st, p->acc,
                   p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
                   p->theta_hat, p->sd_init, p->sd_mut, p->vt_add, p->bart, p->vt, p->theta_bt, p->proc_slot,
                   p->obs_slot, p->proc_cslot, p->obs_tslot, p->vals, p->hat, p->pred, p->pop, p->cov_ts0, p->sp_meta, p->sp_x, p->sp_y, p->sp_m2, p->data_idx, p->traj_t,
-                  p->traj_j, p->traj_n, p->traj_x, p->x0_cloud};
+                  p->traj_j, p->traj_n, p->traj_x, p->x0_cloud, p->mx, p->vol_slot, p->x0_slot, p->pop0,
+                  p->fls_out};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (p->acc_h) {
@@ -717,6 +737,65 @@ int mif_group_tables(const plomgpu_mif_desc* mif, plomgpu_plan* p) {
     return rc;
   if (obs_multi && (rc = upload<int>(mif->obs_ts_slot, (size_t)M::N_PAR_OBS * M::N_TS, &p->obs_tslot, p->stream)))
     return rc;
+  return PLOMGPU_OK;
+}
+
+// fixed-lag smoothing and prior tables of iterated filtering
+int mif_fls_tables(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mif, plomgpu_plan* p) {
+  const int Q = mif->n_theta;
+  cudaStream_t s = p->stream;
+  int rc = PLOMGPU_OK;
+  if (mif->vol_slot && M::N_DRIFT > 0) {
+    for (int i = 0; i < M::N_DRIFT * M::N_CAC; ++i)
+      if (mif->vol_slot[i] < -1 || mif->vol_slot[i] >= Q) return fail(PLOMGPU_EINVAL, "bad vol_slot");
+    if ((rc = upload<int>(mif->vol_slot, (size_t)M::N_DRIFT * M::N_CAC, &p->vol_slot, s))) return rc;
+  }
+  if (mif->x0_slot) {
+    if (!mif->pop0) return fail(PLOMGPU_EINVAL, "x0_slot needs pop0");
+    for (int w = 0; w < M::OFF_INC; ++w)
+      if (mif->x0_slot[w] < -1 || mif->x0_slot[w] >= Q) return fail(PLOMGPU_EINVAL, "bad x0_slot");
+    for (int c = 0; c < M::N_CAC; ++c)
+      if (!(mif->pop0[c] > 0.0)) return fail(PLOMGPU_EINVAL, "pop0 must be > 0");
+    if ((rc = upload<int>(mif->x0_slot, (size_t)M::OFF_INC, &p->x0_slot, s))) return rc;
+    if ((rc = upload<double>(mif->pop0, (size_t)M::N_CAC, &p->pop0, s))) return rc;
+  }
+  if (mif->prior && (!mif->prior_kind || !mif->prior_lo || !mif->prior_hi || !mif->prior_finv))
+    return fail(PLOMGPU_EINVAL, "the prior patch needs prior_kind / prior_lo / prior_hi / prior_finv");
+  if (p->fls_mask || mif->prior) {
+    if (mif->lag < 0) return fail(PLOMGPU_EINVAL, "lag must be >= 0");
+    MifTables h;
+    memset(&h, 0, sizeof h);
+    h.fls_mask = p->fls_mask;
+    h.lag = mif->lag;
+    h.prior = mif->prior ? 1 : 0;
+    h.inv_nobs = d->n_obs > 0 ? 1.0 / (double)d->n_obs : 0.0;
+    h.inv_lag = mif->lag > 0 ? 1.0 / (double)mif->lag : 0.0;
+    for (int q = 0; q < Q && mif->prior; ++q) {
+      h.prior_kind[q] = mif->prior_kind[q];
+      h.prior_lo[q] = mif->prior_lo[q];
+      h.prior_hi[q] = mif->prior_hi[q];
+      memcpy(&h.prior_finv[q], &mif->prior_finv[q], sizeof(plomrt::BackTransform));
+    }
+    if ((rc = upload<MifTables>(&h, 1, &p->mx, s))) return rc;
+    CK(cudaStreamSynchronize(s));
+  }
+  if (p->fls_mask) {
+    // the means are taken at interval L from the weights of the last weighted
+    // interval up to L (the reference's weights persist over intervals without data)
+    p->fls_n = -2;
+    if (mif->lag < d->n_obs) {
+      p->fls_n = -1;
+      for (int n = 0; n <= mif->lag; ++n) {
+        bool any = false;
+        for (int ts = 0; ts < M::N_TS; ++ts)
+          if (!isnan(d->data[(size_t)n * M::N_TS + ts])) any = true;
+        if (d->filter && any) p->fls_n = n;
+      }
+    }
+    CK(cudaMalloc((void**)&p->fls_out, (size_t)p->R * Q * sizeof(double)));
+    std::vector<double> nanv((size_t)p->R * Q, NAN);
+    CK(cudaMemcpy(p->fls_out, nanv.data(), nanv.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   return PLOMGPU_OK;
 }
 
@@ -768,8 +847,12 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
     p->mif = true;
     p->Q = mif->n_theta;
     p->est_mask = 0u;
-    for (int q = 0; q < mif->n_theta; ++q)
+    p->fls_mask = 0u;
+    for (int q = 0; q < mif->n_theta; ++q) {
       if (mif->estimated[q]) p->est_mask |= 1u << q;
+      if (mif->fls && mif->fls[q]) p->fls_mask |= 1u << q;
+    }
+    p->mut_mask = p->est_mask & ~p->fls_mask;
   }
   p->dt = d->dt;
   p->like_min = d->like_min;
@@ -814,7 +897,7 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
                                              &p->theta_bt, p->stream)) ||
         (rc2 = upload<int>(mif->proc_slot, (size_t)(M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 0), &p->proc_slot, p->stream)) ||
         (rc2 = upload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream)) ||
-        (rc2 = mif_group_tables(mif, p))) {
+        (rc2 = mif_group_tables(mif, p)) || (rc2 = mif_fls_tables(d, mif, p))) {
       std::string keep = g_err;
       plan_free(p);
       g_err = keep;
@@ -1175,7 +1258,23 @@ extern "C" int plomgpu_mif_iteration(plomgpu_mif* p, const double* theta_hat, co
     if (n_all_fail) n_all_fail[r] = p->acc_runs_h[r].n_all_fail;
     err |= p->acc_runs_h[r].error;
   }
+  if (err & ERR_IC)
+    return fail(PLOMGPU_EINVAL, "initial conditions: no proposal with proportions summing to at most 1 in " +
+                                    std::to_string(kMaxIcAttempts) + " draws");
   if (err) return fail(PLOMGPU_ETIMEOUT, "a bounded device wait ran out");
+  return PLOMGPU_OK;
+}
+
+extern "C" int plomgpu_mif_fls_means(plomgpu_mif* p, double* out, int* updated) {
+  if (!p || !p->mif || !out) return fail(PLOMGPU_EINVAL, "bad arguments");
+  if (updated) *updated = (p->fls_mask && p->fls_n != -2) ? 1 : 0;
+  const size_t n = (size_t)p->R * p->Q;
+  if (!p->fls_out) {
+    for (size_t i = 0; i < n; ++i) out[i] = NAN;
+    return PLOMGPU_OK;
+  }
+  CK(cudaMemcpyAsync(out, p->fls_out, n * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  CK(cudaStreamSynchronize(p->stream));
   return PLOMGPU_OK;
 }
 

@@ -193,6 +193,23 @@ struct TableDraws {
 };
 
 // ------------------------------------------------------------------ arguments
+constexpr int kMaxTheta = 16;
+
+// Iterated filtering: fixed-lag smoothing and the --prior patch
+// (update_fixed_lag_smoothing / patch_likelihood_prior,
+// model_builder/C/mif/methods.c:370-392,469-520).
+struct MifTables {
+  unsigned fls_mask;   // components fitted by fixed-lag smoothing
+  int lag;             // L
+  int prior;           // 1: --prior patch
+  double inv_nobs;     // exponent of the random-walk components' prior
+  double inv_lag;      // exponent of the fixed-lag components' prior while n < L
+  int prior_kind[kMaxTheta];
+  double prior_lo[kMaxTheta];
+  double prior_hi[kMaxTheta];
+  plomrt::BackTransform prior_finv[kMaxTheta];
+};
+
 template <class T>
 struct Tables {
   const T* par_cac;          // [N_PAR_PROC][N_CAC]
@@ -218,9 +235,10 @@ struct Tables {
   const int* obs_slot;                   // [N_PAR_OBS] component of each observation parameter, -1: table, -2: per series
   const int* proc_cslot;                 // [N_PAR_PROC][N_CAC] components of the per-cac parameters
   const int* obs_tslot;                  // [N_PAR_OBS][N_TS] components of the per-series parameters
+  unsigned mut_mask;                     // components perturbed by the random walk (estimated, not fixed-lag)
+  const int* vol_slot;                   // [N_DRIFT][N_CAC] component of each drift volatility, NULL: table
+  const MifTables* mx;                   // fixed-lag smoothing / prior patch, NULL: off
 };
-
-constexpr int kMaxTheta = 16;
 
 struct StepArgs {
   int n;                  // interval index
@@ -253,7 +271,26 @@ struct MifProcEnv : ProcEnv<T> {
   T parp[M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 1];
   unsigned uni, multi;
   const int* cslot;  // [N_PAR_PROC][N_CAC]
+  const int* vslot;  // [N_DRIFT][N_CAC] volatility components (MULTI only), NULL: table
   T natq[MULTI ? kMaxTheta : 1];
+  // the volatility of drift i, group g, from the particle's parameters when
+  // it is a component (back_transform_theta2par per particle feeds
+  // compute_drift, model_builder/C/core/drift.c:27-41)
+  __device__ __forceinline__ T drift_vol(int i, int g) const {
+    if constexpr (MULTI) {
+      if (vslot) {
+        const int q = __ldg(vslot + i * M::N_CAC + g);
+        if (q >= 0) {
+          T v = T(0);
+#pragma unroll
+          for (int qq = 0; qq < kMaxTheta; ++qq)
+            if (qq == q) v = natq[qq];
+          return v;
+        }
+      }
+    }
+    return ProcEnv<T>::drift_vol(i, g);
+  }
   __device__ __forceinline__ T par(int p, int cac) const {
     if (!((uni >> p) & 1u)) return this->par_[p * M::N_CAC + cac];
     if constexpr (!MULTI) return parp[p];
@@ -355,7 +392,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       nat[q] = 0.0;
       if (q < tb.Q) {
         T v = thp[(size_t)q * RJ + src];
-        if (a.sd_mut && ((tb.est_mask >> q) & 1u)) {
+        if (a.sd_mut && ((tb.mut_mask >> q) & 1u)) {
           T z[1];
           plomrt::NormalGen<T>::template fill<1>(key, (uint32_t)j, (uint32_t)a.n, (uint32_t)q, z,
                                                  (uint32_t)plomrt::STREAM_MUTATE);
@@ -368,6 +405,7 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
     e.uni = 0u;
     e.multi = 0u;
     e.cslot = tb.proc_cslot;
+    e.vslot = tb.vol_slot;
     if constexpr (MULTI) {
 #pragma unroll
       for (int q = 0; q < kMaxTheta; ++q) e.natq[q] = (T)nat[q];
@@ -454,7 +492,25 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
       const double var = M::obs_var(obs[ts], ts, a.t_obs, oe);
       ll += plomrt::log_like_term_p<T>(y, mu, var, tb.like_min, &fl);
     }
-    ((T*)a.lw)[g] = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
+    double lpr = 0.0;
+    if constexpr (MIF) {
+      // --prior: weight x prior^(1/n_obs) for the random-walk components,
+      // prior^(1/L) for the fixed-lag ones while n < L (patch_likelihood_prior,
+      // model_builder/C/mif/methods.c:469-520), on the parameters of this interval
+      const MifTables* mx = tb.mx;
+      if (mx && mx->prior) {
+        const T* __restrict__ thn = (const T*)a.theta_next;
+        for (int q = 0; q < tb.Q; ++q) {
+          if (!((tb.est_mask >> q) & 1u)) continue;
+          const bool fls = (mx->fls_mask >> q) & 1u;
+          if (fls && !(a.n < mx->lag)) continue;
+          const double x = plomrt::back_transform<double>((double)thn[(size_t)q * RJ + g], mx->prior_finv[q]);
+          const double pr = plomrt::prior_density(mx->prior_kind[q], x, mx->prior_lo[q], mx->prior_hi[q]);
+          lpr += plomrt::log_sanitized(pr, tb.like_min) * (fls ? mx->inv_lag : mx->inv_nobs);
+        }
+      }
+    }
+    ((T*)a.lw)[g] = (T)(plomrt::finish_loglik(ll, fl, M::N_TS) + lpr);
   }
 }
 
@@ -671,7 +727,7 @@ struct FilterAcc {
   unsigned tile_ticket;
 };
 
-enum { ERR_SCAN_WAIT = 1, ERR_SYS_TABLE = 2, ERR_ODE = 4 };
+enum { ERR_SCAN_WAIT = 1, ERR_SYS_TABLE = 2, ERR_ODE = 4, ERR_IC = 8 };
 
 template <class T>
 __device__ __forceinline__ bool weight_fails(T l, double thresh) {
@@ -919,6 +975,297 @@ __global__ void __launch_bounds__(BT) k_search(const double* __restrict__ C, int
   if (anc_hist) anc_hist[j] = r;
 }
 
+// ------------------------------------------------------------------ tiled resampling
+// weight() + systematic_sampling() (model_builder/C/core/smc.c:27-112) over
+// tiles of TILE consecutive particles, in two launches:
+//   k_weight_tiles  per tile: (max, sum exp(l - max), sum exp(2 (l - max)),
+//                   failures); the last block folds them in tile order
+//                   (llike, ESS, all-fail rule, systematic points) and lays out
+//                   the exclusive prefix P[b] of the tiles' normalised weights;
+//   k_resample      per tile: the cumulative weights of its particles
+//                   C_i = P[b] + (prefix of exp(l - max_b)) * exp(max_b - max) / sum
+//                   in shared memory, and the ancestor of every systematic
+//                   point P[b] < point_j <= P[b+1] (first i with C_i >= point_j).
+// The points of a tile are found from the closed form of the points, so no
+// cumulative-weight array goes to memory and no search crosses tiles; every
+// reduction runs in a fixed order (results do not depend on timing).
+template <class T>
+__device__ __forceinline__ double surviving_exp(T l, double thresh, double m) {
+  return weight_fails(l, thresh) ? 0.0 : exp((double)l - m);
+}
+
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double thresh,
+                                                     double log_like_min, LseAcc* part, double* P, StepState* st,
+                                                     FilterAcc* acc, int n, double U_crn, const uint64_t* seed,
+                                                     uint32_t filter_id, double* llike_out, double* ess_out,
+                                                     int out_stride) {
+  constexpr int TILE = BT * IPT;
+  __shared__ LseAcc sh[BT / 32];
+  __shared__ double shd[BT / 32];
+  __shared__ bool last;
+  const int ntiles = gridDim.x;
+  {
+    const int r = blockIdx.y;
+    lw += (size_t)r * J;
+    part += (size_t)r * ntiles;
+    P += (size_t)r * (ntiles + 1);
+    st += r;
+    acc += r;
+    if (llike_out) llike_out += (size_t)r * out_stride;
+    if (ess_out) ess_out += (size_t)r * out_stride;
+    filter_id += (uint32_t)r;
+  }
+  const int base = blockIdx.x * TILE;
+  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int i = base + k * BT + threadIdx.x;
+    if (i < J) {
+      const T l = lw[i];
+      if (weight_fails(l, thresh)) {
+        a.nfail += 1;
+      } else {
+        LseAcc b = {(double)l, 1.0, 1.0, 0};
+        a = lse_merge(a, b);
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+    if (threadIdx.x == 0) {
+      part[blockIdx.x] = a;
+      __threadfence();
+      const unsigned t = atomicAdd(&acc->ticket, 1u);
+      last = (t == (unsigned)ntiles - 1u);
+    }
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // the last block: fold the tiles in a fixed order (contiguous chunks per thread)
+  const int chunk = (ntiles + BT - 1) / BT;
+  const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
+  a = LseAcc{-INFINITY, 0.0, 0.0, 0};
+  for (int b = b0; b < b1; ++b) {
+    volatile LseAcc* p = part + b;
+    LseAcc v = {p->m, p->s1, p->s2, p->nfail};
+    a = lse_merge(a, v);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
+    if (threadIdx.x == 0) sh[0] = a;
+  }
+  __syncthreads();
+  a = sh[0];
+  const int all_fail = (a.nfail == J);
+  // exclusive prefix of the tiles' normalised weights: chunk totals, a block
+  // scan of them, then each chunk written in order
+  double tot = 0.0;
+  if (!all_fail) {
+    for (int b = b0; b < b1; ++b) {
+      volatile LseAcc* p = part + b;
+      if (p->s1 > 0.0) tot += p->s1 * (exp(p->m - a.m) / a.s1);
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double v = tot;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double o = __shfl_up_sync(0xffffffffu, v, off);
+    if (lane >= off) v += o;
+  }
+  if (lane == 31) shd[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    double w = (lane < BT / 32) ? shd[lane] : 0.0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += o;
+    }
+    if (lane < BT / 32) shd[lane] = w;
+  }
+  __syncthreads();
+  double run = ((warp > 0) ? shd[warp - 1] : 0.0) + (v - tot);
+  for (int b = b0; b < b1; ++b) {
+    P[b] = run;
+    if (!all_fail) {
+      volatile LseAcc* p = part + b;
+      if (p->s1 > 0.0) run += p->s1 * (exp(p->m - a.m) / a.s1);
+    }
+  }
+  if (b1 == ntiles && b0 < b1) P[ntiles] = run;
+  if (threadIdx.x == 0) {
+    acc->ticket = 0u;
+    double llike, ess;
+    if (all_fail) {
+      // every particle failed: equal weights, identity ancestors (smc.c:55-69)
+      llike = log_like_min * (double)M::N_TS;
+      ess = 0.0;
+      acc->n_all_fail += 1;
+    } else {
+      llike = a.m + log(a.s1 / (double)J);
+      ess = (a.s1 * a.s1) / a.s2;
+    }
+    acc->loglik += llike;
+    st->m = a.m;
+    st->s1 = a.s1;
+    st->s2 = a.s2;
+    st->all_fail = all_fail;
+    if (llike_out) llike_out[n] = llike;
+    if (ess_out) ess_out[n] = ess;
+    const double inc = 1.0 / (double)J;
+    const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(plomrt::make_key(*seed, filter_id), (uint32_t)n);
+    const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
+    st->U = U;
+    int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
+    if (ns < 0) {
+      acc->error |= ERR_SYS_TABLE;
+      ns = 0;
+    }
+    st->nseg = ns;
+  }
+}
+
+// first j in [0, J] whose systematic point exceeds v (J when none): the
+// points are U + j / J up to the rounding of the reference's running sum, so
+// the closed-form guess is off by at most one step; a bounded walk fixes it
+// and a binary search takes over if the walk runs long.
+__device__ __forceinline__ int first_point_above(const plomrt::SysSeg* seg, int ns, int J, double U, double v) {
+  double g = floor((v - U) * (double)J) + 1.0;
+  int j = g < 0.0 ? 0 : (g > (double)J ? J : (int)g);
+  for (int it = 0; it < 64; ++it) {
+    if (j > 0 && plomrt::systematic_point(seg, ns, j - 1) > v) {
+      --j;
+    } else if (j < J && !(plomrt::systematic_point(seg, ns, j) > v)) {
+      ++j;
+    } else {
+      return j;
+    }
+  }
+  int lo = 0, hi = J;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (plomrt::systematic_point(seg, ns, mid) > v) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J, double thresh,
+                                                 const LseAcc* __restrict__ part, const double* __restrict__ P,
+                                                 const StepState* st, uint32_t* __restrict__ anc,
+                                                 uint32_t* __restrict__ anc_hist) {
+  constexpr int TILE = BT * IPT;
+  __shared__ double sC[TILE];
+  __shared__ double swarp[BT / 32];
+  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  __shared__ int s_ns, s_fail, s_jlo, s_jhi, s_lastpos;
+  const int ntiles = gridDim.x;
+  {
+    const int r = blockIdx.y;
+    lw += (size_t)r * J;
+    part += (size_t)r * ntiles;
+    P += (size_t)r * (ntiles + 1);
+    st += r;
+    anc += (size_t)r * J;
+    if (anc_hist) anc_hist += (size_t)r * J;
+  }
+  const int b = blockIdx.x, base = b * TILE;
+  const int n_in = min(TILE, J - base);
+  if (threadIdx.x == 0) {
+    s_ns = st->nseg;
+    s_fail = st->all_fail;
+    s_lastpos = -1;
+  }
+  __syncthreads();
+  if (s_fail || s_ns == 0) {
+    // every particle failed (or the point table overflowed): identity
+    for (int i = threadIdx.x; i < n_in; i += BT) {
+      anc[base + i] = (uint32_t)(base + i);
+      if (anc_hist) anc_hist[base + i] = (uint32_t)(base + i);
+    }
+    return;
+  }
+  const int ns = s_ns;
+  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = st->seg[i];
+  // cumulative weights of the tile, rows of BT particles in order
+  const double mb = part[b].m;
+  const double f = (part[b].s1 > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
+  const double Pb = P[b];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double carry = 0.0;
+  int lastpos = -1;
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int ii = k * BT + threadIdx.x;
+    double p = 0.0;
+    if (ii < n_in) {
+      p = surviving_exp(lw[base + ii], thresh, mb);
+      if (p > 0.0) lastpos = ii;
+    }
+    double v = p;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, v, off);
+      if (lane >= off) v += o;
+    }
+    if (lane == 31) swarp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      double w = (lane < BT / 32) ? swarp[lane] : 0.0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double o = __shfl_up_sync(0xffffffffu, w, off);
+        if (lane >= off) w += o;
+      }
+      if (lane < BT / 32) swarp[lane] = w;
+    }
+    __syncthreads();
+    const double incl = carry + ((warp > 0) ? swarp[warp - 1] : 0.0) + v;
+    sC[ii] = Pb + incl * f;
+    carry += swarp[BT / 32 - 1];
+    __syncthreads();
+  }
+  if (lastpos >= 0) atomicMax(&s_lastpos, lastpos);
+  if (threadIdx.x == 0) {
+    const double U = st->U;
+    s_jlo = (b == 0) ? 0 : first_point_above(seg, ns, J, U, Pb);
+    s_jhi = (b == ntiles - 1) ? J : first_point_above(seg, ns, J, U, P[b + 1]);
+  }
+  __syncthreads();
+  const int jlo = s_jlo, jhi = s_jhi;
+  // past the tile's last cumulative weight (rounding): its last surviving
+  // particle, and the last particle for the last tile (the reference reads on
+  // past the array there)
+  const int clamp = (b == ntiles - 1 || s_lastpos < 0) ? n_in - 1 : s_lastpos;
+  for (int j = jlo + threadIdx.x; j < jhi; j += BT) {
+    const double ran = plomrt::systematic_point(seg, ns, j);
+    int lo = 0, hi = n_in;
+    while (lo < hi) {  // first i with !(ran > C[i])  (smc.c:105-108)
+      const int mid = (lo + hi) >> 1;
+      if (ran > sC[mid]) lo = mid + 1; else hi = mid;
+    }
+    const uint32_t a_ = (uint32_t)(base + (lo < n_in ? lo : clamp));
+    anc[j] = a_;
+    if (anc_hist) anc_hist[j] = a_;
+  }
+}
+
 // ------------------------------------------------------------------ helpers
 template <class T>
 __global__ void k_init_state(const double* __restrict__ x0, int J, T* __restrict__ X) {
@@ -966,25 +1313,108 @@ __global__ void k_reset_acc(FilterAcc* acc, int R = 1) {
 // ------------------------------------------------------------------ iterated filtering
 // Initial parameters of every particle of every run: theta_hat of the run plus a
 // Gaussian proposal on the estimated components (propose_safe_theta_and_load_X0
-// with ran_proposal, model_builder/C/mif/mif.c:119-121, C/core/proposal.c:40-62).
+// with ran_proposal, model_builder/C/mif/mif.c:119-121, C/core/proposal.c:40-79),
+// and, for components that are initial conditions (x0_slot), the particle's
+// initial state: proportion x N(0) for compartments (prop2Xpop_size), the
+// transformed value for drift words (theta_driftIC2Xdrift).  A proposal whose
+// proportions of one cac sum above 1 in a model with a remainder compartment
+// is drawn again (plom_check_IC_assign_theta_remainder, proposal.c:87-114), at
+// most kMaxIcAttempts times (then ERR_IC).
+constexpr int kMaxIcAttempts = 1000;
+
 template <class T>
 __global__ void k_mif_init(const double* __restrict__ theta_hat, const double* __restrict__ sd_init, int Q,
                            unsigned est_mask, int R, int J, const uint64_t* seed, uint32_t filter_id,
-                           T* __restrict__ theta) {
+                           T* __restrict__ theta, const int* __restrict__ x0_slot, const double* __restrict__ pop0,
+                           const double* __restrict__ x0, const plomrt::BackTransform* __restrict__ theta_bt,
+                           T* __restrict__ X, FilterAcc* acc) {
   const size_t RJ = (size_t)R * J;
   for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < RJ; g += (size_t)gridDim.x * blockDim.x) {
     const int r = (int)(g / J);
     const int j = (int)(g - (size_t)r * J);
     const plomrt::PhiloxKey key = plomrt::make_key(*seed, filter_id + (uint32_t)r);
-    for (int q = 0; q < Q; ++q) {
-      double v = theta_hat[(size_t)r * Q + q];
-      if ((est_mask >> q) & 1u) {
-        T z[1];
-        plomrt::NormalGen<T>::template fill<1>(key, (uint32_t)j, 0u, (uint32_t)q, z, (uint32_t)plomrt::STREAM_INIT);
-        v += sd_init[q] * (double)z[0];
+    double th[kMaxTheta];
+    for (int attempt = 0;; ++attempt) {
+      for (int q = 0; q < Q; ++q) {
+        double v = theta_hat[(size_t)r * Q + q];
+        if ((est_mask >> q) & 1u) {
+          T z[1];
+          plomrt::NormalGen<T>::template fill<1>(key, (uint32_t)j, (uint32_t)attempt, (uint32_t)q, z,
+                                                 (uint32_t)plomrt::STREAM_INIT);
+          v += sd_init[q] * (double)z[0];
+        }
+        th[q] = (double)(T)v;
       }
-      theta[(size_t)q * RJ + g] = (T)v;
+      if (!x0_slot || M::POP_SIZE_EQ_SUM_SV) break;
+      bool ok = true;
+      for (int c = 0; c < M::N_CAC && ok; ++c) {
+        double sum = 0.0;
+        for (int i = 0; i < M::N_PAR_SV; ++i) {
+          const int w = i * M::N_CAC + c;
+          const int q = x0_slot[w];
+          sum += q >= 0 ? plomrt::back_transform<double>(th[q], theta_bt[q]) : x0[w] / pop0[c];
+        }
+        if (sum > 1.0) ok = false;
+      }
+      if (ok) break;
+      if (attempt + 1 >= kMaxIcAttempts) {
+        atomicOr(&acc[r].error, (int)ERR_IC);
+        break;
+      }
     }
+    for (int q = 0; q < Q; ++q) theta[(size_t)q * RJ + g] = (T)th[q];
+    if (x0_slot) {
+      for (int w = 0; w < M::OFF_INC; ++w) {
+        const int q = x0_slot[w];
+        if (q < 0) continue;
+        const double v = (w < M::N_PAR_SV * M::N_CAC)
+                             ? plomrt::back_transform<double>(th[q], theta_bt[q]) * pop0[w % M::N_CAC]
+                             : th[q];
+        X[(size_t)w * RJ + g] = (T)v;
+      }
+    }
+  }
+}
+
+// Fixed-lag means of every run (update_fixed_lag_smoothing,
+// model_builder/C/mif/methods.c:370-392): at interval L the reference sums the
+// resampled components (index j of the new population) times the weights of
+// the interval (index j of the population before resampling), i.e.
+// sum_j theta[q][anc[j]] w[j].  Without a weighted interval up to L the
+// weights are 1/J and the components those of the initial proposal (anc
+// NULL).  Grid (Q, R); components outside fls_mask are skipped.
+template <class T, int BT>
+__global__ void __launch_bounds__(BT) k_mif_fls(const T* __restrict__ lw, const T* __restrict__ theta,
+                                                const uint32_t* __restrict__ anc, int J, int R, double thresh,
+                                                const StepState* st, unsigned fls_mask, int Q, double* out) {
+  const int q = blockIdx.x, r = blockIdx.y;
+  if (!((fls_mask >> q) & 1u)) return;
+  const size_t RJ = (size_t)R * J;
+  const StepState* s = st + r;
+  const bool uni = anc == nullptr || s->all_fail;
+  const double m = uni ? 0.0 : s->m, s1 = uni ? 1.0 : s->s1;
+  double acc = 0.0;
+  for (int j = threadIdx.x; j < J; j += BT) {
+    const size_t gj = (size_t)r * J + j;
+    double w;
+    if (uni) {
+      w = 1.0 / (double)J;
+    } else {
+      const T l = lw[gj];
+      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+    }
+    const size_t src = (size_t)r * J + (anc ? anc[gj] : (uint32_t)j);
+    acc += (double)theta[(size_t)q * RJ + src] * w;
+  }
+  __shared__ double sh[BT / 32];
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < BT / 32; ++w) t += sh[w];
+    out[(size_t)r * Q + q] = t;
   }
 }
 

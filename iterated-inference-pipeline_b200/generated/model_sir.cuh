@@ -100,7 +100,9 @@ struct Model {
   // for generators of more than 2 normals per block (FP32) PLOM_MAX_DRAW_GROUP caps the
   // group, leaving part of the last block of a group unused (SEIR 20x2: 4 cacs = 9 whole
   // blocks measured 10 % faster than 1 cac = 3 blocks with 3 of their 12 normals unused)
+  // without draws (Euler skeleton) a group of 4 cacs only sets the unrolling of the cac loop
   static constexpr PLOM_HD int draw_group(int nw, int per_block) {
+    if (nw == 0) return N_CAC >= 4 ? 4 : 1;
     int g = 1;
     while (nw > 0 && (g * nw) % per_block != 0 && g < per_block) ++g;
     g = (nw > 0 && (g * nw) % per_block == 0 && g <= N_CAC) ? g : 1;

@@ -449,17 +449,23 @@ def mif_main(argv, stdin=None, model_dir='.'):
         return 1
     if args.pipe:
         args.quiet = True
-    if args.ic_only:
-        raise CliError('-f/--ic_only: initial conditions are fitted by fixed-lag smoothing, which this engine '
-                       'does not implement')
     unlink_done(args)
     model, settings, lib = load_model_dir(model_dir)
     theta = read_theta(stdin)
+    # L = floor(lag * N_DATA); with -f the filter stops after interval L
+    # (build_mif, model_builder/C/mif/build.c:27-45)
+    n_data = len(settings['data']['data'])
+    L = int(math.floor(args.lag * n_data))
+    if L > n_data:
+        raise CliError('L > N_DATA (%d > %d). Please choose a L <= %d' % (L, n_data, n_data))
+    if args.ic_only:
+        args.nb_obs = min(L + 1, n_data)
     problem = make_problem(model, settings, theta, args)
     best = Best(model, theta, is_bayesian=args.prior)
     engine = Engine(model_name(lib), lib)
     try:
-        run = Mif(engine, problem, n_runs=1, a=args.cooling, b=args.heat, switch=args.switch)
+        run = Mif(engine, problem, n_runs=1, a=args.cooling, b=args.heat, switch=args.switch, lag=L,
+                  prior=best if args.prior else None)
     except MifError as e:
         raise CliError(str(e))
     log(args, 'Starting plom-mif with the following options: i = %d, J = %d, LIKE_MIN = %s, M = %d, a = %s, b = %s, '
@@ -485,7 +491,7 @@ def mif_main(argv, stdin=None, model_dir='.'):
             t0 = time.time()
             freeze, sd_init, sd_mut, vt_add = run.schedules(m)
             ll, nf, bart, vt = run.plan.iteration(run.theta_hat, sd_init, sd_mut, vt_add, seed + 1000003 * m)
-            run.update(m, bart, vt)
+            run.update(m, bart, vt, run.fixed_lag_means())
             best.mean[slots] = run.theta_hat[0]
             if f_mif is not None:
                 f_mif.writelines(_mif_rows(best, run, problem, m, bart[0], vt[0], slots))

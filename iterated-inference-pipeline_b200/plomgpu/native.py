@@ -59,7 +59,10 @@ class BatchDesc(C.Structure):
 
 class MifDesc(C.Structure):
     _fields_ = [('n_runs', C.c_int), ('n_theta', C.c_int), ('proc_slot', _ip), ('obs_slot', _ip),
-                ('theta_bt', _P(BackTransform)), ('estimated', _ip), ('proc_cac_slot', _ip), ('obs_ts_slot', _ip)]
+                ('theta_bt', _P(BackTransform)), ('estimated', _ip), ('proc_cac_slot', _ip), ('obs_ts_slot', _ip),
+                ('fls', _ip), ('x0_slot', _ip), ('pop0', _dp), ('vol_slot', _ip), ('lag', C.c_int),
+                ('prior', C.c_int), ('prior_kind', _ip), ('prior_lo', _dp), ('prior_hi', _dp),
+                ('prior_finv', _P(BackTransform))]
 
 
 class ServerOpts(C.Structure):
@@ -88,7 +91,8 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
                'plomgpu_server_create', 'plomgpu_server_submit', 'plomgpu_server_poll', 'plomgpu_server_wait',
                'plomgpu_server_get_stats', 'plomgpu_server_destroy', 'plomgpu_particle_values',
-               'plomgpu_plan_sample_traj', 'plomgpu_plan_update_drift', 'plomgpu_debug_draws']
+               'plomgpu_plan_sample_traj', 'plomgpu_plan_update_drift', 'plomgpu_debug_draws',
+               'plomgpu_mif_fls_means']
 
 
 def _ptr(a, t):
@@ -230,6 +234,7 @@ def _declare(lib):
     lib.plomgpu_batch_run.argtypes = [_P(BatchDesc), _dp, _ip]
     lib.plomgpu_mif_create.argtypes = [_P(SmcDesc), _P(MifDesc), _P(C.c_void_p)]
     lib.plomgpu_mif_iteration.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_uint64, _dp, _ip, _dp, _dp]
+    lib.plomgpu_mif_fls_means.argtypes = [C.c_void_p, _dp, _ip]
     lib.plomgpu_mif_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_mif_destroy.restype = None
     lib.plomgpu_server_create.argtypes = [_P(SmcDesc), _P(ServerOpts), _P(C.c_void_p)]
@@ -476,9 +481,11 @@ class Batch(object):
 
 class MifDescHolder(object):
     """plomgpu_mif_desc of n_runs runs over the components ``components``: list of
-    (kind, index, back_transform tuple, estimated[, members]) with kind 'proc' or 'obs';
-    ``members`` lists the populations (process) or series (observation) a
-    component applies to when the parameter is fitted per group (None: all)."""
+    (kind, index, back_transform tuple, estimated[, members]) with kind 'proc' or 'obs'
+    (parameters of the step or the observation model) or 'fls' (initial conditions and
+    drift start values, placed by set_fixed_lag); ``members`` lists the populations
+    (process) or series (observation) a component applies to when the parameter is fitted
+    per group (None: all)."""
 
     def __init__(self, n_runs, components, n_par_proc, n_par_obs, n_cac=1, n_ts=1):
         self.R = int(n_runs)
@@ -492,12 +499,13 @@ class MifDescHolder(object):
         for q, comp in enumerate(components):
             kind, idx, bt, est = comp[:4]
             members = comp[4] if len(comp) > 4 else None
-            slots, table = (self.proc_slot, self.proc_cac) if kind == 'proc' else (self.obs_slot, self.obs_ts)
-            if members is None:
-                slots[idx] = q
-            else:
-                slots[idx] = -2
-                table[idx, list(members)] = q
+            if kind in ('proc', 'obs'):
+                slots, table = (self.proc_slot, self.proc_cac) if kind == 'proc' else (self.obs_slot, self.obs_ts)
+                if members is None:
+                    slots[idx] = q
+                else:
+                    slots[idx] = -2
+                    table[idx, list(members)] = q
             f, s_, dur, a_, b_, mult = bt
             self.bts[q] = BackTransform(int(f), int(s_), int(dur), 0, float(a_), float(b_), float(mult))
             self.estimated[q] = 1 if est else 0
@@ -507,6 +515,39 @@ class MifDescHolder(object):
                             C.cast(self.bts, _P(BackTransform)), _ptr(self.estimated, _ip),
                             _ptr(self.proc_cac, _ip) if multi_p else None,
                             _ptr(self.obs_ts, _ip) if multi_o else None)
+
+    def set_fixed_lag(self, fls, x0_slot, pop0, lag):
+        """Components fitted by fixed-lag smoothing (fls[q]), the component of every initial state word
+        (x0_slot[off_inc], -1: x0), N at t = 0 and the lag L."""
+        self.fls = np.ascontiguousarray(fls, dtype=np.int32)
+        self.x0_slot = np.ascontiguousarray(x0_slot, dtype=np.int32)
+        self.pop0 = np.ascontiguousarray(pop0, dtype=np.float64)
+        self.desc.fls = _ptr(self.fls, _ip)
+        self.desc.x0_slot = _ptr(self.x0_slot, _ip) if np.any(self.x0_slot >= 0) else None
+        self.desc.pop0 = _ptr(self.pop0, _dp)
+        self.desc.lag = int(lag)
+
+    def set_vol_slot(self, vol_slot):
+        """[n_drift][n_cac] component of every drift volatility (-1: the problem's table)."""
+        self.vol_slot = np.ascontiguousarray(vol_slot, dtype=np.int32)
+        self.desc.vol_slot = _ptr(self.vol_slot, _ip) if np.any(self.vol_slot >= 0) else None
+
+    def set_prior(self, kinds, lo, hi, finv, lag):
+        """The --prior patch: per component prior kind (0 flat, 1 normal, 2 pseudo-uniform), bounds and the
+        back-transform to the prior's scale (tuples as theta_bt)."""
+        self.prior_kind = np.ascontiguousarray(kinds, dtype=np.int32)
+        self.prior_lo = np.ascontiguousarray(lo, dtype=np.float64)
+        self.prior_hi = np.ascontiguousarray(hi, dtype=np.float64)
+        self.prior_finv = (BackTransform * max(self.Q, 1))()
+        for q, bt in enumerate(finv):
+            f, s_, dur, a_, b_, mult = bt
+            self.prior_finv[q] = BackTransform(int(f), int(s_), int(dur), 0, float(a_), float(b_), float(mult))
+        self.desc.prior = 1
+        self.desc.prior_kind = _ptr(self.prior_kind, _ip)
+        self.desc.prior_lo = _ptr(self.prior_lo, _dp)
+        self.desc.prior_hi = _ptr(self.prior_hi, _dp)
+        self.desc.prior_finv = C.cast(self.prior_finv, _P(BackTransform))
+        self.desc.lag = int(lag)
 
 
 class MifPlan(object):
@@ -531,6 +572,14 @@ class MifPlan(object):
         check(self.lib, self.lib.plomgpu_mif_iteration(self.p, *(x.ctypes.data_as(_dp) for x in a), C.c_uint64(seed),
                                                        _ptr(ll, _dp), _ptr(nf, _ip), _ptr(bart, _dp), _ptr(vt, _dp)))
         return ll, nf, bart, vt
+
+    def fls_means(self):
+        """([n_runs][n_theta] fixed-lag means of the last iteration (NaN outside the fixed-lag
+        components), whether interval L was reached)."""
+        out = np.zeros((self.m.R, self.m.Q))
+        upd = C.c_int()
+        check(self.lib, self.lib.plomgpu_mif_fls_means(self.p, _ptr(out, _dp), C.byref(upd)))
+        return out, bool(upd.value)
 
     def close(self):
         if self.p:

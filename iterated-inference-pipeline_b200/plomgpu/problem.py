@@ -205,28 +205,34 @@ class Problem(object):
         self.x0 = self.params.x0(self.pop_size_t0)
         (self.drift_group, self.drift_ngroups, self.drift_bt, self.drift_vol, _) = self.params.drift_tables()
 
-    def interval_problem(self, n, x0_particles=None):
-        """The one-interval filter of observation interval n: its substeps, covariates and data row,
-        started from the particles x0_particles ([off_inc][J], FP64) when given."""
+    def segment_problem(self, n0, n1, x0_particles=None):
+        """The filter of observation intervals n0 .. n1 - 1: their substeps, covariates and data
+        rows, started from the particles x0_particles ([off_inc][J], FP64) when given."""
         import copy
-        if not 0 <= n < self.n_obs:
-            raise ValueError('interval %d outside [0, %d)' % (n, self.n_obs))
+        if not 0 <= n0 < n1 <= self.n_obs:
+            raise ValueError('intervals [%d, %d) outside [0, %d)' % (n0, n1, self.n_obs))
         q = copy.copy(self)
-        sub0 = int(np.sum(self.n_sub[:n]))
-        k = int(self.n_sub[n])
-        q.n_obs = 1
-        q.n_sub = self.n_sub[n:n + 1].copy()
-        q.t_sub = self.t_sub[sub0:sub0 + k].copy()
-        q.t_obs = self.t_obs[n:n + 1].copy()
-        q.data = self.data[n:n + 1].copy()
-        q.cov_cac = self.cov_cac[sub0:sub0 + k].copy()
-        q.cov_ts = self.cov_ts[n:n + 1].copy()
-        if n > 0:
-            q.cov_ts0 = self.cov_ts[n - 1].copy()
+        s0 = int(np.sum(self.n_sub[:n0]))
+        s1 = int(np.sum(self.n_sub[:n1]))
+        q.n_obs = n1 - n0
+        q.n_sub = self.n_sub[n0:n1].copy()
+        q.t_sub = self.t_sub[s0:s1].copy()
+        q.t_obs = self.t_obs[n0:n1].copy()
+        q.data = self.data[n0:n1].copy()
+        q.cov_cac = self.cov_cac[s0:s1].copy()
+        q.cov_ts = self.cov_ts[n0:n1].copy()
+        if n0 > 0:
+            q.cov_ts0 = self.cov_ts[n0 - 1].copy()
         if self.pop_size is not None:
-            q.pop_size = self.pop_size[n:n + 2].copy()
+            q.pop_size = self.pop_size[n0:n1 + 1].copy()
         q.x0_particles = None if x0_particles is None else np.ascontiguousarray(x0_particles, dtype=float)
         return q
+
+    def interval_problem(self, n, x0_particles=None):
+        """The one-interval filter of observation interval n (segment n .. n)."""
+        if not 0 <= n < self.n_obs:
+            raise ValueError('interval %d outside [0, %d)' % (n, self.n_obs))
+        return self.segment_problem(n, n + 1, x0_particles)
 
     @property
     def particle_steps(self):

@@ -44,7 +44,7 @@ class Oracle(object):
         L.oracle_weight_and_resample.argtypes = [_dp, C.c_int, C.c_double, C.c_double, _dp, _dp,
                                                  C.POINTER(C.c_uint32)]
         L.oracle_mif_iteration.argtypes = [C.POINTER(native.SmcDesc), C.POINTER(native.MifDesc), _dp, _dp, _dp, _dp,
-                                           _dp, C.POINTER(C.c_int), _dp, _dp]
+                                           _dp, C.POINTER(C.c_int), _dp, _dp, _dp]
         L.oracle_psr_samples.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, _dp]
         L.oracle_psr_samples.restype = None
         L.oracle_psr_samples_f.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, _dp]
@@ -90,10 +90,15 @@ class Oracle(object):
         nf = np.zeros(R, dtype=np.int32)
         bart = np.zeros((R, T, Q))
         vt = np.zeros((R, T, Q))
+        fls = np.full((R, Q), np.nan)
         a = [np.ascontiguousarray(x, dtype=np.float64) for x in (theta_hat, sd_init, sd_mut, vt_add)]
-        self.lib.oracle_mif_iteration(C.byref(h.desc), C.byref(mif_desc_holder.desc), *(x.ctypes.data_as(_dp) for x in a),
-                                      ll.ctypes.data_as(_dp), nf.ctypes.data_as(C.POINTER(C.c_int)),
-                                      bart.ctypes.data_as(_dp), vt.ctypes.data_as(_dp))
+        rc = self.lib.oracle_mif_iteration(C.byref(h.desc), C.byref(mif_desc_holder.desc),
+                                           *(x.ctypes.data_as(_dp) for x in a),
+                                           ll.ctypes.data_as(_dp), nf.ctypes.data_as(C.POINTER(C.c_int)),
+                                           bart.ctypes.data_as(_dp), vt.ctypes.data_as(_dp), fls.ctypes.data_as(_dp))
+        if rc:
+            raise RuntimeError('oracle mif iteration failed: %d' % rc)
+        self.last_fls_means = fls
         return ll, nf, bart, vt
 
     def systematic_points(self, U, J, table=False):

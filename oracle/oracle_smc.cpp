@@ -604,10 +604,15 @@ struct HostMifEnv : HostEnv {
   unsigned uni;
   const int* slot;
   const int* cslot;
+  const int* vslot;  // [N_DRIFT][N_CAC] volatility components, NULL: table
   const double* nat;
   double par(int p, int cac) const {
     if (!((uni >> p) & 1u)) return par_[p * M::N_CAC + cac];
     return slot[p] == -2 ? nat[cslot[p * M::N_CAC + cac]] : parp[p];
+  }
+  double drift_vol(int i, int g) const {
+    if (vslot && vslot[i * M::N_CAC + g] >= 0) return nat[vslot[i * M::N_CAC + g]];
+    return dvol_[i * M::N_CAC + g];
   }
 };
 
@@ -646,7 +651,7 @@ extern "C" {
 
 int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, const double* theta_hat,
                          const double* sd_init, const double* sd_mut, const double* vt_add, double* loglik,
-                         int* n_all_fail_out, double* bart, double* vt) {
+                         int* n_all_fail_out, double* bart, double* vt, double* fls_out) {
   const int J = d->J, S = M::S, Q = mf->n_theta, R = mf->n_runs;
   const int v = d->noises_off & 3;
   const bool drift = M::N_DRIFT > 0 && !(d->noises_off & PLOMGPU_NO_DRIFT);
@@ -658,18 +663,55 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
     const plomrt::PhiloxKey key = plomrt::make_key(d->seed, (uint32_t)r);
     std::vector<double> X((size_t)J * S), Xn((size_t)J * S), th((size_t)J * Q), thn((size_t)J * Q), w(J);
     std::vector<uint32_t> select(J);
+    // weights before the first weighted interval (read by the fixed-lag means only)
+    for (int j = 0; j < J; ++j) w[j] = 1.0 / (double)J;
     for (int j = 0; j < J; ++j) {
       for (int s = 0; s < S; ++s) X[(size_t)j * S + s] = (s < M::OFF_INC) ? d->x0[s] : 0.0;
-      for (int q = 0; q < Q; ++q) {
-        double t = theta_hat[(size_t)r * Q + q];
-        if (mf->estimated[q]) {
-          double z[1];
-          plomrt::NormalGen<double>::fill<1>(key, (uint32_t)j, 0u, (uint32_t)q, z, (uint32_t)plomrt::STREAM_INIT);
-          t += sd_init[q] * z[0];
+      // propose_safe_theta_and_load_X0 (C/core/proposal.c:40-62): propose until the
+      // initial proportions of every cac sum to at most 1 (models with a remainder)
+      for (int attempt = 0;; ++attempt) {
+        for (int q = 0; q < Q; ++q) {
+          double t = theta_hat[(size_t)r * Q + q];
+          if (mf->estimated[q]) {
+            double z[1];
+            plomrt::NormalGen<double>::fill<1>(key, (uint32_t)j, (uint32_t)attempt, (uint32_t)q, z,
+                                               (uint32_t)plomrt::STREAM_INIT);
+            t += sd_init[q] * z[0];
+          }
+          th[(size_t)j * Q + q] = t;
         }
-        th[(size_t)j * Q + q] = t;
+        if (!mf->x0_slot || M::POP_SIZE_EQ_SUM_SV) break;
+        bool ok = true;
+        for (int c = 0; c < M::N_CAC && ok; ++c) {
+          double sum = 0.0;
+          for (int i = 0; i < M::N_PAR_SV; ++i) {
+            const int wd = i * M::N_CAC + c, q = mf->x0_slot[wd];
+            plomrt::BackTransform bt;
+            if (q >= 0) memcpy(&bt, &mf->theta_bt[q], sizeof(bt));
+            sum += q >= 0 ? plomrt::back_transform<double>(th[(size_t)j * Q + q], bt) : d->x0[wd] / mf->pop0[c];
+          }
+          if (sum > 1.0) ok = false;
+        }
+        if (ok) break;
+        if (attempt + 1 >= 1000) return 8;
+      }
+      if (mf->x0_slot) {
+        for (int wd = 0; wd < M::OFF_INC; ++wd) {
+          const int q = mf->x0_slot[wd];
+          if (q < 0) continue;
+          const double t = th[(size_t)j * Q + q];
+          if (wd < M::N_PAR_SV * M::N_CAC) {
+            plomrt::BackTransform bt;
+            memcpy(&bt, &mf->theta_bt[q], sizeof(bt));
+            X[(size_t)j * S + wd] = plomrt::back_transform<double>(t, bt) * mf->pop0[wd % M::N_CAC];
+          } else {
+            X[(size_t)j * S + wd] = t;
+          }
+        }
       }
     }
+    const bool is_fls_q = mf->fls != nullptr;
+    auto fls_of = [&](int q) { return is_fls_q && mf->fls[q] != 0; };
     double Llike = 0.0;
     int n_all_fail = 0;
     int sub0 = 0;
@@ -700,6 +742,7 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
         }
         e.slot = mf->proc_slot;
         e.cslot = mf->proc_cac_slot;
+        e.vslot = mf->vol_slot;
         e.nat = nat;
         oe.slot = mf->obs_slot;
         oe.tslot = mf->obs_ts_slot;
@@ -729,7 +772,22 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
             const double var = M::obs_var(obs[ts], ts, d->t_obs[n], oe);
             ll += plomrt::log_like_term(y[ts], mu, var, d->like_min, &fl);
           }
-          w[j] = exp(plomrt::finish_loglik(ll, fl, M::N_TS));
+          // patch_likelihood_prior (C/mif/methods.c:469-520), in log space
+          double lpr = 0.0;
+          if (mf->prior) {
+            for (int q = 0; q < Q; ++q) {
+              if (!mf->estimated[q]) continue;
+              const bool f = fls_of(q);
+              if (f && !(n < mf->lag)) continue;
+              plomrt::BackTransform fb;
+              memcpy(&fb, &mf->prior_finv[q], sizeof(fb));
+              const double xn = plomrt::back_transform<double>(th[(size_t)j * Q + q], fb);
+              const double pr = plomrt::prior_density(mf->prior_kind[q], xn, mf->prior_lo[q], mf->prior_hi[q]);
+              lpr += plomrt::log_sanitized(pr, d->like_min) *
+                     (f ? 1.0 / (double)mf->lag : 1.0 / (double)d->n_obs);
+            }
+          }
+          w[j] = exp(plomrt::finish_loglik(ll, fl, M::N_TS) + lpr);
         }
       }
       sub0 += d->n_sub[n];
@@ -763,7 +821,7 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
           for (int k = 0; k < S; ++k) X[(size_t)j * S + k] = Xn[s * S + k];
           for (int q = 0; q < Q; ++q) {
             double t = th[s * Q + q];
-            if (mf->estimated[q]) {
+            if (mf->estimated[q] && !fls_of(q)) {
               double z[1];
               plomrt::NormalGen<double>::fill<1>(key, (uint32_t)j, (uint32_t)(n + 1), (uint32_t)q, z,
                                                  (uint32_t)plomrt::STREAM_MUTATE);
@@ -775,6 +833,16 @@ int oracle_mif_iteration(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mf, 
         th.swap(thn);
       } else {
         X.swap(Xn);
+      }
+      // update_fixed_lag_smoothing at n == L (C/mif/mif.c:196-198, methods.c:370-392):
+      // resampled components times the weights of the last weighting
+      if (n == mf->lag && fls_out) {
+        for (int q = 0; q < Q; ++q) {
+          if (!fls_of(q)) continue;
+          double acc = 0.0;
+          for (int j = 0; j < J; ++j) acc += th[(size_t)j * Q + q] * w[j];
+          fls_out[(size_t)r * Q + q] = acc;
+        }
       }
     }
     loglik[r] = Llike;

@@ -210,3 +210,29 @@ def test_model_directory_and_cli_reach_the_engine(tmp_path, capsys):
         os.chdir(cwd)
     assert rc == 1
     assert 'no CUDA device' in capsys.readouterr().err
+
+
+def test_mif_components_fixed_lag_tables():
+    """Initial conditions and drift start values become fixed-lag components placed on their
+    state words; a drifted parameter is not a random-walk component; volatilities map to the
+    drift groups."""
+    import numpy as np
+    import models
+    from plomgpu import mif
+    p = models.make_problem('drift', J=8, dt=1.0)
+    m = p.model
+    comp = mif.components(p, names=['S', 'I', 'r0', 'vol'])
+    kinds = sorted(set((c['name'], c['kind']) for c in comp))
+    assert kinds == [('I', 'sv'), ('S', 'sv'), ('r0', 'drift'), ('vol', 'proc')]
+    slots = mif.x0_slots(m, comp)
+    assert len(slots) == len(m.par_sv) * m.N_CAC + len(m.drift_par_proc) * m.N_CAC
+    for q, c in enumerate(comp):
+        if c['kind'] == 'sv':
+            for cac in c['members']:
+                assert slots[m.par_sv.index(c['name']) * m.N_CAC + cac] == q
+        if c['kind'] == 'drift':
+            assert slots[len(m.par_sv) * m.N_CAC + c['g']] == q
+    assert np.all(slots >= 0)
+    vol = mif.vol_slots(p, comp)
+    qv = [q for q, c in enumerate(comp) if c['name'] == 'vol']
+    assert set(vol[0][:p.params.routers['r0'].n_gp].tolist()) <= set(qv)

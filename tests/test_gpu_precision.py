@@ -15,9 +15,11 @@ Philox parity tests).
   the whole filter (the conditional measurement below rests on it);
 * conditional per-interval error on the SEIR 20x2 model (the model of the
   J = 1e5, T = 520 benchmark): the same FP64 particle cloud advanced over
-  one interval in FP32 and in FP64, many intervals and seeds;
-* whole filters: paired FP32 - FP64 log-likelihood over seeds, SEIR 20x2 at
-  J = 20000, T = 60 and the SIR model of the batched workload.
+  one interval in FP32 and in FP64, at every interval of an FP64 filter path
+  (plomgpu.precision);
+* whole filters: paired FP32 - FP64 log-likelihood over seeds on the SIR
+  model of the batched workload (on SEIR 20x2 whole filters diverge: the
+  estimator's own spread, see plomgpu.precision).
 """
 
 import copy
@@ -27,6 +29,7 @@ import numpy as np
 import pytest
 
 import models
+from plomgpu import precision
 
 pytestmark = pytest.mark.gpu
 
@@ -75,52 +78,17 @@ def test_interval_from_cloud_equals_interval_in_filter():
         np.testing.assert_array_equal(o.ancestors[0], full.ancestors[n])
 
 
-def conditional_interval_errors(eng, prob, intervals, seed0=100):
-    """FP32 - FP64 llike of one interval advanced from the same FP64 cloud with paired draws."""
-    off_inc = eng.info.off_inc
-    d = []
-    for k, n in enumerate(intervals):
-        if n > 0:
-            before = eng.smc(_with(prob, seed=seed0 + k, n_obs=n), precision=64, x_final=True)
-            cloud = before.x_final[:off_inc]
-        else:
-            cloud = np.repeat(prob.x0[:off_inc, None], prob.J, axis=1)
-        q = _with(prob.interval_problem(n, cloud), seed=seed0 + 1000 + k, paired_draws=True)
-        l32 = eng.smc(q, precision=32).llike_n[0]
-        l64 = eng.smc(q, precision=64).llike_n[0]
-        d.append(l32 - l64)
-    return np.array(d)
-
-
 def test_conditional_interval_error_seir20x2():
-    """Per-interval precision error on the benchmark's model, well below the
-    0.5-nat budget of a whole filter: |bias| and its standard error under
-    0.01 nats per interval."""
-    eng = models.engine('seir20x2')
-    p = models.make_problem('seir20x2', J=20000, dt=1.0, precision=32, seed=1, nb_obs=64)
-    d = conditional_interval_errors(eng, p, list(range(0, 64, 2)))
-    se = d.std(ddof=1) / math.sqrt(len(d))
-    assert se < 0.01, (d.mean(), se)
-    assert abs(d.mean()) < 0.01, (d.mean(), se, d)
-
-
-def paired_filter_errors(eng, prob, seeds):
-    out = []
-    for s in seeds:
-        q = _with(prob, seed=s, paired_draws=True)
-        out.append(eng.smc(q, precision=32).loglik - eng.smc(q, precision=64).loglik)
-    return np.array(out)
-
-
-def test_paired_filter_error_seir20x2():
-    """Whole SEIR 20x2 filters (J = 20000, T = 60): the FP32 - FP64
-    log-likelihood over 12 seeds has a bias within 0.5 nats."""
+    """Per-interval precision error on the benchmark's model (SEIR 20x2, J = 20000), every interval
+    of a 60-interval FP64 filter path: bias and standard error below 0.005 nats per interval, and
+    the whole-filter bias they imply within the 0.5-nat budget."""
     eng = models.engine('seir20x2')
     p = models.make_problem('seir20x2', J=20000, dt=1.0, precision=32, seed=1, nb_obs=60)
-    d = paired_filter_errors(eng, p, range(500, 512))
-    se = d.std(ddof=1) / math.sqrt(len(d))
-    assert abs(d.mean()) < 0.5, (d.mean(), se, d)
-    assert se < 0.5, (d.mean(), se, d)
+    n, d = precision.conditional_interval_errors(eng, p, stride=1, seed=100)
+    st = precision.summary(p, n, d)
+    assert st['per_interval_se'] < 0.005, st
+    assert abs(st['per_interval_mean']) < 0.005, st
+    assert abs(st['implied_filter_bias']) < 0.5, st
 
 
 def test_paired_filter_error_sir():
@@ -128,7 +96,7 @@ def test_paired_filter_error_sir():
     bias within 0.5 nats."""
     eng = models.engine('sir')
     p = models.make_problem('sir', J=1000, dt=1.0, precision=32, seed=1)
-    d = paired_filter_errors(eng, p, range(64))
+    d = precision.paired_filter_errors(eng, p, range(64))
     se = d.std(ddof=1) / math.sqrt(len(d))
     assert abs(d.mean()) < 0.5, (d.mean(), se)
     assert se < 0.5, (d.mean(), se)
