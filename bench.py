@@ -64,8 +64,8 @@ def parse():
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
     ap.add_argument('--error-samples', type=int, default=26,
                     help='intervals sampled for loglik_error (0: skip)')
-    ap.add_argument('--plan-pool', type=int, default=4, help='serve: concurrent plans of the shared-memory model '
-                    '(the SEIR 20x2 requests took 29.3 / 24.9 / 24.5 s with 2 / 3 / 4)')
+    ap.add_argument('--plan-pool', type=int, default=0, help='serve: run the shared-memory model on a pool of this '
+                    'many concurrent plans instead of the tiled device loop (0: device loop)')
     return ap.parse_args()
 
 
@@ -404,7 +404,7 @@ def run_serve(args, window_s=0.25, rate=2000.0):
     for c in classes.values():
         c['eng'] = Engine(c['lib'])
         c['server'] = Server(c['eng'], c['prob'], max_J=c['J'], memory_budget=150e9 / 2, plan_pool=args.plan_pool,
-                             precision=32)
+                             precision=32, use_plan_pool=args.plan_pool > 0)
     rng = np.random.Generator(np.random.Philox(12))
     chains = []
     for i in range(32):

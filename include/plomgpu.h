@@ -361,12 +361,14 @@ int plomgpu_batch_run(const plomgpu_batch_desc *desc, double *loglik, int *n_all
  * Likelihood server for concurrent callers (pmcmc chains, C/pmcmc/pmcmc.c:
  * 186-266): requests (parameters, initial state, seed, J) on one data set
  * are queued, admitted while their HBM footprint fits the memory budget,
- * and run concurrently.  Models whose particle fits registers run on a
- * device-resident loop (a persistent kernel taking requests from a ring in
- * mapped host memory, one CTA per request, continuous batching); larger
- * models run on a pool of captured plans, one stream each.  A result does
- * not depend on what else runs: each request is computed by the same
- * deterministic kernels alone or in the mix.  Thread-safe. */
+ * and run concurrently on a device-resident loop: a persistent kernel takes
+ * requests from a ring in mapped host memory (continuous batching).  Models
+ * whose particle fits registers run one CTA per request; larger models
+ * (shared-memory particles) split every request into tiles of particles,
+ * one tile of one interval being the unit of work, so that tiles of
+ * different requests share the SMs.  A result does not depend on what else
+ * runs: each request is computed by the same deterministic arithmetic alone
+ * or in the mix.  Thread-safe. */
 typedef struct plomgpu_server_opts {
     int max_J;              /* largest particle count of a request */
     double memory_budget;   /* bytes of HBM the requests may hold (0: 150e9) */
@@ -375,6 +377,8 @@ typedef struct plomgpu_server_opts {
                              * 2e4 particles fills half of a B200's resident slots: 2 / 3 / 4 plans run
                              * 1.6 / 2.0 / 2.1x the filters per second of one) */
     int precision;          /* 32 or 64 */
+    int use_plan_pool;      /* 1: models with shared-memory particles run on the plan pool instead of the
+                             * device loop (one captured whole filter per request, for comparison) */
 } plomgpu_server_opts;
 
 typedef struct plomgpu_server_stats {

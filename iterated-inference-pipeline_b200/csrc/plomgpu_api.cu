@@ -60,9 +60,12 @@ constexpr int kIptScan = 8;
 constexpr int kTile = kBtScan * kIptScan;
 constexpr int kBtSearch = 256;
 constexpr int kMaxWeightBlocks = 592;
-// tiles of the filters' weighting / resampling (k_weight_tiles, k_resample)
-constexpr int kBtRes = 256;
-constexpr int kIptRes = 4;
+// tiles of the filters' weighting / resampling (k_weight_tiles, k_resample):
+// the propagate block's particles for shared-memory models (the tiles of the
+// serving loop, so that a served request and the plain filter reduce in the
+// same order), 1024 particles otherwise
+constexpr int kBtRes = kSmem ? kBtProp : 256;
+constexpr int kIptRes = kSmem ? 1 : 4;
 constexpr int kTileRes = kBtRes * kIptRes;
 
 int variant_of(int noises_off) { return noises_off & 3; }
@@ -411,6 +414,7 @@ int enqueue_filter(plomgpu_plan* p) {
     a.theta_next = p->mif ? p->theta[th_cur ^ 1] : nullptr;
     // the random walk applies where the previous interval resampled (C/mif/mif.c:190-191)
     a.sd_mut = (p->mif && n > 0 && p->weigh[n - 1]) ? p->sd_mut + (size_t)(n - 1) * p->Q : nullptr;
+    a.x0_rep = nullptr;
     crn_off += RJ * p->n_sub[n] * D;
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
     if (p->ode) {
@@ -1785,9 +1789,21 @@ int server_build(plomgpu_server* sv, int dev) {
   sv->pool.init(pool);
   int sms = 0, per_sm = 0;
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  ServeKernel<T> k = pick_serve<T>(d.noises_off);
-  if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, sv->bt, 0));
+  if (sv->tiled) {
+    ServeTilesKernel<T> k = pick_serve_tiles<T>(d.noises_off);
+    if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
+    sv->bt = kBtProp;
+    sv->tiles_smem = serve_tiles_smem<T, kBtProp>();
+    if (sv->tiles_smem > 48 * 1024)
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sv->tiles_smem));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, sv->bt, sv->tiles_smem));
+    CK(cudaMalloc((void**)&sv->d_live, (size_t)kServeLive * sizeof(long long)));
+    CK(cudaMemsetAsync(sv->d_live, 0xff, (size_t)kServeLive * sizeof(long long), s));  // -1: free
+  } else {
+    ServeKernel<T> k = pick_serve<T>(d.noises_off);
+    if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, sv->bt, 0));
+  }
   sv->grid = sms * std::max(per_sm, 1);
   CK(cudaStreamSynchronize(s));
   return PLOMGPU_OK;
@@ -1811,7 +1827,7 @@ void server_free(plomgpu_server* sv) {
   }
   void* bufs[] = {sv->d_n_sub, sv->d_sub0, sv->d_t_sub, sv->d_t_obs, sv->d_cov_ts, sv->d_data, sv->d_cov_cac,
                   sv->d_coupling, sv->d_drift_vol, sv->d_drift_group, sv->d_drift_ngroups, sv->d_drift_bt,
-                  sv->d_error, sv->d_head, sv->d_pool};
+                  sv->d_error, sv->d_head, sv->d_pool, sv->d_live};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (sv->slots_h) cudaFreeHost(sv->slots_h);
@@ -1852,6 +1868,10 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->max_J = o->max_J;
   sv->ring = o->ring_slots > 0 ? o->ring_slots : 1024;
   sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 4;
+  if (kSmem && o->use_plan_pool) {
+    sv->persistent = false;
+    sv->tiled = false;
+  }
   sv->budget = o->memory_budget > 0 ? (size_t)o->memory_budget : (size_t)150e9;
   // keep host copies of the shared problem
   const int n = d->n_obs;

@@ -1,7 +1,8 @@
 // Host side of the likelihood server (plomgpu_server_*): request queue,
-// admission by HBM footprint, the persistent device loop (smc_serve.cuh) for
-// models whose particle fits registers, and a pool of captured plans (one
-// stream each) for the others.  Included by plomgpu_api.cu.
+// admission by HBM footprint, the persistent device loops (smc_serve.cuh):
+// one CTA per request for models whose particle fits registers, tiles of
+// particles for the others; a pool of captured plans (one stream each)
+// remains as an option.  Included by plomgpu_api.cu.
 #pragma once
 
 #include <atomic>
@@ -92,7 +93,10 @@ struct plomgpu_server {
   // configuration
   int precision = 32, max_J = 0, ring = 1024, plan_pool = 4;
   size_t budget = 0;
-  bool persistent = !kSmem;
+  bool persistent = true;
+  bool tiled = kSmem;           // the tiled loop (shared-memory particles)
+  size_t tiles_smem = 0;        // its dynamic shared memory
+  long long* d_live = nullptr;  // its live-request table [kServeLive]
   int bt = 256, grid = 0;
   long long idle_limit = 20000;
   // base problem (host copies; every request shares it)
@@ -210,12 +214,48 @@ ServeKernel<T> pick_serve(int noises_off) {
 }
 
 template <class T>
+using ServeTilesKernel = void (*)(const BatchArgs<T>, ServeSlot*, const int*, int, ServeCtl*, unsigned long long*,
+                                  unsigned char*, long long*, long long);
+
+template <class T>
+ServeTilesKernel<T> pick_serve_tiles(int noises_off) {
+  if constexpr (kSmem) {
+    const int v = variant_of(noises_off);
+    if (drift_on(noises_off)) {
+      if constexpr (M::N_DRIFT > 0) {
+        switch (v) {
+          case 0: return &k_serve_tiles<T, 0, true, kBtProp>;
+          case 1: return &k_serve_tiles<T, 1, true, kBtProp>;
+          case 2: return &k_serve_tiles<T, 2, true, kBtProp>;
+          default: return &k_serve_tiles<T, 3, true, kBtProp>;
+        }
+      }
+      return nullptr;
+    }
+    switch (v) {
+      case 0: return &k_serve_tiles<T, 0, false, kBtProp>;
+      case 1: return &k_serve_tiles<T, 1, false, kBtProp>;
+      case 2: return &k_serve_tiles<T, 2, false, kBtProp>;
+      default: return &k_serve_tiles<T, 3, false, kBtProp>;
+    }
+  }
+  return nullptr;
+}
+
+template <class T>
 int serve_launch(plomgpu_server* sv, int inst, int grid) {
-  ServeKernel<T> k = pick_serve<T>(sv->base.noises_off);
-  if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
   cudaStream_t st = sv->loop_stream[inst];
-  k<<<grid, sv->bt, 0, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d, sv->d_head, sv->d_pool,
-                             sv->idle_limit);
+  if (sv->tiled) {
+    ServeTilesKernel<T> k = pick_serve_tiles<T>(sv->base.noises_off);
+    if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
+    k<<<grid, sv->bt, sv->tiles_smem, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d,
+                                            sv->d_head, sv->d_pool, sv->d_live, sv->idle_limit);
+  } else {
+    ServeKernel<T> k = pick_serve<T>(sv->base.noises_off);
+    if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
+    k<<<grid, sv->bt, 0, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d, sv->d_head,
+                               sv->d_pool, sv->idle_limit);
+  }
   CK(cudaGetLastError());
   CK(cudaEventRecord(sv->loop_ev[inst], st));
   sv->loop_live[inst] = true;
@@ -226,7 +266,9 @@ int serve_launch(plomgpu_server* sv, int inst, int grid) {
 }
 
 size_t serve_ws_bytes(plomgpu_server* sv, int J) {
-  const size_t b = (sv->precision == 64) ? batch_ws_bytes<double>(J) : batch_ws_bytes<float>(J);
+  size_t b;
+  if (sv->tiled) b = (sv->precision == 64) ? tile_req_bytes<double, kBtProp>(J) : tile_req_bytes<float, kBtProp>(J);
+  else b = (sv->precision == 64) ? batch_ws_bytes<double>(J) : batch_ws_bytes<float>(J);
   return (b + 255) & ~(size_t)255;
 }
 
@@ -253,7 +295,8 @@ void serve_pass(plomgpu_server* sv) {
     for (int i = 0; i < sv->ring; ++i) {
       if (sv->slot_ticket[i] < 0) continue;
       if (__atomic_load_n(&sv->slots_h[i].done, __ATOMIC_ACQUIRE)) {
-        record_result(sv, sv->slot_ticket[i], PLOMGPU_OK, sv->slots_h[i].loglik, sv->slots_h[i].n_all_fail,
+        const int status = sv->slots_h[i].status ? PLOMGPU_ETIMEOUT : PLOMGPU_OK;
+        record_result(sv, sv->slot_ticket[i], status, sv->slots_h[i].loglik, sv->slots_h[i].n_all_fail,
                       sv->slot_t[i]);
         sv->pool.release(sv->slot_off[i], sv->slot_bytes[i]);
         sv->slot_ticket[i] = -1;
@@ -288,6 +331,7 @@ void serve_pass(plomgpu_server* sv) {
       sl.n_obs = sv->base.n_obs;
       sl.seed = rq.seed;
       sl.ws_offset = off;
+      sl.status = 0;
       memcpy(sl.par_cac, rq.par_cac.data(), sizeof(double) * rq.par_cac.size());
       memcpy(sl.par_ts, rq.par_ts.data(), sizeof(double) * rq.par_ts.size());
       memcpy(sl.x0, rq.x0.data(), sizeof(double) * rq.x0.size());
@@ -372,7 +416,14 @@ void serve_pass(plomgpu_server* sv) {
     sv->kernel_live = live_ctas > 0;
     long long waiting = 0;
     for (int i = 0; i < sv->ring; ++i) waiting += sv->slot_ticket[i] >= 0;
-    if (waiting > live_ctas && live_ctas < sv->grid) {
+    if (sv->tiled) {
+      // one instance holding every resident CTA slot: the tiles of all live
+      // requests share it; restarted when it has run out of work and more came
+      if (waiting > 0 && live_ctas == 0) {
+        const int rc = (sv->precision == 64) ? serve_launch<double>(sv, 0, sv->grid) : serve_launch<float>(sv, 0, sv->grid);
+        if (rc) sv->last_error = g_err;
+      }
+    } else if (waiting > live_ctas && live_ctas < sv->grid) {
       for (int i = 0; i < plomgpu_server::kLoops; ++i) {
         if (sv->loop_live[i]) continue;
         const long long want = std::max<long long>(std::max<long long>(waiting - live_ctas, (live_ctas + 1) / 2), 8);

@@ -259,6 +259,7 @@ struct StepArgs {
   const void* theta_prev; // [Q][R*J] (T) per-particle transformed parameters, MIF only
   void* theta_next;       // [Q][R*J] (T)
   const double* sd_mut;   // [Q] random-walk sd applied when gathering from ancestors, NULL: none
+  const double* x0_rep;   // [S] initial particle read by every particle instead of X_prev, NULL: X_prev
 };
 
 // environments with per-particle parameters (iterated filtering)
@@ -333,21 +334,33 @@ constexpr size_t propagate_smem_bytes() {
 // PSR: the Poisson-system step (M::step_psr, the reference's default "psr"
 // implementation) instead of Euler-Maruyama; bit 1 of V turns its white
 // noise off.
-template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false>
-__global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// The propagate block's shared tables: the coupling matrix (when
+// `coupling`) and the per-cac parameters, read by every thread at the same
+// address.  Ends with a block barrier.
+template <class T, int BT>
+__device__ __forceinline__ void propagate_tables(const Tables<T>& tb, unsigned char* smem_raw, bool coupling) {
   T* s_coup = reinterpret_cast<T*>(smem_raw);
   T* s_par = s_coup + kSmemCoup;
-  T* s_state = s_par + kSmemPar;
   if constexpr (M::COUPLED) {
-    for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = tb.coupling[i];
+    if (coupling)
+      for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = tb.coupling[i];
   }
   for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
   __syncthreads();
+}
+
+// Particle g (of all runs) over one interval: gather, substeps, store,
+// log-weight.  Returns the log-weight written (NaN when the interval is not
+// weighted).  The shared tables must be loaded; the particle's shared-memory
+// state column is the calling thread's.
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR, bool MULTI>
+__device__ __forceinline__ double propagate_particle(const Tables<T>& tb, const StepArgs& a, size_t g,
+                                                     unsigned char* smem_raw) {
+  T* s_coup = reinterpret_cast<T*>(smem_raw);
+  T* s_par = s_coup + kSmemCoup;
+  T* s_state = s_par + kSmemPar;
   const int J = tb.J;
   const size_t RJ = (size_t)tb.R * J;
-  const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;  // particle of all runs
-  if (g >= RJ) return;
   const int r = (int)(g / J);
   const int j = (int)(g - (size_t)r * J);                  // slot within its run
   const size_t src = (size_t)r * J + (a.anc ? __ldg(a.anc + g) : (uint32_t)j);
@@ -359,8 +372,14 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   if constexpr (SMEM) {
     x.b = s_state + threadIdx.x;
   }
+  if (a.x0_rep) {
+    // the initial particle, replicated (build_D_J_p_X / replicate_J_p_X_0, smc.c:167-176)
 #pragma unroll
-  for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * RJ + src];
+    for (int w = 0; w < M::OFF_INC; ++w) x[w] = (T)__ldg(a.x0_rep + w);
+  } else {
+#pragma unroll
+    for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * RJ + src];
+  }
 #pragma unroll
   for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);  // reset_inc
 
@@ -510,8 +529,20 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
         }
       }
     }
-    ((T*)a.lw)[g] = (T)(plomrt::finish_loglik(ll, fl, M::N_TS) + lpr);
+    const T lwv = (T)(plomrt::finish_loglik(ll, fl, M::N_TS) + lpr);
+    ((T*)a.lw)[g] = lwv;
+    return (double)lwv;
   }
+  return NAN;
+}
+
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false>
+__global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  propagate_tables<T, BT>(tb, smem_raw, true);
+  const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;  // particle of all runs
+  if (g >= (size_t)tb.R * tb.J) return;
+  propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
 }
 
 // ------------------------------------------------------------------ propagate, one team per particle
@@ -994,73 +1025,24 @@ __device__ __forceinline__ double surviving_exp(T l, double thresh, double m) {
   return weight_fails(l, thresh) ? 0.0 : exp((double)l - m);
 }
 
-template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double thresh,
-                                                     double log_like_min, LseAcc* part, double* P, StepState* st,
-                                                     FilterAcc* acc, int n, double U_crn, const uint64_t* seed,
-                                                     uint32_t filter_id, double* llike_out, double* ess_out,
-                                                     int out_stride) {
-  constexpr int TILE = BT * IPT;
-  __shared__ LseAcc sh[BT / 32];
-  __shared__ double shd[BT / 32];
-  __shared__ bool last;
-  const int ntiles = gridDim.x;
-  {
-    const int r = blockIdx.y;
-    lw += (size_t)r * J;
-    part += (size_t)r * ntiles;
-    P += (size_t)r * (ntiles + 1);
-    st += r;
-    acc += r;
-    if (llike_out) llike_out += (size_t)r * out_stride;
-    if (ess_out) ess_out += (size_t)r * out_stride;
-    filter_id += (uint32_t)r;
-  }
-  const int base = blockIdx.x * TILE;
-  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
-#pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    const int i = base + k * BT + threadIdx.x;
-    if (i < J) {
-      const T l = lw[i];
-      if (weight_fails(l, thresh)) {
-        a.nfail += 1;
-      } else {
-        LseAcc b = {(double)l, 1.0, 1.0, 0};
-        a = lse_merge(a, b);
-      }
-    }
-  }
+// Shared scratch of the weighting / resampling of one tile (BT threads,
+// IPT particles each); placed by the caller (static in the stand-alone
+// kernels, inside the dynamic region of the serving loop).
+template <int BT, int IPT>
+struct TileScratch {
+  double sC[BT * IPT];
+  double swarp[BT / 32];
+  LseAcc lse[BT / 32];
+  plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  int ns, fail, jlo, jhi, lastpos, last;
+};
+
+// (max, sum exp(l - max), sum exp(2 (l - max)), failures) of one thread's
+// log-weights merged over the block (fixed order); every thread gets it.
+template <int BT>
+__device__ __forceinline__ LseAcc block_lse_all(LseAcc a, LseAcc* sh) {
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-    if (threadIdx.x == 0) {
-      part[blockIdx.x] = a;
-      __threadfence();
-      const unsigned t = atomicAdd(&acc->ticket, 1u);
-      last = (t == (unsigned)ntiles - 1u);
-    }
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the last block: fold the tiles in a fixed order (contiguous chunks per thread)
-  const int chunk = (ntiles + BT - 1) / BT;
-  const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
-  a = LseAcc{-INFINITY, 0.0, 0.0, 0};
-  for (int b = b0; b < b1; ++b) {
-    volatile LseAcc* p = part + b;
-    LseAcc v = {p->m, p->s1, p->s2, p->nfail};
-    a = lse_merge(a, v);
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-  __syncthreads();
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
   __syncthreads();
   if (threadIdx.x < 32) {
@@ -1071,13 +1053,34 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   }
   __syncthreads();
   a = sh[0];
+  __syncthreads();
+  return a;
+}
+
+// The fold of the tile partials by one block (all threads call it): the
+// filter's (max, sums, failures) in tile order, the exclusive prefix P[b] of
+// the tiles' normalised weights (P[ntiles] = their total), llike, ESS, the
+// all-fail rule (smc.c:55-69) and the systematic points of the interval.
+template <int BT>
+__device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_like_min, double* P, StepState* st,
+                           FilterAcc* acc, int n, double U_crn, plomrt::PhiloxKey key, double* llike_out,
+                           double* ess_out, LseAcc* sh, double* shd) {
+  const int chunk = (ntiles + BT - 1) / BT;
+  const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
+  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+  for (int b = b0; b < b1; ++b) {
+    volatile const LseAcc* p = part + b;
+    LseAcc v = {p->m, p->s1, p->s2, p->nfail};
+    a = lse_merge(a, v);
+  }
+  a = block_lse_all<BT>(a, sh);
   const int all_fail = (a.nfail == J);
   // exclusive prefix of the tiles' normalised weights: chunk totals, a block
   // scan of them, then each chunk written in order
   double tot = 0.0;
   if (!all_fail) {
     for (int b = b0; b < b1; ++b) {
-      volatile LseAcc* p = part + b;
+      volatile const LseAcc* p = part + b;
       if (p->s1 > 0.0) tot += p->s1 * (exp(p->m - a.m) / a.s1);
     }
   }
@@ -1104,13 +1107,12 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   for (int b = b0; b < b1; ++b) {
     P[b] = run;
     if (!all_fail) {
-      volatile LseAcc* p = part + b;
+      volatile const LseAcc* p = part + b;
       if (p->s1 > 0.0) run += p->s1 * (exp(p->m - a.m) / a.s1);
     }
   }
   if (b1 == ntiles && b0 < b1) P[ntiles] = run;
   if (threadIdx.x == 0) {
-    acc->ticket = 0u;
     double llike, ess;
     if (all_fail) {
       // every particle failed: equal weights, identity ancestors (smc.c:55-69)
@@ -1129,7 +1131,7 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
     if (llike_out) llike_out[n] = llike;
     if (ess_out) ess_out[n] = ess;
     const double inc = 1.0 / (double)J;
-    const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(plomrt::make_key(*seed, filter_id), (uint32_t)n);
+    const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(key, (uint32_t)n);
     const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
     st->U = U;
     int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
@@ -1139,6 +1141,57 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
     }
     st->nseg = ns;
   }
+}
+
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double thresh,
+                                                     double log_like_min, LseAcc* part, double* P, StepState* st,
+                                                     FilterAcc* acc, int n, double U_crn, const uint64_t* seed,
+                                                     uint32_t filter_id, double* llike_out, double* ess_out,
+                                                     int out_stride) {
+  __shared__ LseAcc sh[BT / 32];
+  __shared__ double shd[BT / 32];
+  __shared__ bool last;
+  const int ntiles = gridDim.x;
+  {
+    const int r = blockIdx.y;
+    lw += (size_t)r * J;
+    part += (size_t)r * ntiles;
+    P += (size_t)r * (ntiles + 1);
+    st += r;
+    acc += r;
+    if (llike_out) llike_out += (size_t)r * out_stride;
+    if (ess_out) ess_out += (size_t)r * out_stride;
+    filter_id += (uint32_t)r;
+  }
+  const int base = blockIdx.x * BT * IPT;
+  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    const int i = base + k * BT + threadIdx.x;
+    if (i < J) {
+      const T l = lw[i];
+      if (weight_fails(l, thresh)) {
+        a.nfail += 1;
+      } else {
+        LseAcc b = {(double)l, 1.0, 1.0, 0};
+        a = lse_merge(a, b);
+      }
+    }
+  }
+  a = block_lse_all<BT>(a, sh);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = a;
+    __threadfence();
+    const unsigned t = atomicAdd(&acc->ticket, 1u);
+    last = (t == (unsigned)ntiles - 1u);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) acc->ticket = 0u;
+  fold_tiles<BT>(part, ntiles, J, log_like_min, P, st, acc, n, U_crn, plomrt::make_key(*seed, filter_id), llike_out,
+                 ess_out, sh, shd);
 }
 
 // first j in [0, J] whose systematic point exceeds v (J when none): the
@@ -1165,35 +1218,22 @@ __device__ __forceinline__ int first_point_above(const plomrt::SysSeg* seg, int 
   return lo;
 }
 
+// Ancestors of the systematic points of tile b (all threads of the block
+// call it; `sc` is the block's scratch).
 template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J, double thresh,
-                                                 const LseAcc* __restrict__ part, const double* __restrict__ P,
-                                                 const StepState* st, uint32_t* __restrict__ anc,
-                                                 uint32_t* __restrict__ anc_hist) {
+__device__ void resample_tile(const T* __restrict__ lw, int J, double thresh, const LseAcc* __restrict__ part,
+                              const double* __restrict__ P, const StepState* st, int b, int ntiles,
+                              uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, TileScratch<BT, IPT>& sc) {
   constexpr int TILE = BT * IPT;
-  __shared__ double sC[TILE];
-  __shared__ double swarp[BT / 32];
-  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  __shared__ int s_ns, s_fail, s_jlo, s_jhi, s_lastpos;
-  const int ntiles = gridDim.x;
-  {
-    const int r = blockIdx.y;
-    lw += (size_t)r * J;
-    part += (size_t)r * ntiles;
-    P += (size_t)r * (ntiles + 1);
-    st += r;
-    anc += (size_t)r * J;
-    if (anc_hist) anc_hist += (size_t)r * J;
-  }
-  const int b = blockIdx.x, base = b * TILE;
+  const int base = b * TILE;
   const int n_in = min(TILE, J - base);
   if (threadIdx.x == 0) {
-    s_ns = st->nseg;
-    s_fail = st->all_fail;
-    s_lastpos = -1;
+    sc.ns = st->nseg;
+    sc.fail = st->all_fail;
+    sc.lastpos = -1;
   }
   __syncthreads();
-  if (s_fail || s_ns == 0) {
+  if (sc.fail || sc.ns == 0) {
     // every particle failed (or the point table overflowed): identity
     for (int i = threadIdx.x; i < n_in; i += BT) {
       anc[base + i] = (uint32_t)(base + i);
@@ -1201,8 +1241,8 @@ __global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J
     }
     return;
   }
-  const int ns = s_ns;
-  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = st->seg[i];
+  const int ns = sc.ns;
+  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = st->seg[i];
   // cumulative weights of the tile, rows of BT particles in order
   const double mb = part[b].m;
   const double f = (part[b].s1 > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
@@ -1224,46 +1264,59 @@ __global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J
       const double o = __shfl_up_sync(0xffffffffu, v, off);
       if (lane >= off) v += o;
     }
-    if (lane == 31) swarp[warp] = v;
+    if (lane == 31) sc.swarp[warp] = v;
     __syncthreads();
     if (warp == 0) {
-      double w = (lane < BT / 32) ? swarp[lane] : 0.0;
+      double w = (lane < BT / 32) ? sc.swarp[lane] : 0.0;
 #pragma unroll
       for (int off = 1; off < 32; off <<= 1) {
         const double o = __shfl_up_sync(0xffffffffu, w, off);
         if (lane >= off) w += o;
       }
-      if (lane < BT / 32) swarp[lane] = w;
+      if (lane < BT / 32) sc.swarp[lane] = w;
     }
     __syncthreads();
-    const double incl = carry + ((warp > 0) ? swarp[warp - 1] : 0.0) + v;
-    sC[ii] = Pb + incl * f;
-    carry += swarp[BT / 32 - 1];
+    const double incl = carry + ((warp > 0) ? sc.swarp[warp - 1] : 0.0) + v;
+    sc.sC[ii] = Pb + incl * f;
+    carry += sc.swarp[BT / 32 - 1];
     __syncthreads();
   }
-  if (lastpos >= 0) atomicMax(&s_lastpos, lastpos);
+  if (lastpos >= 0) atomicMax(&sc.lastpos, lastpos);
   if (threadIdx.x == 0) {
     const double U = st->U;
-    s_jlo = (b == 0) ? 0 : first_point_above(seg, ns, J, U, Pb);
-    s_jhi = (b == ntiles - 1) ? J : first_point_above(seg, ns, J, U, P[b + 1]);
+    sc.jlo = (b == 0) ? 0 : first_point_above(sc.seg, ns, J, U, Pb);
+    sc.jhi = (b == ntiles - 1) ? J : first_point_above(sc.seg, ns, J, U, P[b + 1]);
   }
   __syncthreads();
-  const int jlo = s_jlo, jhi = s_jhi;
+  const int jlo = sc.jlo, jhi = sc.jhi;
   // past the tile's last cumulative weight (rounding): its last surviving
   // particle, and the last particle for the last tile (the reference reads on
   // past the array there)
-  const int clamp = (b == ntiles - 1 || s_lastpos < 0) ? n_in - 1 : s_lastpos;
+  const int clamp = (b == ntiles - 1 || sc.lastpos < 0) ? n_in - 1 : sc.lastpos;
   for (int j = jlo + threadIdx.x; j < jhi; j += BT) {
-    const double ran = plomrt::systematic_point(seg, ns, j);
+    const double ran = plomrt::systematic_point(sc.seg, ns, j);
     int lo = 0, hi = n_in;
     while (lo < hi) {  // first i with !(ran > C[i])  (smc.c:105-108)
       const int mid = (lo + hi) >> 1;
-      if (ran > sC[mid]) lo = mid + 1; else hi = mid;
+      if (ran > sc.sC[mid]) lo = mid + 1; else hi = mid;
     }
     const uint32_t a_ = (uint32_t)(base + (lo < n_in ? lo : clamp));
     anc[j] = a_;
     if (anc_hist) anc_hist[j] = a_;
   }
+}
+
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J, double thresh,
+                                                 const LseAcc* __restrict__ part, const double* __restrict__ P,
+                                                 const StepState* st, uint32_t* __restrict__ anc,
+                                                 uint32_t* __restrict__ anc_hist) {
+  __shared__ TileScratch<BT, IPT> sc;
+  const int ntiles = gridDim.x;
+  const int r = blockIdx.y;
+  resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, thresh, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
+                            st + r, blockIdx.x, ntiles, anc + (size_t)r * J,
+                            anc_hist ? anc_hist + (size_t)r * J : nullptr, sc);
 }
 
 // ------------------------------------------------------------------ helpers

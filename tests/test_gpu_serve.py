@@ -56,11 +56,41 @@ def test_admission_respects_memory_budget():
     assert st['peak_in_flight'] <= 3
 
 
+@pytest.mark.parametrize('precision', [32, 64])
+def test_tiled_loop_same_alone_in_the_mix_and_plain(precision):
+    """Models whose particle does not fit registers (SEIR 20x2, 180 words) run on the tiled device
+    loop: tiles of many requests share the SMs; a request's result is bit-identical alone and in
+    the mix, and equal to the plain filter with the same parameters and seed (same tiles, same
+    reduction order)."""
+    eng = models.engine('seir20x2')
+    p = models.make_problem('seir20x2', J=1000, dt=1.0, precision=precision, seed=1, nb_obs=30)
+    rng = np.random.default_rng(5)
+    pcs = _thetas(p, 9, rng)
+    sv = Server(eng, p, max_J=3000, precision=precision)
+    alone = sv.wait(sv.submit(1000, par_cac=pcs[0], seed=5))[0]
+    Js = [1000] + [int(rng.integers(300, 3000)) for _ in pcs[1:]]
+    ts = [sv.submit(Js[i], par_cac=pc, seed=5 if i == 0 else 100 + i) for i, pc in enumerate(pcs)]
+    mixed = [sv.wait(t) for t in ts]
+    st = sv.stats()
+    sv.close()
+    assert st['persistent_loop'] == 1
+    assert mixed[0][0] == alone
+    assert st['completed'] == 10 and st['pending'] == 0 and st['in_flight'] == 0
+    q = models.make_problem('seir20x2', J=1000, dt=1.0, precision=precision, seed=5, nb_obs=30)
+    q.par_cac = pcs[0]
+    assert eng.smc(q).loglik == alone
+    # other requests of the mix equal their own plain filters too
+    for i in (3, 7):
+        qi = models.make_problem('seir20x2', J=Js[i], dt=1.0, precision=precision, seed=100 + i, nb_obs=30)
+        qi.par_cac = pcs[i]
+        assert eng.smc(qi).loglik == mixed[i][0]
+
+
 def test_plan_pool_same_alone_and_in_the_mix():
-    """Models whose particle does not fit registers are served by concurrent plans."""
+    """Models whose particle does not fit registers can also be served by concurrent plans."""
     eng = models.engine('seir20x2')
     p = models.make_problem('seir20x2', J=1024, dt=1.0, precision=32, seed=1, nb_obs=40)
-    sv = Server(eng, p, max_J=2048, plan_pool=4, precision=32)
+    sv = Server(eng, p, max_J=2048, plan_pool=4, precision=32, use_plan_pool=True)
     alone = sv.wait(sv.submit(1024, seed=5))[0]
     ts = [sv.submit(1024 if i % 2 == 0 else 2048, seed=5 if i == 0 else 100 + i) for i in range(10)]
     mixed = [sv.wait(t) for t in ts]
