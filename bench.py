@@ -298,7 +298,7 @@ def run_batch(args):
         torch.cuda.synchronize()
     ms = start.elapsed_time(end) / args.steps
     ll, nf, ess = b.results()
-    bt, grid = b.config
+    bt, ppt, grid = b.config
     b.close()
     value = bp.particle_steps / (ms / 1000.0)
     # plain single-filter path on the config-0 filter (J = 1000, T = 52), graph replay
@@ -332,7 +332,8 @@ def run_batch(args):
             'warmup': args.warmup, 'ms_per_step': ms, 'higher_is_better': True, 'scaling': 'weak',
             'vs_baseline': None, 'dtype': 'f32 state / f64 reductions', 'data': 'synthetic',
             'config': {'workload': 'sir_batch', 'filters': 4096, 'particle_steps': bp.particle_steps,
-                       'J_range': [256, 16384], 'T_range': [52, 520], 'block_threads': bt, 'grid': grid},
+                       'J_range': [256, 16384], 'T_range': [52, 520], 'block_threads': bt,
+                       'particles_per_thread': ppt, 'grid': grid, 'tuned_by': 'plomgpu batch autotuner'},
             'plain_single_filter': {'value': single_value, 'ms_per_filter': ms_single, 'J': single.J,
                                     'T': single.n_obs},
             'batched_over_plain': value / single_value,

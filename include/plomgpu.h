@@ -342,17 +342,20 @@ typedef struct plomgpu_batch_desc {
     double like_min;
     int precision;             /* 32 or 64 */
     int block_threads;         /* 0: autotuned among 128 / 256 / 512 */
+    int particles_per_thread;  /* particles a thread advances together: 0 autotuned among 1 / 2 (FP64: 1) */
 } plomgpu_batch_desc;
 
 typedef struct plomgpu_batch plomgpu_batch;
 
-/* Uploads the batch, sizes the per-CTA workspaces and (block_threads == 0)
- * times the candidate block sizes on a sample of the batch. */
+/* Uploads the batch, sizes the per-CTA workspaces and (block_threads or
+ * particles_per_thread == 0) times the candidate (block size, particles per
+ * thread) pairs on a sample of the batch, keeping the fastest. */
 int plomgpu_batch_create(const plomgpu_batch_desc *desc, plomgpu_batch **out);
 int plomgpu_batch_launch(plomgpu_batch *batch);
 int plomgpu_batch_results(plomgpu_batch *batch, double *loglik, int *n_all_fail, double *ess_min);
 void *plomgpu_batch_stream(plomgpu_batch *batch);
-int plomgpu_batch_config(plomgpu_batch *batch, int *block_threads, int *grid);
+/* The configuration in use: threads per block, particles per thread, CTAs. */
+int plomgpu_batch_config(plomgpu_batch *batch, int *block_threads, int *particles_per_thread, int *grid);
 void plomgpu_batch_destroy(plomgpu_batch *batch);
 /* One-shot: create, launch, results, destroy. */
 int plomgpu_batch_run(const plomgpu_batch_desc *desc, double *loglik, int *n_all_fail);

@@ -60,7 +60,7 @@ constexpr int kIptScan = 8;
 constexpr int kTile = kBtScan * kIptScan;
 constexpr int kBtSearch = 256;
 constexpr int kMaxWeightBlocks = 592;
-// tiles of the filters' weighting / resampling (k_weight_tiles, k_resample):
+// tiles of the filters' weighting / resampling (k_weight_tiles, k_cum_tiles, k_search_tiles):
 // the propagate block's particles for shared-memory models (the tiles of the
 // serving loop, so that a served request and the plain filter reduce in the
 // same order), 1024 particles otherwise
@@ -94,6 +94,7 @@ struct plomgpu_plan {
   void* X[2] = {nullptr, nullptr};
   void* lw = nullptr;
   double* P = nullptr;            // [R][ntiles + 1] tile prefixes of the normalised weights
+  double* C = nullptr;            // [R][J] cumulative normalised weights
   uint32_t* anc[2] = {nullptr, nullptr};
   LseAcc* part = nullptr;         // [R][ntiles] tile partials
   StepState* st = nullptr;
@@ -449,10 +450,11 @@ int enqueue_filter(plomgpu_plan* p) {
         ++kernels;
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
-      k_resample<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->thresh, p->part, p->P, p->st, p->anc[nxt],
-          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
-      kernels += 2;
+      k_cum_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>((const T*)p->lw, J, p->thresh, p->part,
+                                                                           p->P, p->st, p->C);
+      k_search_tiles<kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+      kernels += 3;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
         ++kernels;
@@ -567,6 +569,7 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(cudaMalloc(&p->X[0], (size_t)M::S * RJ * sizeof(T)));
   CK(cudaMalloc(&p->X[1], (size_t)M::S * RJ * sizeof(T)));
   CK(cudaMalloc(&p->lw, RJ * sizeof(T)));
+  CK(cudaMalloc((void**)&p->C, RJ * sizeof(double)));
   CK(cudaMalloc((void**)&p->anc[0], RJ * sizeof(uint32_t)));
   CK(cudaMalloc((void**)&p->anc[1], RJ * sizeof(uint32_t)));
   if (p->mif) {
@@ -709,7 +712,7 @@ void plan_free(plomgpu_plan* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->anc[0], p->anc[1], p->part, p->st, p->acc,
+  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->C, p->anc[0], p->anc[1], p->part, p->st, p->acc,
                   p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
@@ -1375,7 +1378,7 @@ extern "C" int plomgpu_resample_noalloc(const void* log_weights, int precision, 
 
 struct plomgpu_batch {
   int n = 0, max_obs = 0, max_J = 0, precision = 32, noises_off = 0, filter = 1;
-  int bt = 0, grid = 0, kernels = 1;
+  int bt = 0, ppt = 0, grid = 0, kernels = 1;
   double dt = 1.0, like_min = 1e-17;
   cudaStream_t stream = nullptr;
   std::vector<BatchFilter> filters_h;
@@ -1402,44 +1405,57 @@ namespace {
 template <class T>
 using BatchKernel = void (*)(const BatchArgs<T>);
 
-template <class T, int BT>
+template <class T, int BT, int PPT>
 BatchKernel<T> pick_batch_bt(int v, bool drift) {
   if constexpr (!kSmem) {
     if (drift) {
       if constexpr (M::N_DRIFT > 0) {
         switch (v) {
-          case 0: return &k_batch<T, 0, true, BT>;
-          case 1: return &k_batch<T, 1, true, BT>;
-          case 2: return &k_batch<T, 2, true, BT>;
-          default: return &k_batch<T, 3, true, BT>;
+          case 0: return &k_batch<T, 0, true, BT, PPT>;
+          case 1: return &k_batch<T, 1, true, BT, PPT>;
+          case 2: return &k_batch<T, 2, true, BT, PPT>;
+          default: return &k_batch<T, 3, true, BT, PPT>;
         }
       }
       return nullptr;
     }
     switch (v) {
-      case 0: return &k_batch<T, 0, false, BT>;
-      case 1: return &k_batch<T, 1, false, BT>;
-      case 2: return &k_batch<T, 2, false, BT>;
-      default: return &k_batch<T, 3, false, BT>;
+      case 0: return &k_batch<T, 0, false, BT, PPT>;
+      case 1: return &k_batch<T, 1, false, BT, PPT>;
+      case 2: return &k_batch<T, 2, false, BT, PPT>;
+      default: return &k_batch<T, 3, false, BT, PPT>;
     }
   }
   return nullptr;
 }
 
+// the batched kernel of a block size and a count of particles per thread
+// (FP64, the parity mode: 256 threads, one particle per thread)
 template <class T>
-BatchKernel<T> pick_batch(int bt, int noises_off) {
+BatchKernel<T> pick_batch(int bt, int ppt, int noises_off) {
   const int v = variant_of(noises_off);
   const bool d = drift_on(noises_off);
   if constexpr (std::is_same<T, double>::value) {
-    if (bt == 256) return pick_batch_bt<T, 256>(v, d);
+    if (bt == 256 && ppt == 1) return pick_batch_bt<T, 256, 1>(v, d);
     return nullptr;
   } else {
-    switch (bt) {
-      case 128: return pick_batch_bt<T, 128>(v, d);
-      case 256: return pick_batch_bt<T, 256>(v, d);
-      case 512: return pick_batch_bt<T, 512>(v, d);
-      default: return nullptr;
+    if (ppt == 1) {
+      switch (bt) {
+        case 128: return pick_batch_bt<T, 128, 1>(v, d);
+        case 256: return pick_batch_bt<T, 256, 1>(v, d);
+        case 512: return pick_batch_bt<T, 512, 1>(v, d);
+        default: return nullptr;
+      }
     }
+    if (ppt == 2) {
+      switch (bt) {
+        case 128: return pick_batch_bt<T, 128, 2>(v, d);
+        case 256: return pick_batch_bt<T, 256, 2>(v, d);
+        case 512: return pick_batch_bt<T, 512, 2>(v, d);
+        default: return nullptr;
+      }
+    }
+    return nullptr;
   }
 }
 
@@ -1481,8 +1497,8 @@ BatchArgs<T> batch_args(plomgpu_batch* b, const BatchFilter* filters, int n, con
 }
 
 template <class T>
-int batch_enqueue(plomgpu_batch* b, int bt, int grid, const BatchFilter* filters, int n, const int* order) {
-  BatchKernel<T> k = pick_batch<T>(bt, b->noises_off);
+int batch_enqueue(plomgpu_batch* b, int bt, int ppt, int grid, const BatchFilter* filters, int n, const int* order) {
+  BatchKernel<T> k = pick_batch<T>(bt, ppt, b->noises_off);
   if (!k) return fail(PLOMGPU_EINVAL, "no batched kernel for this block size / precision / model");
   CK(cudaMemsetAsync(b->queue, 0, sizeof(unsigned), b->stream));
   CK(cudaMemsetAsync(b->error, 0, sizeof(int), b->stream));
@@ -1492,23 +1508,32 @@ int batch_enqueue(plomgpu_batch* b, int bt, int grid, const BatchFilter* filters
 }
 
 template <class T>
-int batch_occupancy(int bt, int noises_off, int* per_sm) {
-  BatchKernel<T> k = pick_batch<T>(bt, noises_off);
+int batch_occupancy(int bt, int ppt, int noises_off, int* per_sm) {
+  BatchKernel<T> k = pick_batch<T>(bt, ppt, noises_off);
   if (!k) return fail(PLOMGPU_EINVAL, "no batched kernel");
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k, bt, 0));
   return PLOMGPU_OK;
 }
 
-// Picks the block size (and the grid from the occupancy of that kernel) by
-// timing the candidates on a sample of the batch: the longest filters, cut
-// to a few intervals.
+// Picks the block size and the particles per thread (and the grid from the
+// occupancy of that kernel) by timing the candidates on a sample of the
+// batch: the longest filters, cut to a few intervals.
 template <class T>
 int batch_autotune(plomgpu_batch* b, int sms) {
-  std::vector<int> cands;
-  if (std::is_same<T, double>::value) cands = {256};
-  else cands = {128, 256, 512};
-  if (b->bt > 0) cands = {b->bt};
-  int best_bt = 0, best_grid = 0;
+  std::vector<std::pair<int, int>> cands;
+  if (std::is_same<T, double>::value) {
+    cands = {{256, 1}};
+  } else {
+    for (int bt : {128, 256, 512})
+      for (int ppt : {1, 2}) cands.push_back({bt, ppt});
+  }
+  {
+    std::vector<std::pair<int, int>> keep;
+    for (auto c : cands)
+      if ((b->bt <= 0 || c.first == b->bt) && (b->ppt <= 0 || c.second == b->ppt)) keep.push_back(c);
+    cands = keep;
+  }
+  int best_bt = 0, best_ppt = 0, best_grid = 0;
   float best = 1e30f;
   // sample: enough filters to fill the largest grid twice, 12 intervals each
   std::vector<BatchFilter> sample;
@@ -1529,15 +1554,16 @@ int batch_autotune(plomgpu_batch* b, int sms) {
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   int rc = PLOMGPU_OK;
-  for (int bt : cands) {
+  for (auto c : cands) {
+    const int bt = c.first, ppt = c.second;
     int per_sm = 0;
-    if ((rc = batch_occupancy<T>(bt, b->noises_off, &per_sm))) break;
+    if ((rc = batch_occupancy<T>(bt, ppt, b->noises_off, &per_sm))) break;
     if (per_sm < 1) continue;
     const int grid = sms * per_sm;
-    if ((size_t)grid * b->ws_stride > (size_t)b->grid * b->ws_stride) continue;  // workspace sized for b->grid
-    if ((rc = batch_enqueue<T>(b, bt, grid, d_sample, (int)sample.size(), d_sorder))) break;  // warm
+    if (grid > b->grid) continue;  // workspace sized for b->grid
+    if ((rc = batch_enqueue<T>(b, bt, ppt, grid, d_sample, (int)sample.size(), d_sorder))) break;  // warm
     CK(cudaEventRecord(e0, b->stream));
-    if ((rc = batch_enqueue<T>(b, bt, grid, d_sample, (int)sample.size(), d_sorder))) break;
+    if ((rc = batch_enqueue<T>(b, bt, ppt, grid, d_sample, (int)sample.size(), d_sorder))) break;
     CK(cudaEventRecord(e1, b->stream));
     CK(cudaEventSynchronize(e1));
     float ms = 0.f;
@@ -1545,6 +1571,7 @@ int batch_autotune(plomgpu_batch* b, int sms) {
     if (ms < best) {
       best = ms;
       best_bt = bt;
+      best_ppt = ppt;
       best_grid = grid;
     }
   }
@@ -1555,6 +1582,7 @@ int batch_autotune(plomgpu_batch* b, int sms) {
   if (rc) return rc;
   if (!best_bt) return fail(PLOMGPU_EINVAL, "no batched configuration fits");
   b->bt = best_bt;
+  b->ppt = best_ppt;
   b->grid = best_grid;
   return PLOMGPU_OK;
 }
@@ -1614,11 +1642,14 @@ int batch_build(const plomgpu_batch_desc* d, plomgpu_batch* b) {
   CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   int max_grid = 0;
   for (int bt : {128, 256, 512}) {
-    if (std::is_same<T, double>::value && bt != 256) continue;
-    if (d->block_threads > 0 && bt != d->block_threads) continue;
-    int per_sm = 0;
-    if ((rc = batch_occupancy<T>(bt, d->noises_off, &per_sm))) return rc;
-    max_grid = std::max(max_grid, sms * per_sm);
+    for (int ppt : {1, 2}) {
+      if (std::is_same<T, double>::value && (bt != 256 || ppt != 1)) continue;
+      if (d->block_threads > 0 && bt != d->block_threads) continue;
+      if (d->particles_per_thread > 0 && ppt != d->particles_per_thread) continue;
+      int per_sm = 0;
+      if ((rc = batch_occupancy<T>(bt, ppt, d->noises_off, &per_sm))) return rc;
+      max_grid = std::max(max_grid, sms * per_sm);
+    }
   }
   if (max_grid < 1) return fail(PLOMGPU_EINVAL, "batched kernel does not fit on the device");
   b->ws_stride = (batch_ws_bytes<T>(b->max_J) + 255) & ~(size_t)255;
@@ -1626,6 +1657,7 @@ int batch_build(const plomgpu_batch_desc* d, plomgpu_batch* b) {
   CK(cudaMalloc((void**)&b->ws, b->ws_stride * (size_t)max_grid));
   CK(cudaStreamSynchronize(s));
   b->bt = d->block_threads;
+  b->ppt = d->particles_per_thread;
   if ((rc = batch_autotune<T>(b, sms))) return rc;
   return PLOMGPU_OK;
 }
@@ -1645,6 +1677,8 @@ int plomgpu_batch_create(const plomgpu_batch_desc* d, plomgpu_batch** out) {
   if (M::COUPLED && !d->coupling) return fail(PLOMGPU_EINVAL, "coupled model needs a coupling matrix");
   if (d->block_threads != 0 && d->block_threads != 128 && d->block_threads != 256 && d->block_threads != 512)
     return fail(PLOMGPU_EINVAL, "block_threads must be 0 (autotune), 128, 256 or 512");
+  if (d->particles_per_thread != 0 && d->particles_per_thread != 1 && d->particles_per_thread != 2)
+    return fail(PLOMGPU_EINVAL, "particles_per_thread must be 0 (autotune), 1 or 2");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PLOMGPU_ENODEV, "no CUDA device");
   plomgpu_batch* b = new plomgpu_batch();
@@ -1692,8 +1726,8 @@ int plomgpu_batch_create(const plomgpu_batch_desc* d, plomgpu_batch** out) {
 
 int plomgpu_batch_launch(plomgpu_batch* b) {
   if (!b) return fail(PLOMGPU_EINVAL, "null batch");
-  return (b->precision == 64) ? batch_enqueue<double>(b, b->bt, b->grid, b->filters, b->n, b->order)
-                              : batch_enqueue<float>(b, b->bt, b->grid, b->filters, b->n, b->order);
+  return (b->precision == 64) ? batch_enqueue<double>(b, b->bt, b->ppt, b->grid, b->filters, b->n, b->order)
+                              : batch_enqueue<float>(b, b->bt, b->ppt, b->grid, b->filters, b->n, b->order);
 }
 
 int plomgpu_batch_results(plomgpu_batch* b, double* loglik, int* n_all_fail, double* ess_min) {
@@ -1711,9 +1745,10 @@ int plomgpu_batch_results(plomgpu_batch* b, double* loglik, int* n_all_fail, dou
 
 void* plomgpu_batch_stream(plomgpu_batch* b) { return b ? (void*)b->stream : nullptr; }
 
-int plomgpu_batch_config(plomgpu_batch* b, int* block_threads, int* grid) {
+int plomgpu_batch_config(plomgpu_batch* b, int* block_threads, int* particles_per_thread, int* grid) {
   if (!b) return fail(PLOMGPU_EINVAL, "null batch");
   if (block_threads) *block_threads = b->bt;
+  if (particles_per_thread) *particles_per_thread = b->ppt;
   if (grid) *grid = b->grid;
   return PLOMGPU_OK;
 }
@@ -1913,13 +1948,18 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->base.par_cac = sv->par_cac_h.data();
   sv->base.par_ts = sv->par_ts_h.data();
   sv->base.x0 = sv->x0_h.data();
-  cudaError_t e = cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking);
+  // the tiled loop fills whatever the GPU leaves free (lowest priority); a
+  // one-CTA-per-request loop serves small, latency-bound requests (highest)
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  const int prio = sv->tiled ? prio_low : prio_high;
+  cudaError_t e = cudaStreamCreateWithPriority(&sv->stream, cudaStreamNonBlocking, prio);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->kernel_ev, cudaEventDisableTiming);
   if (e == cudaSuccess) {
     sv->loop_stream[0] = sv->stream;
     sv->loop_ev[0] = sv->kernel_ev;
     for (int i = 1; i < plomgpu_server::kLoops && e == cudaSuccess; ++i) {
-      e = cudaStreamCreateWithFlags(&sv->loop_stream[i], cudaStreamNonBlocking);
+      e = cudaStreamCreateWithPriority(&sv->loop_stream[i], cudaStreamNonBlocking, prio);
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sv->loop_ev[i], cudaEventDisableTiming);
     }
   }

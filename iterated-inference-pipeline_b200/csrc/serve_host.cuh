@@ -97,6 +97,7 @@ struct plomgpu_server {
   bool tiled = kSmem;           // the tiled loop (shared-memory particles)
   size_t tiles_smem = 0;        // its dynamic shared memory
   long long* d_live = nullptr;  // its live-request table [kServeLive]
+  int task_budget = 64;         // tasks a CTA of the tiled loop runs before it returns
   int bt = 256, grid = 0;
   long long idle_limit = 20000;
   // base problem (host copies; every request shares it)
@@ -215,7 +216,7 @@ ServeKernel<T> pick_serve(int noises_off) {
 
 template <class T>
 using ServeTilesKernel = void (*)(const BatchArgs<T>, ServeSlot*, const int*, int, ServeCtl*, unsigned long long*,
-                                  unsigned char*, long long*, long long);
+                                  unsigned char*, long long*, long long, int);
 
 template <class T>
 ServeTilesKernel<T> pick_serve_tiles(int noises_off) {
@@ -249,7 +250,7 @@ int serve_launch(plomgpu_server* sv, int inst, int grid) {
     ServeTilesKernel<T> k = pick_serve_tiles<T>(sv->base.noises_off);
     if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
     k<<<grid, sv->bt, sv->tiles_smem, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d,
-                                            sv->d_head, sv->d_pool, sv->d_live, sv->idle_limit);
+                                            sv->d_head, sv->d_pool, sv->d_live, sv->idle_limit, sv->task_budget);
   } else {
     ServeKernel<T> k = pick_serve<T>(sv->base.noises_off);
     if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
@@ -417,11 +418,22 @@ void serve_pass(plomgpu_server* sv) {
     long long waiting = 0;
     for (int i = 0; i < sv->ring; ++i) waiting += sv->slot_ticket[i] >= 0;
     if (sv->tiled) {
-      // one instance holding every resident CTA slot: the tiles of all live
-      // requests share it; restarted when it has run out of work and more came
-      if (waiting > 0 && live_ctas == 0) {
-        const int rc = (sv->precision == 64) ? serve_launch<double>(sv, 0, sv->grid) : serve_launch<float>(sv, 0, sv->grid);
-        if (rc) sv->last_error = g_err;
+      // instances of every resident CTA slot: the tiles of all live requests
+      // share them.  Their CTAs return after a budget of tasks, so a next
+      // instance is kept queued behind the running one while requests wait;
+      // the loop's streams have the lowest priority, so that the blocks of
+      // other kernels (a one-CTA-per-request loop, plain filters) take the
+      // slots they free first.
+      int live_inst = 0;
+      for (int i = 0; i < plomgpu_server::kLoops; ++i) live_inst += sv->loop_live[i] ? 1 : 0;
+      if (waiting > 0 && live_inst < 2) {
+        for (int i = 0; i < plomgpu_server::kLoops; ++i) {
+          if (sv->loop_live[i]) continue;
+          const int rc =
+              (sv->precision == 64) ? serve_launch<double>(sv, i, sv->grid) : serve_launch<float>(sv, i, sv->grid);
+          if (rc) sv->last_error = g_err;
+          break;
+        }
       }
     } else if (waiting > live_ctas && live_ctas < sv->grid) {
       for (int i = 0; i < plomgpu_server::kLoops; ++i) {

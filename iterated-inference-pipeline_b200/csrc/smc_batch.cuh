@@ -165,7 +165,9 @@ struct FilterJob {
   const double* x0;       // [S]
 };
 
-template <class T, int V, bool DRIFT, int BT>
+// PPT particles per thread are advanced together (particles j, j + BT, ...):
+// their independent Philox / Box-Muller chains fill each other's latency.
+template <class T, int V, bool DRIFT, int BT, int PPT = 1>
 __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const FilterJob& job, const BatchWs<T>& ws,
                            const size_t ld, double* out_ll, int* out_nf, double* out_ess) {
   const int J = job.J;
@@ -203,46 +205,60 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
     const T* Xp = ws.X[cur];
     T* Xn = ws.X[cur ^ 1];
     LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
-    for (int j = threadIdx.x; j < J; j += BT) {
-      const uint32_t src = resampled ? ws.anc[j] : (uint32_t)j;
-      RegState<T, M::S> x;
+    for (int j0 = threadIdx.x; j0 < J; j0 += BT * PPT) {
+      // a lane past the end recomputes the last particle and stores nothing
+      int jj[PPT];
+      RegState<T, M::S> x[PPT];
 #pragma unroll
-      for (int w = 0; w < M::OFF_INC; ++w) x[w] = Xp[(size_t)w * ld + src];
+      for (int q = 0; q < PPT; ++q) {
+        jj[q] = min(j0 + q * BT, J - 1);
+        const uint32_t src = resampled ? ws.anc[jj[q]] : (uint32_t)jj[q];
 #pragma unroll
-      for (int w = M::OFF_INC; w < M::S; ++w) x[w] = T(0);
+        for (int w = 0; w < M::OFF_INC; ++w) x[q][w] = Xp[(size_t)w * ld + src];
+#pragma unroll
+        for (int w = M::OFF_INC; w < M::S; ++w) x[q][w] = T(0);
+      }
       for (int k = 0; k < K; ++k) {
         const int sub = sub0 + k;
         e.cov_ = a.cov_cac + (size_t)sub * M::N_COV_CAC * M::N_CAC;
         const T t = (T)__ldg(a.t_sub + sub);
-        PhiloxDraws<T, V> d;
-        d.key = key;
-        d.j = (uint32_t)j;
-        d.n = (uint32_t)n;
-        d.sub = (uint32_t)k;
-        M::template step<V, DRIFT, T>(x, t, dt, e, d);
+#pragma unroll
+        for (int q = 0; q < PPT; ++q) {
+          PhiloxDraws<T, V> d;
+          d.key = key;
+          d.j = (uint32_t)jj[q];
+          d.n = (uint32_t)n;
+          d.sub = (uint32_t)k;
+          M::template step<V, DRIFT, T>(x[q], t, dt, e, d);
+        }
       }
 #pragma unroll
-      for (int w = 0; w < M::OFF_INC; ++w) Xn[(size_t)w * ld + j] = x[w];
-      if (weigh) {
-        double obs[M::N_TS];
-        M::template proj2obs<T>(x, obs);
-        double ll = 0.0;
-        int fl = 0;
+      for (int q = 0; q < PPT; ++q) {
+        const int j = j0 + q * BT;
+        if (j >= J) continue;
 #pragma unroll
-        for (int ts = 0; ts < M::N_TS; ++ts) {
-          const double yy = y[ts];
-          if (isnan(yy)) continue;
-          const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
-          const double var = M::obs_var(obs[ts], ts, t_obs, oe);
-          ll += plomrt::log_like_term_p<T>(yy, mu, var, a.like_min, &fl);
-        }
-        const T l = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
-        ws.lw[j] = l;
-        if (weight_fails(l, a.thresh)) {
-          acc.nfail += 1;
-        } else {
-          LseAcc b = {(double)l, 1.0, 1.0, 0};
-          acc = lse_merge(acc, b);
+        for (int w = 0; w < M::OFF_INC; ++w) Xn[(size_t)w * ld + j] = x[q][w];
+        if (weigh) {
+          double obs[M::N_TS];
+          M::template proj2obs<T>(x[q], obs);
+          double ll = 0.0;
+          int fl = 0;
+#pragma unroll
+          for (int ts = 0; ts < M::N_TS; ++ts) {
+            const double yy = y[ts];
+            if (isnan(yy)) continue;
+            const double mu = M::obs_mean(obs[ts], ts, t_obs, oe);
+            const double var = M::obs_var(obs[ts], ts, t_obs, oe);
+            ll += plomrt::log_like_term_p<T>(yy, mu, var, a.like_min, &fl);
+          }
+          const T l = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
+          ws.lw[j] = l;
+          if (weight_fails(l, a.thresh)) {
+            acc.nfail += 1;
+          } else {
+            LseAcc b = {(double)l, 1.0, 1.0, 0};
+            acc = lse_merge(acc, b);
+          }
         }
       }
     }
@@ -322,7 +338,7 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
   }
 }
 
-template <class T, int V, bool DRIFT, int BT>
+template <class T, int V, bool DRIFT, int BT, int PPT = 1>
 __global__ void __launch_bounds__(BT) k_batch(const BatchArgs<T> a) {
   __shared__ CtaShared<T, BT> sh;
   if constexpr (M::COUPLED) {
@@ -348,7 +364,8 @@ __global__ void __launch_bounds__(BT) k_batch(const BatchArgs<T> a) {
     job.par_cac = a.par_cac + (size_t)f * M::N_PAR_PROC * M::N_CAC;
     job.par_ts = a.par_ts + (size_t)f * M::N_PAR_OBS * M::N_TS;
     job.x0 = a.x0 + (size_t)f * M::S;
-    cta_filter<T, V, DRIFT, BT>(sh, a, job, ws, ld, a.loglik + f, a.n_all_fail + f, a.ess_min ? a.ess_min + f : nullptr);
+    cta_filter<T, V, DRIFT, BT, PPT>(sh, a, job, ws, ld, a.loglik + f, a.n_all_fail + f,
+                                     a.ess_min ? a.ess_min + f : nullptr);
   }
 }
 

@@ -1008,18 +1008,19 @@ __global__ void __launch_bounds__(BT) k_search(const double* __restrict__ C, int
 
 // ------------------------------------------------------------------ tiled resampling
 // weight() + systematic_sampling() (model_builder/C/core/smc.c:27-112) over
-// tiles of TILE consecutive particles, in two launches:
+// tiles of TILE consecutive particles, in three launches:
 //   k_weight_tiles  per tile: (max, sum exp(l - max), sum exp(2 (l - max)),
 //                   failures); the last block folds them in tile order
 //                   (llike, ESS, all-fail rule, systematic points) and lays out
 //                   the exclusive prefix P[b] of the tiles' normalised weights;
-//   k_resample      per tile: the cumulative weights of its particles
-//                   C_i = P[b] + (prefix of exp(l - max_b)) * exp(max_b - max) / sum
-//                   in shared memory, and the ancestor of every systematic
-//                   point P[b] < point_j <= P[b+1] (first i with C_i >= point_j).
-// The points of a tile are found from the closed form of the points, so no
-// cumulative-weight array goes to memory and no search crosses tiles; every
-// reduction runs in a fixed order (results do not depend on timing).
+//   k_cum_tiles     per tile: the cumulative weights of its particles
+//                   C_i = P[b] + (prefix of exp(l - max_b)) * exp(max_b - max) / sum;
+//   k_search_tiles  per tile of points: the ancestor of every systematic point
+//                   (first i with C_i >= point_j).
+// The tile prefixes come from the fold (no look-back across tiles), the
+// points are placed by a search over all cumulative weights (balanced however
+// the weights concentrate), and every reduction runs in a fixed order
+// (results do not depend on timing).
 template <class T>
 __device__ __forceinline__ double surviving_exp(T l, double thresh, double m) {
   return weight_fails(l, thresh) ? 0.0 : exp((double)l - m);
@@ -1067,10 +1068,12 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
                            double* ess_out, LseAcc* sh, double* shd) {
   const int chunk = (ntiles + BT - 1) / BT;
   const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
+  // the partials of the other blocks are read from L2 (written before their
+  // ticket, after a fence)
   LseAcc a = {-INFINITY, 0.0, 0.0, 0};
   for (int b = b0; b < b1; ++b) {
-    volatile const LseAcc* p = part + b;
-    LseAcc v = {p->m, p->s1, p->s2, p->nfail};
+    const LseAcc* p = part + b;
+    LseAcc v = {__ldcg(&p->m), __ldcg(&p->s1), __ldcg(&p->s2), __ldcg(&p->nfail)};
     a = lse_merge(a, v);
   }
   a = block_lse_all<BT>(a, sh);
@@ -1080,8 +1083,8 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   double tot = 0.0;
   if (!all_fail) {
     for (int b = b0; b < b1; ++b) {
-      volatile const LseAcc* p = part + b;
-      if (p->s1 > 0.0) tot += p->s1 * (exp(p->m - a.m) / a.s1);
+      const double s1b = __ldcg(&part[b].s1);
+      if (s1b > 0.0) tot += s1b * (exp(__ldcg(&part[b].m) - a.m) / a.s1);
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1107,8 +1110,8 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   for (int b = b0; b < b1; ++b) {
     P[b] = run;
     if (!all_fail) {
-      volatile const LseAcc* p = part + b;
-      if (p->s1 > 0.0) run += p->s1 * (exp(p->m - a.m) / a.s1);
+      const double s1b = __ldcg(&part[b].s1);
+      if (s1b > 0.0) run += s1b * (exp(__ldcg(&part[b].m) - a.m) / a.s1);
     }
   }
   if (b1 == ntiles && b0 < b1) P[ntiles] = run;
@@ -1194,70 +1197,27 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
                  ess_out, sh, shd);
 }
 
-// first j in [0, J] whose systematic point exceeds v (J when none): the
-// points are U + j / J up to the rounding of the reference's running sum, so
-// the closed-form guess is off by at most one step; a bounded walk fixes it
-// and a binary search takes over if the walk runs long.
-__device__ __forceinline__ int first_point_above(const plomrt::SysSeg* seg, int ns, int J, double U, double v) {
-  double g = floor((v - U) * (double)J) + 1.0;
-  int j = g < 0.0 ? 0 : (g > (double)J ? J : (int)g);
-  for (int it = 0; it < 64; ++it) {
-    if (j > 0 && plomrt::systematic_point(seg, ns, j - 1) > v) {
-      --j;
-    } else if (j < J && !(plomrt::systematic_point(seg, ns, j) > v)) {
-      ++j;
-    } else {
-      return j;
-    }
-  }
-  int lo = 0, hi = J;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (plomrt::systematic_point(seg, ns, mid) > v) hi = mid; else lo = mid + 1;
-  }
-  return lo;
-}
-
-// Ancestors of the systematic points of tile b (all threads of the block
-// call it; `sc` is the block's scratch).
+// Cumulative normalised weights of tile b: C_i = P[b] + (prefix of
+// exp(l - max_b) in particle order) * exp(max_b - max) / sum, written to C
+// (all threads of the block call it).
 template <class T, int BT, int IPT>
-__device__ void resample_tile(const T* __restrict__ lw, int J, double thresh, const LseAcc* __restrict__ part,
-                              const double* __restrict__ P, const StepState* st, int b, int ntiles,
-                              uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, TileScratch<BT, IPT>& sc) {
+__device__ void cum_tile(const T* __restrict__ lw, int J, double thresh, const LseAcc* __restrict__ part,
+                         const double* __restrict__ P, const StepState* st, int b, double* __restrict__ C,
+                         TileScratch<BT, IPT>& sc) {
   constexpr int TILE = BT * IPT;
   const int base = b * TILE;
   const int n_in = min(TILE, J - base);
-  if (threadIdx.x == 0) {
-    sc.ns = st->nseg;
-    sc.fail = st->all_fail;
-    sc.lastpos = -1;
-  }
-  __syncthreads();
-  if (sc.fail || sc.ns == 0) {
-    // every particle failed (or the point table overflowed): identity
-    for (int i = threadIdx.x; i < n_in; i += BT) {
-      anc[base + i] = (uint32_t)(base + i);
-      if (anc_hist) anc_hist[base + i] = (uint32_t)(base + i);
-    }
-    return;
-  }
-  const int ns = sc.ns;
-  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = st->seg[i];
-  // cumulative weights of the tile, rows of BT particles in order
-  const double mb = part[b].m;
-  const double f = (part[b].s1 > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
-  const double Pb = P[b];
+  if (st->all_fail) return;
+  const double mb = __ldcg(&part[b].m);
+  const double s1b = __ldcg(&part[b].s1);
+  const double f = (s1b > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
+  const double Pb = __ldcg(P + b);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double carry = 0.0;
-  int lastpos = -1;
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const int ii = k * BT + threadIdx.x;
-    double p = 0.0;
-    if (ii < n_in) {
-      p = surviving_exp(lw[base + ii], thresh, mb);
-      if (p > 0.0) lastpos = ii;
-    }
+    const double p = (ii < n_in) ? surviving_exp(lw[base + ii], thresh, mb) : 0.0;
     double v = p;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -1277,46 +1237,65 @@ __device__ void resample_tile(const T* __restrict__ lw, int J, double thresh, co
     }
     __syncthreads();
     const double incl = carry + ((warp > 0) ? sc.swarp[warp - 1] : 0.0) + v;
-    sc.sC[ii] = Pb + incl * f;
+    if (ii < n_in) C[base + ii] = Pb + incl * f;
     carry += sc.swarp[BT / 32 - 1];
     __syncthreads();
   }
-  if (lastpos >= 0) atomicMax(&sc.lastpos, lastpos);
+}
+
+// Ancestors of the systematic points j of one tile of points (TILE
+// consecutive j): the first particle i with C_i >= point_j (smc.c:105-108),
+// the last particle when rounding leaves a point above every C (the
+// reference reads on past the array); identity when every particle failed.
+template <int BT, int IPT>
+__device__ void search_tile(const double* __restrict__ C, int J, const StepState* st, int b,
+                            uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, TileScratch<BT, IPT>& sc) {
+  constexpr int TILE = BT * IPT;
   if (threadIdx.x == 0) {
-    const double U = st->U;
-    sc.jlo = (b == 0) ? 0 : first_point_above(sc.seg, ns, J, U, Pb);
-    sc.jhi = (b == ntiles - 1) ? J : first_point_above(sc.seg, ns, J, U, P[b + 1]);
+    sc.ns = st->nseg;
+    sc.fail = st->all_fail;
   }
   __syncthreads();
-  const int jlo = sc.jlo, jhi = sc.jhi;
-  // past the tile's last cumulative weight (rounding): its last surviving
-  // particle, and the last particle for the last tile (the reference reads on
-  // past the array there)
-  const int clamp = (b == ntiles - 1 || sc.lastpos < 0) ? n_in - 1 : sc.lastpos;
-  for (int j = jlo + threadIdx.x; j < jhi; j += BT) {
-    const double ran = plomrt::systematic_point(sc.seg, ns, j);
-    int lo = 0, hi = n_in;
-    while (lo < hi) {  // first i with !(ran > C[i])  (smc.c:105-108)
-      const int mid = (lo + hi) >> 1;
-      if (ran > sc.sC[mid]) lo = mid + 1; else hi = mid;
+  const int ns = sc.ns;
+  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = st->seg[i];
+  __syncthreads();
+  const int j1 = min(J, (b + 1) * TILE);
+  for (int j = b * TILE + threadIdx.x; j < j1; j += BT) {
+    uint32_t r;
+    if (sc.fail || ns == 0) {
+      r = (uint32_t)j;
+    } else {
+      const double ran = plomrt::systematic_point(sc.seg, ns, j);
+      int lo = 0, hi = J - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (ran > __ldg(C + mid)) lo = mid + 1; else hi = mid;
+      }
+      r = (uint32_t)lo;
     }
-    const uint32_t a_ = (uint32_t)(base + (lo < n_in ? lo : clamp));
-    anc[j] = a_;
-    if (anc_hist) anc_hist[j] = a_;
+    anc[j] = r;
+    if (anc_hist) anc_hist[j] = r;
   }
 }
 
 template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_resample(const T* __restrict__ lw, int J, double thresh,
-                                                 const LseAcc* __restrict__ part, const double* __restrict__ P,
-                                                 const StepState* st, uint32_t* __restrict__ anc,
-                                                 uint32_t* __restrict__ anc_hist) {
+__global__ void __launch_bounds__(BT) k_cum_tiles(const T* __restrict__ lw, int J, double thresh,
+                                                  const LseAcc* __restrict__ part, const double* __restrict__ P,
+                                                  const StepState* st, double* __restrict__ C) {
   __shared__ TileScratch<BT, IPT> sc;
   const int ntiles = gridDim.x;
   const int r = blockIdx.y;
-  resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, thresh, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
-                            st + r, blockIdx.x, ntiles, anc + (size_t)r * J,
-                            anc_hist ? anc_hist + (size_t)r * J : nullptr, sc);
+  cum_tile<T, BT, IPT>(lw + (size_t)r * J, J, thresh, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1), st + r,
+                       blockIdx.x, C + (size_t)r * J, sc);
+}
+
+template <int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_search_tiles(const double* __restrict__ C, int J, const StepState* st,
+                                                     uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
+  __shared__ TileScratch<BT, IPT> sc;
+  const int r = blockIdx.y;
+  search_tile<BT, IPT>(C + (size_t)r * J, J, st + r, blockIdx.x, anc + (size_t)r * J,
+                       anc_hist ? anc_hist + (size_t)r * J : nullptr, sc);
 }
 
 // ------------------------------------------------------------------ helpers

@@ -126,8 +126,8 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
 //   propagate(n)  the tile's particles over interval n (gather from the
 //                 ancestors, substeps, log-weights) and the tile's
 //                 log-sum-exp partial;
-//   resample(n)   the ancestors of the systematic points that fall in the
-//                 tile (resample_tile).
+//   cumulate(n)   the cumulative normalised weights of the tile (cum_tile);
+//   search(n)     the ancestors of the tile's systematic points (search_tile).
 // The CTA that finishes the last tile of a phase does the phase's serial
 // part itself (the fold of the partials: llike, ESS, all-fail rule,
 // systematic points, tile prefixes) and publishes the next phase; nothing
@@ -145,7 +145,7 @@ struct TileReq {
                              // order << 12, so a stale read of a reused workspace never matches
   unsigned done;             // tiles of the current phase finished
   int n;                     // interval of the current phase
-  int kind;                  // 0 propagate, 1 resample
+  int kind;                  // 0 propagate, 1 cumulate, 2 search
   int cur;                   // generation holding the particles before interval n
   int resampled;             // the ancestors of interval n - 1 apply (else identity)
   int slot;                  // ring slot of the request (its result)
@@ -163,6 +163,7 @@ struct TileReqWs {
   double* P;
   T* lw;
   uint32_t* anc;
+  double* C;
   T* X[2];
   T* par_cac;
   double* par_ts;
@@ -176,7 +177,8 @@ __host__ __device__ inline size_t tile_req_bytes(int J) {
   const size_t nt = (size_t)((J + BT - 1) / BT);
   const size_t mj = (size_t)((J + 31) & ~31);
   return ws_align(sizeof(TileReq)) + ws_align(nt * sizeof(LseAcc)) + ws_align((nt + 1) * sizeof(double)) +
-         ws_align(mj * sizeof(T)) + ws_align(mj * sizeof(uint32_t)) + 2 * ws_align((size_t)M::S * mj * sizeof(T)) +
+         ws_align(mj * sizeof(T)) + ws_align(mj * sizeof(uint32_t)) + ws_align(mj * sizeof(double)) +
+         2 * ws_align((size_t)M::S * mj * sizeof(T)) +
          ws_align((size_t)kServeParCac * sizeof(T)) + ws_align((size_t)kServeParTs * sizeof(double)) +
          ws_align((size_t)M::S * sizeof(double));
 }
@@ -197,6 +199,8 @@ __device__ inline TileReqWs<T> tile_req_ws(unsigned char* base, int J) {
   p += ws_align(mj * sizeof(T));
   w.anc = reinterpret_cast<uint32_t*>(p);
   p += ws_align(mj * sizeof(uint32_t));
+  w.C = reinterpret_cast<double*>(p);
+  p += ws_align(mj * sizeof(double));
   w.X[0] = reinterpret_cast<T*>(p);
   p += ws_align((size_t)M::S * mj * sizeof(T));
   w.X[1] = reinterpret_cast<T*>(p);
@@ -221,7 +225,8 @@ constexpr size_t serve_tiles_smem() {
 template <class T, int V, bool DRIFT, int BT>
 __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeSlot* slots, const int* ring_map,
                                                     int ring, ServeCtl* ctl, unsigned long long* head,
-                                                    unsigned char* pool, long long* live, long long idle_limit) {
+                                                    unsigned char* pool, long long* live, long long idle_limit,
+                                                    int task_budget) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // the tile scratch sits after the coupling / parameter tables
   TileScratch<BT, 1>& sc = *reinterpret_cast<TileScratch<BT, 1>*>(
@@ -237,8 +242,13 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
     T* s_coup = reinterpret_cast<T*>(smem_raw);
     for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = a.coupling[i];
   }
+  // after task_budget tasks a CTA returns (the host keeps a next instance
+  // queued), so that its SM slot can go to other kernels between tasks
+  int tasks = 0;
   for (;;) {
     __syncthreads();
+    if (task_budget > 0 && tasks >= task_budget) return;
+    ++tasks;
     if (threadIdx.x < 32) {
       // warp 0 polls: lane l looks at live entries l and l + 32 in parallel
       const int lane = threadIdx.x;
@@ -279,20 +289,20 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         if (who) {
           int got = 0;
           if (lane == __ffs(who) - 1) {
+            // fetch-and-add hands out the tiles of the phase one by one; a
+            // count past the tiles (the phase is taken, or the workspace was
+            // reused by a newer request after the read above) claims nothing
             TileReq* q = reinterpret_cast<TileReq*>(pool + my_off);
-            if (atomicCAS(&q->phase, my_v, my_v + 1ull) == my_v) {
-              __threadfence();
-              // a claim past the tiles (a count read before the workspace was
-              // reused by a newer request) is dropped
-              if ((int)(my_v & 0xffffffffull) < *(volatile int*)&q->ntiles) {
-                s_off = my_off;
-                s_tile = (int)(my_v & 0xffffffffull);
-                got = 1;
-              }
+            const unsigned long long v = atomicAdd(&q->phase, 1ull);
+            __threadfence();
+            if ((int)(v & 0xffffffffull) < *(volatile int*)&q->ntiles) {
+              s_off = my_off;
+              s_tile = (int)(v & 0xffffffffull);
+              got = 1;
             }
           }
           if (__shfl_sync(0xffffffffu, got, __ffs(who) - 1)) break;
-          continue;  // another CTA took it: look again
+          continue;  // look again
         }
         // else the next published request, if a live entry is free
         const unsigned freem = __ballot_sync(0xffffffffu, free_entry >= 0);
@@ -420,8 +430,10 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         acc = block_lse_all<BT>(acc, sc.lse);
         if (threadIdx.x == 0) w.part[tile] = acc;
       }
+    } else if (kind == 1) {
+      cum_tile<T, BT, 1>(w.lw, J, a.thresh, w.part, w.P, &q->st, tile, w.C, sc);
     } else {
-      resample_tile<T, BT, 1>(w.lw, J, a.thresh, w.part, w.P, &q->st, tile, ntiles, w.anc, nullptr, sc);
+      search_tile<BT, 1>(w.C, J, &q->st, tile, w.anc, nullptr, sc);
     }
     // the last tile of the phase does its serial part and publishes the next phase
     __threadfence();
@@ -445,6 +457,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         next_n = n + 1;
         if (next_n == T_obs) finished = true;
       }
+    } else if (kind == 1) {
+      next_kind = 2;
     } else {
       next_kind = 0;
       next_res = 1;

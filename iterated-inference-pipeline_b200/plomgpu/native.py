@@ -54,7 +54,8 @@ class BatchDesc(C.Structure):
                 ('seed', _P(C.c_uint64)), ('max_obs', C.c_int), ('n_sub', _ip), ('t_sub', _dp), ('t_obs', _dp),
                 ('dt', C.c_double), ('cov_cac', _dp), ('cov_ts', _dp), ('coupling', _dp), ('drift_group', _ip),
                 ('drift_ngroups', _ip), ('drift_bt', _P(BackTransform)), ('drift_vol', _dp), ('noises_off', C.c_int),
-                ('filter', C.c_int), ('like_min', C.c_double), ('precision', C.c_int), ('block_threads', C.c_int)]
+                ('filter', C.c_int), ('like_min', C.c_double), ('precision', C.c_int), ('block_threads', C.c_int),
+                ('particles_per_thread', C.c_int)]
 
 
 class MifDesc(C.Structure):
@@ -228,7 +229,7 @@ def _declare(lib):
     lib.plomgpu_batch_results.argtypes = [C.c_void_p, _dp, _ip, _dp]
     lib.plomgpu_batch_stream.argtypes = [C.c_void_p]
     lib.plomgpu_batch_stream.restype = C.c_void_p
-    lib.plomgpu_batch_config.argtypes = [C.c_void_p, _ip, _ip]
+    lib.plomgpu_batch_config.argtypes = [C.c_void_p, _ip, _ip, _ip]
     lib.plomgpu_batch_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_batch_destroy.restype = None
     lib.plomgpu_batch_run.argtypes = [_P(BatchDesc), _dp, _ip]
@@ -398,7 +399,7 @@ class Plan(object):
 class Batch(object):
     """Many filters of one model in one persistent launch (plomgpu_batch_*)."""
 
-    def __init__(self, engine, bp, precision=32, block_threads=0):
+    def __init__(self, engine, bp, precision=32, block_threads=0, particles_per_thread=0):
         self.engine = engine
         self.lib = engine.lib
         self.bp = bp
@@ -442,7 +443,7 @@ class Batch(object):
             cov_ts=_ptr(cov_ts, _dp), coupling=_ptr(coup, _dp), drift_group=_ptr(dg, _ip),
             drift_ngroups=_ptr(dng, _ip), drift_bt=C.cast(bts, _P(BackTransform)), drift_vol=_ptr(dvol, _dp),
             noises_off=base.noises_off, filter=1 if base.filter else 0, like_min=base.like_min,
-            precision=precision, block_threads=block_threads)
+            precision=precision, block_threads=block_threads, particles_per_thread=particles_per_thread)
         self.p = C.c_void_p()
         check(self.lib, self.lib.plomgpu_batch_create(C.byref(self.desc), C.byref(self.p)))
 
@@ -463,9 +464,10 @@ class Batch(object):
 
     @property
     def config(self):
-        bt, grid = C.c_int(), C.c_int()
-        check(self.lib, self.lib.plomgpu_batch_config(self.p, C.byref(bt), C.byref(grid)))
-        return bt.value, grid.value
+        """(threads per block, particles per thread, CTAs) chosen by the autotuner."""
+        bt, ppt, grid = C.c_int(), C.c_int(), C.c_int()
+        check(self.lib, self.lib.plomgpu_batch_config(self.p, C.byref(bt), C.byref(ppt), C.byref(grid)))
+        return bt.value, ppt.value, grid.value
 
     def close(self):
         if self.p:

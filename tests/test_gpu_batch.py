@@ -28,12 +28,13 @@ def test_batch_fp64_matches_oracle_per_filter():
         assert nf[i] == o.n_all_fail
 
 
+@pytest.mark.parametrize('ppt', [1, 2])
 @pytest.mark.parametrize('bt', [128, 256, 512])
-def test_batch_fp32_matches_single_filter_path(bt):
+def test_batch_fp32_matches_single_filter_path(bt, ppt):
     eng = models.engine('sir')
     bp = small_batch(n=16, seed=9)
-    b = Batch(eng, bp, precision=32, block_threads=bt)
-    assert b.config[0] == bt
+    b = Batch(eng, bp, precision=32, block_threads=bt, particles_per_thread=ppt)
+    assert b.config[:2] == (bt, ppt)
     b.launch()
     ll, _, _ = b.results()
     b.launch()
@@ -49,8 +50,8 @@ def test_batch_autotune_picks_a_candidate_and_handles_uneven_sizes():
     eng = models.engine('sir')
     bp = workloads.sir_batch(n_sets=300, seed=10, J_range=(256, 4096), T_range=(52, 104))
     b = Batch(eng, bp, precision=32)
-    bt, grid = b.config
-    assert bt in (128, 256, 512) and grid >= 148
+    bt, ppt, grid = b.config
+    assert bt in (128, 256, 512) and ppt in (1, 2) and grid >= 148
     b.launch()
     ll, nf, ess = b.results()
     b.close()
