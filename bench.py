@@ -64,6 +64,8 @@ def parse():
     ap.add_argument('--e2e-runs', type=int, default=3, help='one-shot C-ABI calls timed for e2e (0: skip)')
     ap.add_argument('--error-samples', type=int, default=26,
                     help='intervals sampled for loglik_error (0: skip)')
+    ap.add_argument('--serve-load', type=float, default=0.6,
+                    help='serve: offered load, as a fraction of the measured saturation rate, of the latency runs')
     ap.add_argument('--plan-pool', type=int, default=0, help='serve: run the shared-memory model on a pool of this '
                     'many concurrent plans instead of the tiled device loop (0: device loop)')
     return ap.parse_args()
@@ -391,6 +393,42 @@ def run_mif(args):
     return 0
 
 
+def serve_class_profile(c, rng, load):
+    """One request class on its server alone: the saturation rate (a backlog of requests submitted at
+    once, completed per second) and the p50 / p99 latency of Poisson arrivals at ``load`` x that rate."""
+    import numpy as np
+    sv, J, p = c['server'], c['J'], c['prob']
+    n_sat = 64 if J > 5000 else 512
+    t0 = time.perf_counter()
+    ts = [sv.submit(J, par_cac=p.par_cac * np.exp(0.02 * rng.standard_normal(p.par_cac.shape)), seed=50000 + i)
+          for i in range(n_sat)]
+    for t in ts:
+        sv.wait(t, 600.0)
+    sat = n_sat / (time.perf_counter() - t0)
+    rate = load * sat
+    n_req = 48 if J > 5000 else 400
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    pending, lat = [], []
+    start = time.perf_counter()
+    k = 0
+    while k < n_req or pending:
+        now = time.perf_counter() - start
+        if k < n_req and now >= arrivals[k]:
+            pending.append(sv.submit(J, seed=60000 + k))
+            k += 1
+            continue
+        for t in list(pending):
+            r = sv.poll(t)
+            if r is not None:
+                lat.append(r[2])
+                pending.remove(t)
+        time.sleep(1e-4)
+    pct = lambda q: float(np.percentile(lat, q))
+    return {'saturation_requests_per_s': sat, 'saturation_particle_steps_per_s': sat * J * p.n_obs,
+            'load': load, 'offered_requests_per_s': rate, 'requests': n_req,
+            'latency_s': {'p50': pct(50), 'p99': pct(99)}}
+
+
 def run_serve(args, window_s=0.25, rate=2000.0):
     """Served pMCMC likelihoods: asynchronous random-walk chains submit requests as
     Poisson arrivals; results feed Metropolis-Hastings accept / reject."""
@@ -459,6 +497,7 @@ def run_serve(args, window_s=0.25, rate=2000.0):
     t_total = time.perf_counter() - t_start
     stats = dict((cl, c['server'].stats()) for cl, c in classes.items())
     n_req = sum(len(v) for v in lat.values())
+    per_class = dict((cl, serve_class_profile(c, rng, args.serve_load)) for cl, c in classes.items())
     psteps = sum(len(lat[cl]) * classes[cl]['J'] * classes[cl]['prob'].n_obs for cl in lat)
     # plain filter per request: one-shot plomgpu_smc_run, sequential, on a sample
     plain = {}
@@ -484,6 +523,7 @@ def run_serve(args, window_s=0.25, rate=2000.0):
             'latency_s': dict((cl, {'p50': pct(lat[cl], 50), 'p99': pct(lat[cl], 99), 'n': len(lat[cl])}) for cl in lat),
             'plain_filter_per_request': {'latency_s': plain, 'total_s_for_same_requests': plain_time,
                                          'speedup_of_serving': plain_time / t_total},
+            'per_class_alone': per_class,
             'server_stats': stats, 'acceptance': [c['accepted'] / max(c['done'], 1) for c in chains],
             'clocks': clk.summary()}
     print(json.dumps(line))

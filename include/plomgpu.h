@@ -382,6 +382,8 @@ typedef struct plomgpu_server_opts {
     int precision;          /* 32 or 64 */
     int use_plan_pool;      /* 1: models with shared-memory particles run on the plan pool instead of the
                              * device loop (one captured whole filter per request, for comparison) */
+    int task_budget;        /* tiles a CTA of the tiled loop runs before it returns and frees its SM slot
+                             * for other kernels (0: 64; < 0: no limit) */
 } plomgpu_server_opts;
 
 typedef struct plomgpu_server_stats {

@@ -416,6 +416,17 @@ int enqueue_filter(plomgpu_plan* p) {
     // the random walk applies where the previous interval resampled (C/mif/mif.c:190-191)
     a.sd_mut = (p->mif && n > 0 && p->weigh[n - 1]) ? p->sd_mut + (size_t)(n - 1) * p->Q : nullptr;
     a.x0_rep = nullptr;
+    // the weighting in the propagate epilogue when its blocks are the resampling tiles
+    const bool fuse = a.weigh && !p->ode && !p->mif && R == 1 && kp.per_block == kTileRes && kBtRes == kp.bt;
+    a.fused = fuse ? 1 : 0;
+    a.fw_part = p->part;
+    a.fw_P = p->P;
+    a.fw_st = p->st;
+    a.fw_acc = p->acc;
+    a.fw_log_like_min = p->log_like_min;
+    a.fw_U_crn = p->crn_tab ? p->crn_u[n] : -1.0;
+    a.fw_llike = p->llike;
+    a.fw_ess = p->ess;
     crn_off += RJ * p->n_sub[n] * D;
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
     if (p->ode) {
@@ -440,9 +451,12 @@ int enqueue_filter(plomgpu_plan* p) {
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
       const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
-      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u, p->llike,
-          p->ess, p->n_obs);
+      if (!a.fused) {
+        k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+            (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
+            p->llike, p->ess, p->n_obs);
+        ++kernels;
+      }
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
                                                             p->thresh, p->st, p->theta_hat, p->vt_add, p->Q, n,
@@ -454,7 +468,7 @@ int enqueue_filter(plomgpu_plan* p) {
                                                                            p->P, p->st, p->C);
       k_search_tiles<kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
           p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
-      kernels += 3;
+      kernels += 2;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
         ++kernels;
@@ -1903,6 +1917,7 @@ int plomgpu_server_create(const plomgpu_smc_desc* d, const plomgpu_server_opts* 
   sv->max_J = o->max_J;
   sv->ring = o->ring_slots > 0 ? o->ring_slots : 1024;
   sv->plan_pool = o->plan_pool > 0 ? o->plan_pool : 4;
+  sv->task_budget = o->task_budget == 0 ? 64 : (o->task_budget < 0 ? 0 : o->task_budget);
   if (kSmem && o->use_plan_pool) {
     sv->persistent = false;
     sv->tiled = false;

@@ -68,7 +68,7 @@ class MifDesc(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [('max_J', C.c_int), ('memory_budget', C.c_double), ('ring_slots', C.c_int), ('plan_pool', C.c_int),
-                ('precision', C.c_int), ('use_plan_pool', C.c_int)]
+                ('precision', C.c_int), ('use_plan_pool', C.c_int), ('task_budget', C.c_int)]
 
 
 class ServerStats(C.Structure):
@@ -599,12 +599,12 @@ class Server(object):
     """plomgpu_server_*: concurrent likelihood requests on one data set."""
 
     def __init__(self, engine, problem, max_J, memory_budget=0.0, ring_slots=0, plan_pool=0, precision=32,
-                 use_plan_pool=False):
+                 use_plan_pool=False, task_budget=0):
         self.engine = engine
         self.lib = engine.lib
         self.h = DescHolder(problem, precision=precision)
         self.opts = ServerOpts(int(max_J), float(memory_budget), int(ring_slots), int(plan_pool), int(precision),
-                               1 if use_plan_pool else 0)
+                               1 if use_plan_pool else 0, int(task_budget))
         self.p = C.c_void_p()
         check(self.lib, self.lib.plomgpu_server_create(C.byref(self.h.desc), C.byref(self.opts), C.byref(self.p)))
 
