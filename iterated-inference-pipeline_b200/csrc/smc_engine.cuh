@@ -1042,24 +1042,42 @@ struct TileScratch {
   int ns, fail, jlo, jhi, lastpos, last;
 };
 
-// (max, sum exp(l - max), sum exp(2 (l - max)), failures) of one thread's
-// log-weights merged over the block (fixed order); every thread gets it.
+// (max, sum exp(l - max), sum exp(2 (l - max)), failures) of the threads'
+// partials merged over the block (fixed order); every thread gets it.  The
+// block maximum first, then every partial rescaled to it once and the sums
+// added: one exponential per thread instead of one per merge of a tree.
 template <int BT>
 __device__ __forceinline__ LseAcc block_lse_all(LseAcc a, LseAcc* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double m = a.m;
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+  if (lane == 0) sh[warp].m = m;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
+  m = sh[0].m;
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-    if (threadIdx.x == 0) sh[0] = a;
+  for (int w = 1; w < BT / 32; ++w) m = fmax(m, sh[w].m);
+  const double f = (a.s1 > 0.0) ? exp(a.m - m) : 0.0;
+  double s1 = a.s1 * f, s2 = a.s2 * f * f;
+  int nf = a.nfail;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
+    nf += __shfl_xor_sync(0xffffffffu, nf, off);
   }
   __syncthreads();
-  a = sh[0];
+  if (lane == 0) sh[warp] = LseAcc{m, s1, s2, nf};
   __syncthreads();
-  return a;
+  LseAcc r = {m, 0.0, 0.0, 0};
+#pragma unroll
+  for (int w = 0; w < BT / 32; ++w) {
+    r.s1 += sh[w].s1;
+    r.s2 += sh[w].s2;
+    r.nfail += sh[w].nfail;
+  }
+  __syncthreads();
+  return r;
 }
 
 // The fold of the tile partials by one block (all threads call it): the
