@@ -416,17 +416,6 @@ int enqueue_filter(plomgpu_plan* p) {
     // the random walk applies where the previous interval resampled (C/mif/mif.c:190-191)
     a.sd_mut = (p->mif && n > 0 && p->weigh[n - 1]) ? p->sd_mut + (size_t)(n - 1) * p->Q : nullptr;
     a.x0_rep = nullptr;
-    // the weighting in the propagate epilogue when its blocks are the resampling tiles
-    const bool fuse = a.weigh && !p->ode && !p->mif && R == 1 && kp.per_block == kTileRes && kBtRes == kp.bt;
-    a.fused = fuse ? 1 : 0;
-    a.fw_part = p->part;
-    a.fw_P = p->P;
-    a.fw_st = p->st;
-    a.fw_acc = p->acc;
-    a.fw_log_like_min = p->log_like_min;
-    a.fw_U_crn = p->crn_tab ? p->crn_u[n] : -1.0;
-    a.fw_llike = p->llike;
-    a.fw_ess = p->ess;
     crn_off += RJ * p->n_sub[n] * D;
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n], s, cudaEventRecordExternal));
     if (p->ode) {
@@ -451,12 +440,10 @@ int enqueue_filter(plomgpu_plan* p) {
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
       const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
-      if (!a.fused) {
-        k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-            (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
-            p->llike, p->ess, p->n_obs);
-        ++kernels;
-      }
+      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
+          p->llike, p->ess, p->n_obs);
+      ++kernels;
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
                                                             p->thresh, p->st, p->theta_hat, p->vt_add, p->Q, n,

@@ -260,18 +260,6 @@ struct StepArgs {
   void* theta_next;       // [Q][R*J] (T)
   const double* sd_mut;   // [Q] random-walk sd applied when gathering from ancestors, NULL: none
   const double* x0_rep;   // [S] initial particle read by every particle instead of X_prev, NULL: X_prev
-  // weighting fused into the epilogue (one run whose resampling tiles are the
-  // propagate blocks): the block's log-sum-exp partial, and the fold of the
-  // partials by the last block (fused = 0: a separate k_weight_tiles)
-  int fused;
-  void* fw_part;          // LseAcc [blocks]
-  double* fw_P;           // [blocks + 1]
-  void* fw_st;            // StepState
-  void* fw_acc;           // FilterAcc
-  double fw_log_like_min;
-  double fw_U_crn;        // CRN resampling uniform, < 0: Philox
-  double* fw_llike;       // [n_obs] or NULL
-  double* fw_ess;         // [n_obs] or NULL
 };
 
 // environments with per-particle parameters (iterated filtering)
@@ -1219,46 +1207,17 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
                  ess_out, sh, shd);
 }
 
-// The propagate launch: one particle per thread.  With a.fused (and a
-// weighted interval) the block's particles are a resampling tile: the block
-// merges their log-weights (the partial k_weight_tiles computes) and the last
-// block folds the partials, so that no separate launch re-reads them.
+// The propagate launch: one particle per thread.  (Merging the block's
+// log-weights here, so that no separate launch re-reads them, measured
+// slower: the epilogue's registers cost the propagate loop more, 0.563
+// against 0.505 ms per SEIR 20x2 interval, than the launch it saves.)
 template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   propagate_tables<T, BT>(tb, smem_raw, true);
-  const size_t RJ = (size_t)tb.R * tb.J;
   const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;  // particle of all runs
-  double l = NAN;
-  if (g < RJ) l = propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
-  // (register-state models keep their tiles apart from the blocks: never fused)
-  if (!SMEM || !(a.fused && a.weigh)) return;
-  __syncthreads();  // the state columns are free: the scratch below reuses them
-  unsigned char* scr = smem_raw + ((size_t)(kSmemCoup + kSmemPar) * sizeof(T) + 15) / 16 * 16;
-  LseAcc* sh = reinterpret_cast<LseAcc*>(scr);
-  double* shd = reinterpret_cast<double*>(sh + BT / 32);
-  int* s_last = reinterpret_cast<int*>(shd + BT / 32);
-  const double thresh = pow(tb.like_min, (double)M::N_TS);
-  LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
-  if (g < RJ) {
-    if (weight_fails((T)l, thresh)) acc.nfail = 1;
-    else acc = LseAcc{l, 1.0, 1.0, 0};
-  }
-  acc = block_lse_all<BT>(acc, sh);
-  LseAcc* part = reinterpret_cast<LseAcc*>(a.fw_part);
-  FilterAcc* facc = reinterpret_cast<FilterAcc*>(a.fw_acc);
-  if (threadIdx.x == 0) {
-    part[blockIdx.x] = acc;
-    __threadfence();
-    const unsigned t = atomicAdd(&facc->ticket, 1u);
-    *s_last = (t == gridDim.x - 1u) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!*s_last) return;
-  __threadfence();
-  if (threadIdx.x == 0) facc->ticket = 0u;
-  fold_tiles<BT>(part, (int)gridDim.x, tb.J, a.fw_log_like_min, a.fw_P, reinterpret_cast<StepState*>(a.fw_st), facc,
-                 a.n, a.fw_U_crn, plomrt::make_key(*tb.seed, tb.filter_id), a.fw_llike, a.fw_ess, sh, shd);
+  if (g >= (size_t)tb.R * tb.J) return;
+  propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
 }
 
 // Cumulative normalised weights of tile b: C_i = P[b] + (prefix of
