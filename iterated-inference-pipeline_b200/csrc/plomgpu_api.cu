@@ -1813,6 +1813,13 @@ int server_build(plomgpu_server* sv, int dev) {
   memset(sv->map_h, 0, (size_t)sv->ring * sizeof(int));
   CK(cudaHostGetDevicePointer((void**)&sv->slots_d, sv->slots_h, 0));
   CK(cudaHostGetDevicePointer((void**)&sv->ctl_d, sv->ctl_h, 0));
+  if (sv->tiled) {
+    CK(cudaMalloc((void**)&sv->ctl_dev, sizeof(ServeCtl)));
+    CK(cudaMemsetAsync(sv->ctl_dev, 0, sizeof(ServeCtl), s));
+    int lo = 0, hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CK(cudaStreamCreateWithPriority(&sv->ctl_stream, cudaStreamNonBlocking, hi));
+  }
   CK(cudaHostGetDevicePointer((void**)&sv->map_d, sv->map_h, 0));
   CK(cudaMalloc((void**)&sv->d_head, sizeof(unsigned long long)));
   CK(cudaMemsetAsync(sv->d_head, 0, sizeof(unsigned long long), s));
@@ -1854,6 +1861,10 @@ void server_free(plomgpu_server* sv) {
   sv->cv.notify_all();
   if (sv->worker.joinable()) sv->worker.join();
   if (sv->ctl_h) __atomic_store_n(&sv->ctl_h->stop, 1, __ATOMIC_RELEASE);
+  if (sv->ctl_dev && sv->ctl_stream) {
+    cudaMemcpyAsync(&sv->ctl_dev->stop, &sv->ctl_h->stop, sizeof(int), cudaMemcpyHostToDevice, sv->ctl_stream);
+    cudaStreamSynchronize(sv->ctl_stream);
+  }
   for (int i = 1; i < plomgpu_server::kLoops; ++i)
     if (sv->loop_stream[i]) cudaStreamSynchronize(sv->loop_stream[i]);
   if (sv->stream) cudaStreamSynchronize(sv->stream);
@@ -1863,7 +1874,7 @@ void server_free(plomgpu_server* sv) {
   }
   void* bufs[] = {sv->d_n_sub, sv->d_sub0, sv->d_t_sub, sv->d_t_obs, sv->d_cov_ts, sv->d_data, sv->d_cov_cac,
                   sv->d_coupling, sv->d_drift_vol, sv->d_drift_group, sv->d_drift_ngroups, sv->d_drift_bt,
-                  sv->d_error, sv->d_head, sv->d_pool, sv->d_live};
+                  sv->d_error, sv->d_head, sv->d_pool, sv->d_live, sv->ctl_dev};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (sv->slots_h) cudaFreeHost(sv->slots_h);
@@ -1873,6 +1884,7 @@ void server_free(plomgpu_server* sv) {
     if (sv->loop_ev[i]) cudaEventDestroy(sv->loop_ev[i]);
     if (sv->loop_stream[i]) cudaStreamDestroy(sv->loop_stream[i]);
   }
+  if (sv->ctl_stream) cudaStreamDestroy(sv->ctl_stream);
   if (sv->kernel_ev) cudaEventDestroy(sv->kernel_ev);
   if (sv->stream) cudaStreamDestroy(sv->stream);
   delete sv;

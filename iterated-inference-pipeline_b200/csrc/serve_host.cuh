@@ -118,6 +118,11 @@ struct plomgpu_server {
   ServeSlot* slots_d = nullptr;
   ServeCtl* ctl_h = nullptr;     // mapped
   ServeCtl* ctl_d = nullptr;
+  // a device-memory copy of the control block for the tiled loop, refreshed
+  // by a small copy after every publication: its CTAs poll device memory,
+  // not the host's
+  ServeCtl* ctl_dev = nullptr;
+  cudaStream_t ctl_stream = nullptr;
   int* map_h = nullptr;          // mapped: ring position -> slot
   int* map_d = nullptr;
   unsigned long long* d_head = nullptr;
@@ -139,6 +144,7 @@ struct plomgpu_server {
   int loop_grid[kLoops] = {};
   bool loop_live[kLoops] = {};
   unsigned long long published = 0;
+  unsigned long long pushed_tail = 0;  // tail last copied to ctl_dev
   std::vector<long long> slot_ticket;  // ring slot -> ticket (-1 free)
   std::vector<size_t> slot_off, slot_bytes;
   std::vector<Clock::time_point> slot_t;
@@ -249,7 +255,7 @@ int serve_launch(plomgpu_server* sv, int inst, int grid) {
   if (sv->tiled) {
     ServeTilesKernel<T> k = pick_serve_tiles<T>(sv->base.noises_off);
     if (!k) return fail(PLOMGPU_EINVAL, "no serving kernel for this model");
-    k<<<grid, sv->bt, sv->tiles_smem, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_d,
+    k<<<grid, sv->bt, sv->tiles_smem, st>>>(serve_args<T>(sv), sv->slots_d, sv->map_d, sv->ring, sv->ctl_dev,
                                             sv->d_head, sv->d_pool, sv->d_live, sv->idle_limit, sv->task_budget);
   } else {
     ServeKernel<T> k = pick_serve<T>(sv->base.noises_off);
@@ -406,6 +412,11 @@ void serve_pass(plomgpu_server* sv) {
       sv->pending.pop_front();
       sv->launches++;
     }
+  }
+  if (sv->tiled && sv->ctl_dev && sv->published != sv->pushed_tail) {
+    cudaMemcpyAsync(&sv->ctl_dev->tail, &sv->ctl_h->tail, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                    sv->ctl_stream);
+    sv->pushed_tail = sv->published;
   }
   // (re)start device loops while published requests outnumber the live CTAs
   if (sv->persistent) {

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
       long long got = -1;
       long long spins = 0;
       for (;;) {
-        if (stop_ref.load(cuda::memory_order_acquire)) break;
+        if ((spins & 255) == 0 && stop_ref.load(cuda::memory_order_acquire)) break;
         const unsigned long long t = tail_ref.load(cuda::memory_order_acquire);
         const unsigned long long h = atomicAdd(head, 0ull);
         if (h < t) {
@@ -140,21 +140,29 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
 constexpr int kServeLive = 64;
 
 // device state of one admitted request, at the start of its workspace
+// The claim counter, the completion counter and the rest sit in cache lines
+// of their own: every polling CTA reads the first, every finishing one adds
+// to the second.
 struct TileReq {
-  unsigned long long phase;  // (phase number << 32) | next unclaimed tile; phase numbers start at
-                             // order << 12, so a stale read of a reused workspace never matches
-  unsigned done;             // tiles of the current phase finished
-  int n;                     // interval of the current phase
+  alignas(128) unsigned long long phase;  // (phase number << 32) | next unclaimed tile; phase numbers
+                                          // start at order << 12, so a stale read of a reused workspace
+                                          // never matches
+  alignas(128) unsigned done;             // tiles of the current phase finished
+  alignas(128) int n;                     // interval of the current phase
   int kind;                  // 0 propagate, 1 cumulate, 2 search
   int cur;                   // generation holding the particles before interval n
   int resampled;             // the ancestors of interval n - 1 apply (else identity)
   int slot;                  // ring slot of the request (its result)
   int J, ntiles;
+  int n_obs;                 // intervals of the request
   long long order;           // publication order (older requests first)
   uint64_t seed;
   StepState st;
   FilterAcc acc;
 };
+
+// tiles a CTA claims at once: one propagate tile, a few of the short phases
+constexpr int kServeShortClaim = 4;
 
 template <class T>
 struct TileReqWs {
@@ -232,12 +240,15 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
   TileScratch<BT, 1>& sc = *reinterpret_cast<TileScratch<BT, 1>*>(
       smem_raw + ((size_t)(kSmemCoup + kSmemPar) * sizeof(T) + 15) / 16 * 16);
   __shared__ long long s_off;   // workspace of the claimed request, -1: none
-  __shared__ int s_tile;        // claimed tile, -1: admission of a new request
+  __shared__ int s_tile;        // first claimed tile, -1: admission of a new request
+  __shared__ int s_ntask;       // tiles claimed
   __shared__ int s_entry;       // live-table entry of an admission
   __shared__ long long s_req;   // publication order of an admission
   __shared__ int s_last;
-  cuda::atomic_ref<unsigned long long, cuda::thread_scope_system> tail_ref(ctl->tail);
-  cuda::atomic_ref<int, cuda::thread_scope_system> stop_ref(ctl->stop);
+  // ctl is a device-memory copy of the host's control block (the host copies
+  // it after every publication)
+  cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> tail_ref(ctl->tail);
+  cuda::atomic_ref<int, cuda::thread_scope_device> stop_ref(ctl->stop);
   if constexpr (M::COUPLED) {
     T* s_coup = reinterpret_cast<T*>(smem_raw);
     for (int i = threadIdx.x; i < M::N_CAC * M::N_CAC; i += BT) s_coup[i] = a.coupling[i];
@@ -255,9 +266,10 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       if (lane == 0) s_off = -1;
       __syncwarp();
       long long spins = 0;
+      unsigned backoff = 128u;  // ns between polls that find nothing, doubling up to 8 us
       for (;;) {
         int stop = 0;
-        if (lane == 0) stop = stop_ref.load(cuda::memory_order_acquire);
+        if (lane == 0) stop = stop_ref.load(cuda::memory_order_relaxed);
         if (__shfl_sync(0xffffffffu, stop, 0)) break;
         // a tile of the oldest live request that has one
         long long my_off = -1, my_order = LLONG_MAX;
@@ -282,6 +294,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         }
         // the lane holding the oldest claimable request
         long long best = my_order;
+        int my_kind = 0;
+        if (my_off >= 0) my_kind = *(volatile int*)&reinterpret_cast<TileReq*>(pool + my_off)->kind;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(0xffffffffu, best, o));
         const unsigned who = __ballot_sync(0xffffffffu, my_off >= 0 && my_order == best);
@@ -293,11 +307,14 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
             // count past the tiles (the phase is taken, or the workspace was
             // reused by a newer request after the read above) claims nothing
             TileReq* q = reinterpret_cast<TileReq*>(pool + my_off);
-            const unsigned long long v = atomicAdd(&q->phase, 1ull);
+            const int k = (my_kind == 0) ? 1 : kServeShortClaim;
+            const unsigned long long v = atomicAdd(&q->phase, (unsigned long long)k);
             __threadfence();
-            if ((int)(v & 0xffffffffull) < *(volatile int*)&q->ntiles) {
+            const int t0 = (int)(v & 0xffffffffull), nt = *(volatile int*)&q->ntiles;
+            if (t0 < nt) {
               s_off = my_off;
-              s_tile = (int)(v & 0xffffffffull);
+              s_tile = t0;
+              s_ntask = min(k, nt - t0);
               got = 1;
             }
           }
@@ -335,15 +352,19 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         // nothing to do now: while requests are live the wait is long (their
         // serial parts run on one CTA), else short; bounded either way
         if (++spins > (any_live ? idle_limit * 2500 : idle_limit)) break;
-        __nanosleep(500);
+        __nanosleep(backoff);
+        backoff = backoff < 8192u ? 2u * backoff : 8192u;
       }
     }
     __syncthreads();
     if (s_off < 0) return;
+    // the tiles' data come from other CTAs of this GPU (device-scope
+    // acquire); only an admission reads a slot the host wrote (system scope,
+    // which costs about as much as a whole tile of propagation)
     __threadfence();
-    cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_system);
     unsigned char* base = pool + s_off;
     if (s_tile < 0) {
+      cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_system);
       // admission: the request's device state and its parameters in the state precision
       const int slot = ring_map[s_req % ring];
       const ServeSlot* sl = slots + slot;
@@ -364,6 +385,7 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         q->slot = slot;
         q->J = J;
         q->ntiles = (J + BT - 1) / BT;
+        q->n_obs = sl->n_obs;
         q->order = s_req;
         q->seed = sl->seed;
         q->acc.loglik = 0.0;
@@ -379,13 +401,13 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       continue;
     }
     TileReq* q = reinterpret_cast<TileReq*>(base);
-    const int J = q->J, ntiles = q->ntiles, n = q->n, kind = q->kind, tile = s_tile;
-    const ServeSlot* sl = slots + q->slot;
+    const int J = q->J, ntiles = q->ntiles, n = q->n, kind = q->kind, ntask = s_ntask;
     const TileReqWs<T> w = tile_req_ws<T, BT>(base, J);
     const double* y = a.data + (size_t)n * M::N_TS;
     bool any = false;
     for (int ts = 0; ts < M::N_TS; ++ts) any |= !isnan(__ldg(y + ts));
     const bool weigh = a.filter_on && any;
+    for (int tile = s_tile; tile < s_tile + ntask; ++tile) {
     if (kind == 0) {
       Tables<T> tb{};
       tb.par_cac = w.par_cac;
@@ -435,14 +457,17 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
     } else {
       search_tile<BT, 1>(w.C, J, &q->st, tile, w.anc, nullptr, sc);
     }
+    __syncthreads();  // the shared scratch of one tile before the next
+    }
     // the last tile of the phase does its serial part and publishes the next phase
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) s_last = (atomicAdd(&q->done, 1u) == (unsigned)ntiles - 1u) ? 1 : 0;
+    if (threadIdx.x == 0)
+      s_last = (atomicAdd(&q->done, (unsigned)ntask) + (unsigned)ntask == (unsigned)ntiles) ? 1 : 0;
     __syncthreads();
     if (!s_last) continue;
     __threadfence();
-    const int T_obs = sl->n_obs;
+    const int T_obs = q->n_obs;
     bool finished = false;
     int next_kind = 0, next_n = n, next_cur = q->cur, next_res = q->resampled;
     if (kind == 0) {
