@@ -13,6 +13,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -28,6 +29,31 @@ thread_local std::string g_err;
 int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
+}
+
+// The largest double x with exp(x) <= thresh, by bisection over the doubles
+// in order (exp is non-decreasing): weight() (model_builder/C/core/smc.c:44)
+// fails a particle when exp(loglik) <= LIKE_MIN^N_TS, which is loglik <= x,
+// with the host's exp as the reference computes it.
+double fail_boundary(double thresh) {
+  auto key = [](double v) -> int64_t {
+    int64_t b;
+    memcpy(&b, &v, sizeof b);
+    return b >= 0 ? b : -(b & INT64_MAX);
+  };
+  auto val = [](int64_t k) -> double {
+    const int64_t b = k >= 0 ? k : ((-k) | INT64_MIN);
+    double v;
+    memcpy(&v, &b, sizeof v);
+    return v;
+  };
+  int64_t lo = key(-HUGE_VAL), hi = key(HUGE_VAL);  // exp(lo) <= thresh < exp(hi)
+  if (!(exp(val(hi)) > thresh)) return val(hi);      // nothing survives
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (exp(val(mid)) <= thresh) lo = mid; else hi = mid;
+  }
+  return val(lo);
 }
 
 #define CK(call)                                                                              \
@@ -54,13 +80,7 @@ constexpr int kBtOde = 64;
 constexpr int kOdeMaxSteps = 1000000;  // attempted RKF45 steps per interval
 static_assert(kTeam == 1 || kTeam == 2 || kTeam == 4 || kTeam == 8 || kTeam == 16 || kTeam == 32,
               "team size must be a power of two up to 32");
-constexpr int kBtWeight = 256;
-constexpr int kBtScan = 256;
-constexpr int kIptScan = 8;
-constexpr int kTile = kBtScan * kIptScan;
-constexpr int kBtSearch = 256;
-constexpr int kMaxWeightBlocks = 592;
-// tiles of the filters' weighting / resampling (k_weight_tiles, k_cum_tiles, k_search_tiles):
+// tiles of the filters' weighting / resampling (k_weight_tiles, k_resample_tiles):
 // the propagate block's particles for shared-memory models (the tiles of the
 // serving loop, so that a served request and the plain filter reduce in the
 // same order), 1024 particles otherwise
@@ -82,7 +102,7 @@ struct plomgpu_plan {
   bool crn = false, want_anc = false, want_xpred = false, want_llike = true;
   bool paired = false;           // CRN kernels on the FP64 Philox draws (no table)
   double* x0_cloud = nullptr;    // optional [OFF_INC][J] initial particles
-  double dt = 1.0, like_min = 1e-17, thresh = 0.0, log_like_min = 0.0;
+  double dt = 1.0, like_min = 1e-17, fail_b = 0.0, log_like_min = 0.0;
   std::vector<int> n_sub, sub0;
   std::vector<double> t_obs, crn_u;
   std::vector<char> weigh;
@@ -94,7 +114,9 @@ struct plomgpu_plan {
   void* X[2] = {nullptr, nullptr};
   void* lw = nullptr;
   double* P = nullptr;            // [R][ntiles + 1] tile prefixes of the normalised weights
-  double* C = nullptr;            // [R][J] cumulative normalised weights
+  double* C = nullptr;            // [R][J] cumulative normalised weights of tiles left to k_resample_heavy
+  HeavyTile* heavy = nullptr;     // [R][ntiles] those tiles
+  int heavy_blocks = 1;
   uint32_t* anc[2] = {nullptr, nullptr};
   LseAcc* part = nullptr;         // [R][ntiles] tile partials
   StepState* st = nullptr;
@@ -315,7 +337,7 @@ int enqueue_hat(plomgpu_plan* p, const T* X, int row, const double* cov_ts, doub
   const double* pop = p->pop ? p->pop + (size_t)row * M::N_CAC : nullptr;
   const int g = (J + 255) / 256 < 4096 ? (J + 255) / 256 : 4096;
   k_hat_values<T><<<g, 256, 0, s>>>(X, J, pop, p->par_ts, cov_ts, t, p->drift_bt, (const T*)p->lw, p->st,
-                                    weighted ? 1 : 0, p->thresh, p->vals);
+                                    weighted ? 1 : 0, p->fail_b, p->vals);
   k_hat_stats<T, 256><<<kHatQ, 256, 0, s>>>(p->vals, J, p->st, weighted ? 1 : 0, p->hat_rank[0], p->hat_rank[1],
                                             p->hat + (size_t)row * kHatQ * 3);
   return 2;
@@ -384,7 +406,7 @@ int enqueue_filter(plomgpu_plan* p) {
                                     (T*)p->theta[0], p->x0_slot, p->pop0, p->x0, p->theta_bt, (T*)p->X[0], p->acc);
     ++kernels;
     if (p->fls_n == -1) {
-      k_mif_fls<T, 256><<<dim3(p->Q, R), 256, 0, s>>>(nullptr, (const T*)p->theta[0], nullptr, J, R, p->thresh, p->st,
+      k_mif_fls<T, 256><<<dim3(p->Q, R), 256, 0, s>>>(nullptr, (const T*)p->theta[0], nullptr, J, R, p->fail_b, p->st,
                                                       p->fls_mask, p->Q, p->fls_out);
       ++kernels;
     }
@@ -441,20 +463,21 @@ int enqueue_filter(plomgpu_plan* p) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
       const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
       k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->thresh, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
+          (const T*)p->lw, J, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
           p->llike, p->ess, p->n_obs);
       ++kernels;
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
-                                                            p->thresh, p->st, p->theta_hat, p->vt_add, p->Q, n,
+                                                            p->fail_b, p->st, p->theta_hat, p->vt_add, p->Q, n,
                                                             p->n_obs, p->bart, p->vt);
         ++kernels;
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
-      k_cum_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>((const T*)p->lw, J, p->thresh, p->part,
-                                                                           p->P, p->st, p->C);
-      k_search_tiles<kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          p->C, J, p->st, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+      k_resample_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->fail_b, p->part, p->P, p->st, p->anc[nxt],
+          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr, p->C, p->heavy);
+      k_resample_heavy<256><<<dim3(p->heavy_blocks, R), 256, 0, s>>>(
+          p->C, J, p->ntiles, kTileRes, p->st, p->heavy, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
       kernels += 2;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
@@ -462,7 +485,7 @@ int enqueue_filter(plomgpu_plan* p) {
       }
       if (p->mif && n == p->fls_n) {
         k_mif_fls<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], p->anc[nxt], J, R,
-                                                        p->thresh, p->st, p->fls_mask, p->Q, p->fls_out);
+                                                        p->fail_b, p->st, p->fls_mask, p->Q, p->fls_out);
         ++kernels;
       }
       anc_cur = nxt;
@@ -580,6 +603,8 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   p->ntiles = (J + kTileRes - 1) / kTileRes;
   CK(cudaMalloc((void**)&p->part, (size_t)p->R * p->ntiles * sizeof(LseAcc)));
   CK(cudaMalloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
+  CK(cudaMalloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
+  p->heavy_blocks = std::min(p->ntiles, 2 * 148);
   CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
   CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
   CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
@@ -713,7 +738,7 @@ void plan_free(plomgpu_plan* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->C, p->anc[0], p->anc[1], p->part, p->st, p->acc,
+  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->C, p->heavy, p->anc[0], p->anc[1], p->part, p->st, p->acc,
                   p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
@@ -864,7 +889,7 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   }
   p->dt = d->dt;
   p->like_min = d->like_min;
-  p->thresh = pow(d->like_min, (double)M::N_TS);
+  p->fail_b = fail_boundary(pow(d->like_min, (double)M::N_TS));
   p->log_like_min = log(d->like_min);
   p->n_sub.assign(d->n_sub, d->n_sub + d->n_obs);
   p->t_obs.assign(d->t_obs, d->t_obs + d->n_obs);
@@ -953,8 +978,7 @@ int plan_results(plomgpu_plan* p, plomgpu_smc_result* r) {
       r->status = PLOMGPU_EINVAL;
       return fail(PLOMGPU_EINVAL, "ode: integration time step is too small to match the desired precision");
     }
-    return fail(PLOMGPU_ETIMEOUT, (p->acc_h->error & ERR_SCAN_WAIT) ? "cumulative-weight scan wait ran out"
-                                                                      : "systematic point table overflow");
+    return fail(PLOMGPU_ETIMEOUT, "systematic point table overflow");
   }
   r->status = PLOMGPU_OK;
   return PLOMGPU_OK;
@@ -1011,11 +1035,11 @@ int plomgpu_plan_sample_traj(plomgpu_plan* p, double u, int* n_rows, int* rows_t
   if (p->n_data < 2) return fail(PLOMGPU_EINVAL, "trajectory sampling needs at least two intervals with data");
   cudaStream_t s = p->stream;
   if (p->precision == 64)
-    k_sample_traj<double, 256><<<1, 256, 0, s>>>((const double*)p->lw, p->J, p->st, p->thresh, u, p->n_obs,
+    k_sample_traj<double, 256><<<1, 256, 0, s>>>((const double*)p->lw, p->J, p->st, p->fail_b, u, p->n_obs,
                                                  p->data_idx, p->n_data, p->anc_hist, p->x_hist, p->x0, p->traj_t,
                                                  p->traj_j, p->traj_x, p->traj_n);
   else
-    k_sample_traj<float, 256><<<1, 256, 0, s>>>((const float*)p->lw, p->J, p->st, p->thresh, u, p->n_obs,
+    k_sample_traj<float, 256><<<1, 256, 0, s>>>((const float*)p->lw, p->J, p->st, p->fail_b, u, p->n_obs,
                                                 p->data_idx, p->n_data, p->anc_hist, p->x_hist, p->x0, p->traj_t,
                                                 p->traj_j, p->traj_x, p->traj_n);
   CK(cudaGetLastError());
@@ -1269,7 +1293,7 @@ extern "C" int plomgpu_mif_iteration(plomgpu_mif* p, const double* theta_hat, co
   if (err & ERR_IC)
     return fail(PLOMGPU_EINVAL, "initial conditions: no proposal with proportions summing to at most 1 in " +
                                     std::to_string(kMaxIcAttempts) + " draws");
-  if (err) return fail(PLOMGPU_ETIMEOUT, "a bounded device wait ran out");
+  if (err) return fail(PLOMGPU_ETIMEOUT, "systematic point table overflow");
   return PLOMGPU_OK;
 }
 
@@ -1302,13 +1326,15 @@ extern "C" void plomgpu_mif_destroy(plomgpu_mif* p) { plan_free(p); }
 namespace {
 
 constexpr int kNoAllocMaxJ = 1 << 18;  // largest particle count the fixed scratch serves
-constexpr int kNoAllocTiles = (kNoAllocMaxJ + kTile - 1) / kTile;
+constexpr int kNoAllocBt = 256, kNoAllocIpt = 4, kNoAllocTile = kNoAllocBt * kNoAllocIpt;
+constexpr int kNoAllocTiles = (kNoAllocMaxJ + kNoAllocTile - 1) / kNoAllocTile;
 
 struct NoAllocScratch {
-  LseAcc part[kMaxWeightBlocks];
+  LseAcc part[kNoAllocTiles];
+  double P[kNoAllocTiles + 1];
   StepState st;
   FilterAcc acc;
-  TileStatus tstat[kNoAllocTiles];
+  HeavyTile heavy[kNoAllocTiles];
   double C[kNoAllocMaxJ];
 };
 
@@ -1323,21 +1349,21 @@ __global__ void k_noalloc_out(const StepState* st, const FilterAcc* acc, double*
   out[3] = (double)acc->error;
 }
 
+// the filters' own weighting / resampling launches (k_weight_tiles,
+// k_resample_tiles, k_resample_heavy) over tiles of 1024 particles
 template <class T>
 int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, double* out, cudaStream_t s,
                 NoAllocScratch* sc) {
-  const double thresh = pow(like_min, (double)M::N_TS);
-  int nblk = (J + kBtWeight * 4 - 1) / (kBtWeight * 4);
-  if (nblk > kMaxWeightBlocks) nblk = kMaxWeightBlocks;
-  if (nblk < 1) nblk = 1;
-  const int ntiles = (J + kTile - 1) / kTile;
-  // the accumulator and its tickets must start at zero; the previous call's
+  const double fail_b = fail_boundary(pow(like_min, (double)M::N_TS));
+  const int ntiles = (J + kNoAllocTile - 1) / kNoAllocTile;
+  // the accumulator and its ticket must start at zero; the previous call's
   // contents are still there
   k_reset_acc<<<1, 1, 0, s>>>(&sc->acc);
-  k_weight<T, kBtWeight><<<nblk, kBtWeight, 0, s>>>(lw, J, thresh, log(like_min), sc->part, &sc->st, &sc->acc,
-                                                   sc->tstat, ntiles, 0, u, nullptr, 0u, out, out + 1, 0);
-  k_scan<T, kBtScan, kIptScan><<<ntiles, kBtScan, 0, s>>>(lw, J, thresh, &sc->st, sc->tstat, &sc->acc, sc->C);
-  k_search<kBtSearch><<<(J + kBtSearch - 1) / kBtSearch, kBtSearch, 0, s>>>(sc->C, J, &sc->st, anc, nullptr);
+  k_weight_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(
+      lw, J, fail_b, log(like_min), sc->part, sc->P, &sc->st, &sc->acc, 0, u, nullptr, 0u, out, out + 1, 0);
+  k_resample_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(lw, J, fail_b, sc->part, sc->P, &sc->st,
+                                                                             anc, nullptr, sc->C, sc->heavy);
+  k_resample_heavy<256><<<ntiles, 256, 0, s>>>(sc->C, J, ntiles, kNoAllocTile, &sc->st, sc->heavy, anc, nullptr);
   k_noalloc_out<<<1, 1, 0, s>>>(&sc->st, &sc->acc, out);
   CK(cudaGetLastError());
   return PLOMGPU_OK;
@@ -1484,7 +1510,7 @@ BatchArgs<T> batch_args(plomgpu_batch* b, const BatchFilter* filters, int n, con
   a.drift_vol = (const T*)b->drift_vol;
   a.dt = b->dt;
   a.like_min = b->like_min;
-  a.thresh = pow(b->like_min, (double)M::N_TS);
+  a.fail_b = fail_boundary(pow(b->like_min, (double)M::N_TS));
   a.log_like_min = log(b->like_min);
   a.filter_on = b->filter;
   a.ws = b->ws;

@@ -184,7 +184,7 @@ BatchArgs<T> serve_args(plomgpu_server* sv) {
   a.drift_vol = (const T*)sv->d_drift_vol;
   a.dt = sv->base.dt;
   a.like_min = sv->base.like_min;
-  a.thresh = pow(sv->base.like_min, (double)M::N_TS);
+  a.fail_b = fail_boundary(pow(sv->base.like_min, (double)M::N_TS));
   a.log_like_min = log(sv->base.like_min);
   a.filter_on = sv->base.filter;
   a.error = sv->d_error;

@@ -47,7 +47,8 @@ struct BatchArgs {
   const int* drift_ngroups;
   const plomrt::BackTransform* drift_bt;
   const T* drift_vol;
-  double dt, like_min, thresh, log_like_min;
+  double dt, like_min, log_like_min;
+  double fail_b;  // largest log-weight that fails: exp(l) <= LIKE_MIN^N_TS (fail_boundary)
   int filter_on;
   // per-CTA workspace
   unsigned char* ws;
@@ -253,7 +254,7 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
           }
           const T l = (T)plomrt::finish_loglik(ll, fl, M::N_TS);
           ws.lw[j] = l;
-          if (weight_fails(l, a.thresh)) {
+          if (weight_fails_at(l, a.fail_b)) {
             acc.nfail += 1;
           } else {
             LseAcc b = {(double)l, 1.0, 1.0, 0};
@@ -306,14 +307,14 @@ __device__ void cta_filter(CtaShared<T, BT>& sh, const BatchArgs<T>& a, const Fi
       double run = 0.0;
       for (int i = i0; i < i1; ++i) {
         const T l = ws.lw[i];
-        run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+        run += weight_fails_at(l, a.fail_b) ? 0.0 : exp((double)l - m) / s1;
       }
       double tot;
       const double pre = block_exscan<BT>(run, sh.scan, &tot);
       run = pre;
       for (int i = i0; i < i1; ++i) {
         const T l = ws.lw[i];
-        run += weight_fails(l, a.thresh) ? 0.0 : exp((double)l - m) / s1;
+        run += weight_fails_at(l, a.fail_b) ? 0.0 : exp((double)l - m) / s1;
         ws.C[i] = run;
       }
       __syncthreads();

@@ -6,17 +6,19 @@
 //                substeps (f_prediction_sde_*, prediction_util.c:197-287),
 //                map to observations (proj2obs) and write the log-weight
 //                (get_log_likelihood, likelihood.c:56-70);
-//   k_weight     failure test, log-sum-exp normalisation in FP64, ESS,
-//                log-likelihood accumulation and the all-fail rule
-//                (weight(), smc.c:27-83); the last block also lays out the
-//                systematic points of the interval (smc.c:97-111);
-//   k_scan       cumulative normalised weights in FP64 (smc.c:102-108);
-//   k_search     ancestor of each particle slot (systematic_sampling,
-//                smc.c:104-111) = first i with cum[i] >= point[j].
+//   k_weight_tiles    failure test, log-sum-exp normalisation in FP64, ESS,
+//                     log-likelihood accumulation and the all-fail rule
+//                     (weight(), smc.c:27-83); the last block also lays out
+//                     the systematic points of the interval (smc.c:97-111);
+//   k_resample_tiles  cumulative normalised weights in FP64 (smc.c:102-108)
+//                     and the ancestor of each particle slot
+//                     (systematic_sampling, smc.c:104-111) = first i with
+//                     cum[i] >= point[j];
+//   k_resample_heavy  the same for tiles that took many points.
 //
 // State is struct-of-arrays X[w][j] in HBM (two generations), log-weights
-// lw[j] in the state precision, cumulative weights and every reduction in
-// FP64.  The particle loop of the reference (OpenMP / ZeroMQ workers,
+// lw[j] in the state precision, their exponentials, cumulative weights and
+// every sum in FP64.  The particle loop of the reference (OpenMP / ZeroMQ workers,
 // worker_inproc.c:71-80) is the kernel grid.
 #pragma once
 
@@ -727,295 +729,92 @@ __device__ __forceinline__ LseAcc lse_shfl(LseAcc a, int off) {
   return lse_merge(a, b);
 }
 
-struct TileStatus {
-  double agg;
-  int flag;
-  int pad;
-};
-
 // Per-filter device state of the current interval.
 struct StepState {
   double m, s1, s2;
   int all_fail;
   int nseg;
   double U;
+  int nheavy;  // tiles whose points are left to k_resample_heavy
+  int pad;
   plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
 };
 
 struct FilterAcc {
   double loglik;
   int n_all_fail;
-  int error;        // bit 0: scan wait ran out; bit 1: systematic table overflow; bit 2: ODE step control failed
-  unsigned ticket;  // block ticket of k_weight
-  unsigned tile_ticket;
+  int error;        // bit 1: systematic table overflow; bit 2: ODE step control failed; bit 3: no valid initial condition
+  unsigned ticket;  // block ticket of k_weight_tiles
 };
 
-enum { ERR_SCAN_WAIT = 1, ERR_SYS_TABLE = 2, ERR_ODE = 4, ERR_IC = 8 };
+enum { ERR_SYS_TABLE = 2, ERR_ODE = 4, ERR_IC = 8 };
 
+// weight() (smc.c:44): the particle fails if exp(loglik) <= LIKE_MIN^N_TS.
+// fail_b is the largest double whose exponential is <= LIKE_MIN^N_TS
+// (fail_boundary on the host, with the host's exp as in the reference), so
+// the test needs no exponential: the particle fails exactly when l <= fail_b.
 template <class T>
-__device__ __forceinline__ bool weight_fails(T l, double thresh) {
-  // weight() (smc.c:44): the particle fails if exp(loglik) <= LIKE_MIN^N_TS
-  return !(exp((double)l) > thresh);
-}
-
-template <class T, int BT>
-__global__ void __launch_bounds__(BT) k_weight(const T* __restrict__ lw, int J, double thresh, double log_like_min,
-                                               LseAcc* part, StepState* st, FilterAcc* acc, TileStatus* tstat,
-                                               int ntiles, int n, double U_crn, const uint64_t* seed, uint32_t filter_id,
-                                               double* llike_out, double* ess_out, int out_stride) {
-  __shared__ LseAcc sh[BT / 32];
-  __shared__ bool last;
-  {  // run r of the lock-stepped runs
-    const int r = blockIdx.y;
-    lw += (size_t)r * J;
-    part += (size_t)r * gridDim.x;
-    st += r;
-    acc += r;
-    tstat += (size_t)r * ntiles;
-    if (llike_out) llike_out += (size_t)r * out_stride;
-    if (ess_out) ess_out += (size_t)r * out_stride;
-    filter_id += (uint32_t)r;
-  }
-  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
-  for (int i = blockIdx.x * BT + threadIdx.x; i < J; i += gridDim.x * BT) {
-    const T l = lw[i];
-    if (weight_fails(l, thresh)) {
-      a.nfail += 1;
-    } else {
-      LseAcc b = {(double)l, 1.0, 1.0, 0};
-      a = lse_merge(a, b);
-    }
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-    if (threadIdx.x == 0) {
-      part[blockIdx.x] = a;
-      __threadfence();
-      const unsigned t = atomicAdd(&acc->ticket, 1u);
-      last = (t == gridDim.x - 1);
-    }
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the last block folds the partials in a fixed order
-  a = LseAcc{-INFINITY, 0.0, 0.0, 0};
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += BT) {
-    volatile LseAcc* p = part + b;
-    LseAcc v = {p->m, p->s1, p->s2, p->nfail};
-    a = lse_merge(a, v);
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
-  __syncthreads();
-  for (int i = threadIdx.x; i < ntiles; i += BT) tstat[i].flag = 0;
-  if (threadIdx.x < 32) {
-    a = (threadIdx.x < BT / 32) ? sh[threadIdx.x] : LseAcc{-INFINITY, 0.0, 0.0, 0};
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) a = lse_shfl(a, off);
-    if (threadIdx.x == 0) {
-      acc->ticket = 0u;
-      acc->tile_ticket = 0u;
-      double llike, ess;
-      int all_fail = (a.nfail == J);
-      if (all_fail) {
-        // every particle failed: equal weights, identity ancestors (smc.c:55-69)
-        llike = log_like_min * (double)M::N_TS;
-        ess = 0.0;
-        acc->n_all_fail += 1;
-      } else {
-        llike = a.m + log(a.s1 / (double)J);
-        ess = (a.s1 * a.s1) / a.s2;
-      }
-      acc->loglik += llike;
-      st->m = a.m;
-      st->s1 = a.s1;
-      st->s2 = a.s2;
-      st->all_fail = all_fail;
-      if (llike_out) llike_out[n] = llike;
-      if (ess_out) ess_out[n] = ess;
-      const double inc = 1.0 / (double)J;
-      const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(plomrt::make_key(*seed, filter_id), (uint32_t)n);
-      const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
-      st->U = U;
-      int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
-      if (ns < 0) {
-        acc->error |= ERR_SYS_TABLE;
-        ns = 0;
-      }
-      st->nseg = ns;
-    }
-  }
-}
-
-// ------------------------------------------------------------------ cumulative weights
-// Tiles are claimed in launch order through a ticket, publish their
-// aggregate, and take their exclusive prefix as the sum of all earlier
-// aggregates in a fixed order (lane l adds tiles l, l+32, ... then a fixed
-// butterfly), so the result does not depend on timing.  A tile only waits for
-// tiles claimed before it; every wait is bounded.
-template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_scan(const T* __restrict__ lw, int J, double thresh, const StepState* st,
-                                             TileStatus* tstat, FilterAcc* acc, double* __restrict__ C) {
-  constexpr int TILE = BT * IPT;
-  {
-    const int r = blockIdx.y;
-    lw += (size_t)r * J;
-    st += r;
-    acc += r;
-    tstat += (size_t)r * gridDim.x;
-    C += (size_t)r * J;
-  }
-  __shared__ double sv[TILE];
-  __shared__ double swarp[BT / 32];
-  __shared__ int s_tile;
-  __shared__ double s_prefix;
-  if (st->all_fail) return;
-  if (threadIdx.x == 0) s_tile = (int)atomicAdd(&acc->tile_ticket, 1u);
-  __syncthreads();
-  const int tile = s_tile;
-  const int base = tile * TILE;
-  const double m = st->m, s1 = st->s1;
-  for (int k = threadIdx.x; k < TILE; k += BT) {
-    const int i = base + k;
-    double p = 0.0;
-    if (i < J) {
-      const T l = lw[i];
-      p = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
-    }
-    sv[k] = p;
-  }
-  __syncthreads();
-  // thread-sequential inclusive sums of IPT consecutive items
-  double run = 0.0;
-  double loc[IPT];
-#pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    run += sv[threadIdx.x * IPT + k];
-    loc[k] = run;
-  }
-  // block exclusive scan of the thread totals
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double v = run;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const double o = __shfl_up_sync(0xffffffffu, v, off);
-    if (lane >= off) v += o;
-  }
-  if (lane == 31) swarp[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    double w = (lane < BT / 32) ? swarp[lane] : 0.0;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const double o = __shfl_up_sync(0xffffffffu, w, off);
-      if (lane >= off) w += o;
-    }
-    if (lane < BT / 32) swarp[lane] = w;  // inclusive warp totals
-  }
-  __syncthreads();
-  const double warp_excl = (warp > 0) ? swarp[warp - 1] : 0.0;
-  const double thread_excl = warp_excl + (v - run);
-  const double tile_total = swarp[BT / 32 - 1];
-  if (threadIdx.x == 0) {
-    volatile TileStatus* ts = tstat + tile;
-    ts->agg = tile_total;
-    __threadfence();
-    ts->flag = 1;
-  }
-  // exclusive prefix from earlier aggregates, fixed order
-  if (warp == 0) {
-    double s = 0.0;
-    bool timeout = false;
-    for (int k = lane; k < tile; k += 32) {
-      volatile TileStatus* ts = tstat + k;
-      int spins = 0;
-      while (ts->flag == 0) {
-        if (++spins > (1 << 22)) { timeout = true; break; }
-        __nanosleep(64);
-      }
-      __threadfence();
-      s += ts->agg;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (__any_sync(0xffffffffu, timeout) && lane == 0) atomicOr(&acc->error, (int)ERR_SCAN_WAIT);
-    if (lane == 0) s_prefix = s;
-  }
-  __syncthreads();
-  const double prefix = s_prefix + thread_excl;
-#pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    const int i = base + threadIdx.x * IPT + k;
-    if (i < J) C[i] = prefix + loc[k];
-  }
-}
-
-// ------------------------------------------------------------------ ancestors
-template <int BT>
-__global__ void __launch_bounds__(BT) k_search(const double* __restrict__ C, int J, const StepState* st,
-                                               uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
-  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  __shared__ int s_ns, s_fail;
-  {
-    const int r = blockIdx.y;
-    C += (size_t)r * J;
-    st += r;
-    anc += (size_t)r * J;
-    if (anc_hist) anc_hist += (size_t)r * J;
-  }
-  if (threadIdx.x == 0) {
-    s_ns = st->nseg;
-    s_fail = st->all_fail;
-  }
-  __syncthreads();
-  const int ns = s_ns;
-  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = st->seg[i];
-  __syncthreads();
-  const int j = blockIdx.x * BT + threadIdx.x;
-  if (j >= J) return;
-  uint32_t r;
-  if (s_fail || ns == 0) {
-    r = (uint32_t)j;
-  } else {
-    const double ran = plomrt::systematic_point(seg, ns, j);
-    int lo = 0, hi = J - 1;
-    while (lo < hi) {  // first i with !(ran > C[i])  (smc.c:105-108)
-      const int mid = (lo + hi) >> 1;
-      if (ran > __ldg(C + mid)) lo = mid + 1; else hi = mid;
-    }
-    r = (uint32_t)lo;
-  }
-  anc[j] = r;
-  if (anc_hist) anc_hist[j] = r;
+__device__ __forceinline__ bool weight_fails_at(T l, double fail_b) {
+  return !((double)l > fail_b);
 }
 
 // ------------------------------------------------------------------ tiled resampling
 // weight() + systematic_sampling() (model_builder/C/core/smc.c:27-112) over
-// tiles of TILE consecutive particles, in three launches:
-//   k_weight_tiles  per tile: (max, sum exp(l - max), sum exp(2 (l - max)),
-//                   failures); the last block folds them in tile order
-//                   (llike, ESS, all-fail rule, systematic points) and lays out
-//                   the exclusive prefix P[b] of the tiles' normalised weights;
-//   k_cum_tiles     per tile: the cumulative weights of its particles
-//                   C_i = P[b] + (prefix of exp(l - max_b)) * exp(max_b - max) / sum;
-//   k_search_tiles  per tile of points: the ancestor of every systematic point
-//                   (first i with C_i >= point_j).
-// The tile prefixes come from the fold (no look-back across tiles), the
-// points are placed by a search over all cumulative weights (balanced however
-// the weights concentrate), and every reduction runs in a fixed order
-// (results do not depend on timing).
+// tiles of TILE consecutive particles, in two launches (a third only when
+// the weights concentrate):
+//   k_weight_tiles    per tile: (max, sum exp(l - max), sum exp(2 (l - max)),
+//                     failures); the last block folds them in tile order
+//                     (llike, ESS, all-fail rule, systematic points) and lays
+//                     out the exclusive prefix P[b] of the tiles' normalised
+//                     weights;
+//   k_resample_tiles  per tile: the cumulative weights of its particles,
+//                     C_i = P[b] + (prefix of exp(l - max_b)) * exp(max_b - max) / sum,
+//                     in shared memory, and the ancestors of the systematic
+//                     points that fall in the tile (P[b] < point <= P[b + 1]):
+//                     the first i of the tile with C_i >= point (smc.c:105-108);
+//   k_resample_heavy  the points of tiles that hold more than kHeavyPoints of
+//                     them, shared by all blocks (the weights have concentrated
+//                     on a few tiles; the tile's cumulative weights go through
+//                     global memory).
+// The cumulative weights never make a round trip through global memory in
+// the common case, the tile prefixes come from the fold (no look-back across
+// tiles), and every reduction runs in a fixed order (results do not depend on
+// timing).  Tile ends are the fold's prefixes P[b], so every point belongs to
+// exactly one tile; a point that rounding leaves above the tile's last C_i
+// goes to the tile's last particle (the reference reads on past the array).
+// b: the failure boundary (fail_boundary)
 template <class T>
-__device__ __forceinline__ double surviving_exp(T l, double thresh, double m) {
-  return weight_fails(l, thresh) ? 0.0 : exp((double)l - m);
+__device__ __forceinline__ double surviving_exp(T l, double b, double m) {
+  return weight_fails_at(l, b) ? 0.0 : exp((double)l - m);
+}
+
+// points of a tile resampled by its own block; above, the tile goes to k_resample_heavy
+constexpr int kHeavyTiles = 8;  // in tiles' worth of points
+
+// (tile, first point, end of points, particles) of a tile left to k_resample_heavy
+struct HeavyTile {
+  int b, jlo, jhi, n_in;
+};
+
+// #{j in [0, J) : point_j <= x}: points are U + j / J to within rounding far
+// below their spacing, so an estimate is corrected by a step or two.
+__device__ inline int points_at_or_below(const plomrt::SysSeg* seg, int ns, int J, double U, double x) {
+  if (!(x >= U)) return 0;
+  const double e = floor((x - U) * (double)J) + 1.0;
+  int c = (e >= (double)J) ? J : (int)e;
+  while (c > 0 && !(plomrt::systematic_point(seg, ns, c - 1) <= x)) --c;
+  while (c < J && plomrt::systematic_point(seg, ns, c) <= x) ++c;
+  return c;
+}
+
+// first i in [0, n) with !(x > c[i]), or n - 1 if every c[i] < x
+__device__ __forceinline__ int tile_lower_bound(const double* c, int n, double x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (x > c[mid]) lo = mid + 1; else hi = mid;
+  }
+  return lo;
 }
 
 // Shared scratch of the weighting / resampling of one tile (BT threads,
@@ -1027,7 +826,7 @@ struct TileScratch {
   double swarp[BT / 32];
   LseAcc lse[BT / 32];
   plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  int ns, fail, jlo, jhi, lastpos, last;
+  int ns, fail, jlo, jhi;
 };
 
 // (max, sum exp(l - max), sum exp(2 (l - max)), failures) of the threads'
@@ -1068,14 +867,31 @@ __device__ __forceinline__ LseAcc block_lse_all(LseAcc a, LseAcc* sh) {
   return r;
 }
 
+// The systematic points of interval n (smc.c:97-101): U = inc * u and the
+// run table of the J points ran += inc.  They depend on the interval's
+// uniform alone, so one thread lays them out while the others reduce the
+// weights (before its block's ticket, so the fold and the resampling see them).
+__device__ inline void systematic_points(StepState* st, FilterAcc* acc, int J, int n, double U_crn,
+                                         plomrt::PhiloxKey key) {
+  const double inc = 1.0 / (double)J;
+  const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(key, (uint32_t)n);
+  const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
+  st->U = U;
+  int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
+  if (ns < 0) {
+    atomicOr(&acc->error, (int)ERR_SYS_TABLE);
+    ns = 0;
+  }
+  st->nseg = ns;
+}
+
 // The fold of the tile partials by one block (all threads call it): the
 // filter's (max, sums, failures) in tile order, the exclusive prefix P[b] of
 // the tiles' normalised weights (P[ntiles] = their total), llike, ESS, the
 // all-fail rule (smc.c:55-69) and the systematic points of the interval.
 template <int BT>
 __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_like_min, double* P, StepState* st,
-                           FilterAcc* acc, int n, double U_crn, plomrt::PhiloxKey key, double* llike_out,
-                           double* ess_out, LseAcc* sh, double* shd) {
+                           FilterAcc* acc, int n, double* llike_out, double* ess_out, LseAcc* sh, double* shd) {
   const int chunk = (ntiles + BT - 1) / BT;
   const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
   // the partials of the other blocks are read from L2 (written before their
@@ -1143,21 +959,12 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
     st->all_fail = all_fail;
     if (llike_out) llike_out[n] = llike;
     if (ess_out) ess_out[n] = ess;
-    const double inc = 1.0 / (double)J;
-    const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(key, (uint32_t)n);
-    const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
-    st->U = U;
-    int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
-    if (ns < 0) {
-      acc->error |= ERR_SYS_TABLE;
-      ns = 0;
-    }
-    st->nseg = ns;
+    st->nheavy = 0;
   }
 }
 
 template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double thresh,
+__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double fail_b,
                                                      double log_like_min, LseAcc* part, double* P, StepState* st,
                                                      FilterAcc* acc, int n, double U_crn, const uint64_t* seed,
                                                      uint32_t filter_id, double* llike_out, double* ess_out,
@@ -1177,20 +984,28 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
     if (ess_out) ess_out += (size_t)r * out_stride;
     filter_id += (uint32_t)r;
   }
+  static_assert(BT >= 64, "a thread of the second warp lays out the systematic points");
+  if (blockIdx.x == 0 && threadIdx.x == 32)
+    systematic_points(st, acc, J, n, U_crn, plomrt::make_key(seed ? *seed : 0ull, filter_id));
   const int base = blockIdx.x * BT * IPT;
+  // the thread's maximum, then its sums relative to it
+  T lv[IPT];
+  bool ok[IPT];
   LseAcc a = {-INFINITY, 0.0, 0.0, 0};
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const int i = base + k * BT + threadIdx.x;
-    if (i < J) {
-      const T l = lw[i];
-      if (weight_fails(l, thresh)) {
-        a.nfail += 1;
-      } else {
-        LseAcc b = {(double)l, 1.0, 1.0, 0};
-        a = lse_merge(a, b);
-      }
-    }
+    lv[k] = (i < J) ? lw[i] : T(0);
+    ok[k] = (i < J) && !weight_fails_at(lv[k], fail_b);
+    if (i < J && !ok[k]) a.nfail += 1;
+    if (ok[k]) a.m = fmax(a.m, (double)lv[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < IPT; ++k) {
+    if (!ok[k]) continue;
+    const double e = ((double)lv[k] == a.m) ? 1.0 : exp((double)lv[k] - a.m);
+    a.s1 += e;
+    a.s2 += e * e;
   }
   a = block_lse_all<BT>(a, sh);
   if (threadIdx.x == 0) {
@@ -1203,8 +1018,7 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   if (!last) return;
   __threadfence();
   if (threadIdx.x == 0) acc->ticket = 0u;
-  fold_tiles<BT>(part, ntiles, J, log_like_min, P, st, acc, n, U_crn, plomrt::make_key(*seed, filter_id), llike_out,
-                 ess_out, sh, shd);
+  fold_tiles<BT>(part, ntiles, J, log_like_min, P, st, acc, n, llike_out, ess_out, sh, shd);
 }
 
 // The propagate launch: one particle per thread.  (Merging the block's
@@ -1220,17 +1034,15 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
 }
 
-// Cumulative normalised weights of tile b: C_i = P[b] + (prefix of
-// exp(l - max_b) in particle order) * exp(max_b - max) / sum, written to C
+// Cumulative normalised weights of tile b: sC[i] = P[b] + (prefix of
+// exp(l - max_b) in particle order) * exp(max_b - max) / sum, i < n_in
 // (all threads of the block call it).
 template <class T, int BT, int IPT>
-__device__ void cum_tile(const T* __restrict__ lw, int J, double thresh, const LseAcc* __restrict__ part,
-                         const double* __restrict__ P, const StepState* st, int b, double* __restrict__ C,
-                         TileScratch<BT, IPT>& sc) {
+__device__ void cum_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
+                         const double* __restrict__ P, const StepState* st, int b, TileScratch<BT, IPT>& sc) {
   constexpr int TILE = BT * IPT;
   const int base = b * TILE;
   const int n_in = min(TILE, J - base);
-  if (st->all_fail) return;
   const double mb = __ldcg(&part[b].m);
   const double s1b = __ldcg(&part[b].s1);
   const double f = (s1b > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
@@ -1240,7 +1052,7 @@ __device__ void cum_tile(const T* __restrict__ lw, int J, double thresh, const L
 #pragma unroll
   for (int k = 0; k < IPT; ++k) {
     const int ii = k * BT + threadIdx.x;
-    const double p = (ii < n_in) ? surviving_exp(lw[base + ii], thresh, mb) : 0.0;
+    const double p = (ii < n_in) ? surviving_exp(lw[base + ii], fail_b, mb) : 0.0;
     double v = p;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -1260,65 +1072,111 @@ __device__ void cum_tile(const T* __restrict__ lw, int J, double thresh, const L
     }
     __syncthreads();
     const double incl = carry + ((warp > 0) ? sc.swarp[warp - 1] : 0.0) + v;
-    if (ii < n_in) C[base + ii] = Pb + incl * f;
+    sc.sC[ii] = Pb + incl * f;
     carry += sc.swarp[BT / 32 - 1];
     __syncthreads();
   }
 }
 
-// Ancestors of the systematic points j of one tile of points (TILE
-// consecutive j): the first particle i with C_i >= point_j (smc.c:105-108),
-// the last particle when rounding leaves a point above every C (the
-// reference reads on past the array); identity when every particle failed.
-template <int BT, int IPT>
-__device__ void search_tile(const double* __restrict__ C, int J, const StepState* st, int b,
-                            uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, TileScratch<BT, IPT>& sc) {
+// Tile b of one filter: its cumulative weights and the ancestors of the
+// systematic points that fall in it (all threads of the block call it).
+// heavy == nullptr: the block places all of its points however many; else a
+// tile with more than kHeavyTiles * TILE points writes its cumulative weights
+// to C and is listed for k_resample_heavy.  Identity ancestors when every
+// particle failed (smc.c:55-69).
+template <class T, int BT, int IPT>
+__device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
+                              const double* __restrict__ P, StepState* st, int b, int ntiles,
+                              uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, double* __restrict__ C,
+                              HeavyTile* heavy, TileScratch<BT, IPT>& sc) {
   constexpr int TILE = BT * IPT;
+  static_assert(BT >= 64, "two warps find the tile's points");
+  const int base = b * TILE;
+  const int n_in = min(TILE, J - base);
   if (threadIdx.x == 0) {
     sc.ns = st->nseg;
     sc.fail = st->all_fail;
   }
   __syncthreads();
+  if (sc.fail || sc.ns == 0) {
+    for (int i = threadIdx.x; i < n_in; i += BT) {
+      anc[base + i] = (uint32_t)(base + i);
+      if (anc_hist) anc_hist[base + i] = (uint32_t)(base + i);
+    }
+    __syncthreads();
+    return;
+  }
   const int ns = sc.ns;
   for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = st->seg[i];
   __syncthreads();
-  const int j1 = min(J, (b + 1) * TILE);
-  for (int j = b * TILE + threadIdx.x; j < j1; j += BT) {
-    uint32_t r;
-    if (sc.fail || ns == 0) {
-      r = (uint32_t)j;
-    } else {
+  // the tile's points, P[b] < point <= P[b + 1] (the first tile from point 0,
+  // the last to point J - 1), while the other warps start the weights
+  const double U = st->U;
+  if (threadIdx.x == 0) sc.jlo = (b == 0) ? 0 : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b));
+  if (threadIdx.x == 32) sc.jhi = (b == ntiles - 1) ? J : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b + 1));
+  cum_tile<T, BT, IPT>(lw, J, fail_b, part, P, st, b, sc);
+  const int jlo = sc.jlo, jhi = max(sc.jlo, sc.jhi);
+  if (heavy && jhi - jlo > kHeavyTiles * TILE) {
+    for (int i = threadIdx.x; i < n_in; i += BT) C[base + i] = sc.sC[i];
+    if (threadIdx.x == 0) heavy[atomicAdd(&st->nheavy, 1)] = HeavyTile{b, jlo, jhi, n_in};
+  } else {
+    for (int j = jlo + threadIdx.x; j < jhi; j += BT) {
       const double ran = plomrt::systematic_point(sc.seg, ns, j);
-      int lo = 0, hi = J - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (ran > __ldg(C + mid)) lo = mid + 1; else hi = mid;
-      }
-      r = (uint32_t)lo;
+      const uint32_t r = (uint32_t)(base + tile_lower_bound(sc.sC, n_in, ran));
+      anc[j] = r;
+      if (anc_hist) anc_hist[j] = r;
     }
-    anc[j] = r;
-    if (anc_hist) anc_hist[j] = r;
   }
+  __syncthreads();  // the scratch of one tile before the next
 }
 
 template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_cum_tiles(const T* __restrict__ lw, int J, double thresh,
-                                                  const LseAcc* __restrict__ part, const double* __restrict__ P,
-                                                  const StepState* st, double* __restrict__ C) {
+__global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw, int J, double fail_b,
+                                                       const LseAcc* __restrict__ part, const double* __restrict__ P,
+                                                       StepState* st, uint32_t* __restrict__ anc,
+                                                       uint32_t* __restrict__ anc_hist, double* __restrict__ C,
+                                                       HeavyTile* heavy) {
   __shared__ TileScratch<BT, IPT> sc;
   const int ntiles = gridDim.x;
   const int r = blockIdx.y;
-  cum_tile<T, BT, IPT>(lw + (size_t)r * J, J, thresh, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1), st + r,
-                       blockIdx.x, C + (size_t)r * J, sc);
+  resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, fail_b, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
+                            st + r, blockIdx.x, ntiles, anc + (size_t)r * J, anc_hist ? anc_hist + (size_t)r * J : nullptr,
+                            C + (size_t)r * J, heavy + (size_t)r * ntiles, sc);
 }
 
-template <int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_search_tiles(const double* __restrict__ C, int J, const StepState* st,
-                                                     uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
-  __shared__ TileScratch<BT, IPT> sc;
+// The points of the listed tiles (resample_tile), spread over all blocks:
+// the first i of the tile with C_i >= point, from C in global memory.
+template <int BT>
+__global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict__ C, int J, int ntiles, int tile,
+                                                       const StepState* st, const HeavyTile* __restrict__ heavy,
+                                                       uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
+  __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  __shared__ int s_nh, s_ns;
   const int r = blockIdx.y;
-  search_tile<BT, IPT>(C + (size_t)r * J, J, st + r, blockIdx.x, anc + (size_t)r * J,
-                       anc_hist ? anc_hist + (size_t)r * J : nullptr, sc);
+  st += r;
+  if (threadIdx.x == 0) {
+    s_nh = st->all_fail ? 0 : st->nheavy;
+    s_ns = st->nseg;
+  }
+  __syncthreads();
+  const int nh = s_nh, ns = s_ns;
+  if (nh == 0) return;
+  C += (size_t)r * J;
+  heavy += (size_t)r * ntiles;
+  anc += (size_t)r * J;
+  if (anc_hist) anc_hist += (size_t)r * J;
+  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = st->seg[i];
+  __syncthreads();
+  for (int e = 0; e < nh; ++e) {
+    const HeavyTile h = heavy[e];
+    const double* c = C + (size_t)h.b * tile;
+    for (int j = h.jlo + blockIdx.x * BT + threadIdx.x; j < h.jhi; j += gridDim.x * BT) {
+      const double ran = plomrt::systematic_point(seg, ns, j);
+      const uint32_t a = (uint32_t)(h.b * tile + tile_lower_bound(c, h.n_in, ran));
+      anc[j] = a;
+      if (anc_hist) anc_hist[j] = a;
+    }
+  }
 }
 
 // ------------------------------------------------------------------ helpers
@@ -1361,7 +1219,6 @@ __global__ void k_reset_acc(FilterAcc* acc, int R = 1) {
     acc[r].n_all_fail = 0;
     acc[r].error = 0;
     acc[r].ticket = 0u;
-    acc[r].tile_ticket = 0u;
   }
 }
 
@@ -1440,7 +1297,7 @@ __global__ void k_mif_init(const double* __restrict__ theta_hat, const double* _
 // NULL).  Grid (Q, R); components outside fls_mask are skipped.
 template <class T, int BT>
 __global__ void __launch_bounds__(BT) k_mif_fls(const T* __restrict__ lw, const T* __restrict__ theta,
-                                                const uint32_t* __restrict__ anc, int J, int R, double thresh,
+                                                const uint32_t* __restrict__ anc, int J, int R, double fail_b,
                                                 const StepState* st, unsigned fls_mask, int Q, double* out) {
   const int q = blockIdx.x, r = blockIdx.y;
   if (!((fls_mask >> q) & 1u)) return;
@@ -1456,7 +1313,7 @@ __global__ void __launch_bounds__(BT) k_mif_fls(const T* __restrict__ lw, const 
       w = 1.0 / (double)J;
     } else {
       const T l = lw[gj];
-      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+      w = weight_fails_at(l, fail_b) ? 0.0 : exp((double)l - m) / s1;
     }
     const size_t src = (size_t)r * J + (anc ? anc[gj] : (uint32_t)j);
     acc += (double)theta[(size_t)q * RJ + src] * w;
@@ -1479,7 +1336,7 @@ __global__ void __launch_bounds__(BT) k_mif_fls(const T* __restrict__ lw, const 
 // Grid (Q, R); the sums are shifted by theta_hat for a stable variance.
 template <class T, int BT>
 __global__ void __launch_bounds__(BT) k_mif_moments(const T* __restrict__ lw, const T* __restrict__ theta, int J, int R,
-                                                    double thresh, const StepState* st,
+                                                    double fail_b, const StepState* st,
                                                     const double* __restrict__ theta_hat, const double* __restrict__ vt_add,
                                                     int Q, int n, int n_obs, double* bart, double* vt) {
   const int q = blockIdx.x, r = blockIdx.y;
@@ -1497,7 +1354,7 @@ __global__ void __launch_bounds__(BT) k_mif_moments(const T* __restrict__ lw, co
       w = 1.0 / (double)J;
     } else {
       const T l = lw[g];
-      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+      w = weight_fails_at(l, fail_b) ? 0.0 : exp((double)l - m) / s1;
     }
     sw += w * th;
     const double d = th - c;
@@ -1680,7 +1537,7 @@ template <class T>
 __global__ void k_hat_values(const T* __restrict__ X, int J, const double* __restrict__ pop_size,
                              const double* __restrict__ par_ts, const double* __restrict__ cov_ts, double t_obs,
                              const plomrt::BackTransform* __restrict__ drift_bt, const T* __restrict__ lw,
-                             const StepState* st, int weighted, double thresh, double* __restrict__ vals) {
+                             const StepState* st, int weighted, double fail_b, double* __restrict__ vals) {
   const bool uni = !weighted || st->all_fail;
   const double m = uni ? 0.0 : st->m, s1 = uni ? 1.0 : st->s1;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J; j += gridDim.x * blockDim.x) {
@@ -1689,7 +1546,7 @@ __global__ void k_hat_values(const T* __restrict__ X, int J, const double* __res
     double w = 1.0;
     if (!uni) {
       const T l = lw[j];
-      w = weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+      w = weight_fails_at(l, fail_b) ? 0.0 : exp((double)l - m) / s1;
     }
     vals[(size_t)kHatW * J + j] = w;
   }
@@ -1873,7 +1730,7 @@ __global__ void __launch_bounds__(BT) k_pred_res(const double* __restrict__ vals
 // [r][S].  One block; the walk is serial (T steps), the gathers parallel.
 template <class T, int BT>
 __global__ void __launch_bounds__(BT) k_sample_traj(const T* __restrict__ lw, int J, const StepState* st,
-                                                    double thresh, double u, int n_obs,
+                                                    double fail_b, double u, int n_obs,
                                                     const int* __restrict__ data_idx, int n_data,
                                                     const uint32_t* __restrict__ anc_hist,
                                                     const double* __restrict__ x_hist, const double* __restrict__ x0,
@@ -1886,7 +1743,7 @@ __global__ void __launch_bounds__(BT) k_sample_traj(const T* __restrict__ lw, in
   auto wgt = [&](int j) -> double {
     if (uni) return 1.0 / (double)J;
     const T l = lw[j];
-    return weight_fails(l, thresh) ? 0.0 : exp((double)l - m) / s1;
+    return weight_fails_at(l, fail_b) ? 0.0 : exp((double)l - m) / s1;
   };
   // first j with inclusive running weight >= u: chunk sums, a serial scan of
   // BT partial sums, then a serial search inside the chunk that crosses

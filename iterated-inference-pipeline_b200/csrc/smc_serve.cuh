@@ -126,8 +126,9 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
 //   propagate(n)  the tile's particles over interval n (gather from the
 //                 ancestors, substeps, log-weights) and the tile's
 //                 log-sum-exp partial;
-//   cumulate(n)   the cumulative normalised weights of the tile (cum_tile);
-//   search(n)     the ancestors of the tile's systematic points (search_tile).
+//   resample(n)   the cumulative normalised weights of the tile and the
+//                 ancestors of the systematic points that fall in it
+//                 (resample_tile).
 // The CTA that finishes the last tile of a phase does the phase's serial
 // part itself (the fold of the partials: llike, ESS, all-fail rule,
 // systematic points, tile prefixes) and publishes the next phase; nothing
@@ -149,7 +150,7 @@ struct TileReq {
                                           // never matches
   alignas(128) unsigned done;             // tiles of the current phase finished
   alignas(128) int n;                     // interval of the current phase
-  int kind;                  // 0 propagate, 1 cumulate, 2 search
+  int kind;                  // 0 propagate, 1 resample
   int cur;                   // generation holding the particles before interval n
   int resampled;             // the ancestors of interval n - 1 apply (else identity)
   int slot;                  // ring slot of the request (its result)
@@ -171,7 +172,6 @@ struct TileReqWs {
   double* P;
   T* lw;
   uint32_t* anc;
-  double* C;
   T* X[2];
   T* par_cac;
   double* par_ts;
@@ -185,8 +185,7 @@ __host__ __device__ inline size_t tile_req_bytes(int J) {
   const size_t nt = (size_t)((J + BT - 1) / BT);
   const size_t mj = (size_t)((J + 31) & ~31);
   return ws_align(sizeof(TileReq)) + ws_align(nt * sizeof(LseAcc)) + ws_align((nt + 1) * sizeof(double)) +
-         ws_align(mj * sizeof(T)) + ws_align(mj * sizeof(uint32_t)) + ws_align(mj * sizeof(double)) +
-         2 * ws_align((size_t)M::S * mj * sizeof(T)) +
+         ws_align(mj * sizeof(T)) + ws_align(mj * sizeof(uint32_t)) + 2 * ws_align((size_t)M::S * mj * sizeof(T)) +
          ws_align((size_t)kServeParCac * sizeof(T)) + ws_align((size_t)kServeParTs * sizeof(double)) +
          ws_align((size_t)M::S * sizeof(double));
 }
@@ -207,8 +206,6 @@ __device__ inline TileReqWs<T> tile_req_ws(unsigned char* base, int J) {
   p += ws_align(mj * sizeof(T));
   w.anc = reinterpret_cast<uint32_t*>(p);
   p += ws_align(mj * sizeof(uint32_t));
-  w.C = reinterpret_cast<double*>(p);
-  p += ws_align(mj * sizeof(double));
   w.X[0] = reinterpret_cast<T*>(p);
   p += ws_align((size_t)M::S * mj * sizeof(T));
   w.X[1] = reinterpret_cast<T*>(p);
@@ -392,7 +389,6 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         q->acc.n_all_fail = 0;
         q->acc.error = 0;
         q->acc.ticket = 0u;
-        q->acc.tile_ticket = 0u;
         __threadfence();
         atomicExch(&q->phase, ((unsigned long long)(s_req & 0xfffff) << 12) << 32);
         __threadfence();
@@ -443,19 +439,20 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       double l = NAN;
       if (g < (size_t)J) l = propagate_particle<T, V, DRIFT, false, kSmem, false, BT, false, false>(tb, sa, g, smem_raw);
       __syncthreads();  // the state columns are free again
+      if (weigh && tile == 0 && threadIdx.x == 32)
+        systematic_points(&q->st, &q->acc, J, n, -1.0, plomrt::make_key(q->seed, 0u));
       if (weigh) {
         LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
         if (g < (size_t)J) {
-          if (weight_fails(l, a.thresh)) acc.nfail = 1;
+          if (weight_fails_at(l, a.fail_b)) acc.nfail = 1;
           else acc = LseAcc{l, 1.0, 1.0, 0};
         }
         acc = block_lse_all<BT>(acc, sc.lse);
         if (threadIdx.x == 0) w.part[tile] = acc;
       }
-    } else if (kind == 1) {
-      cum_tile<T, BT, 1>(w.lw, J, a.thresh, w.part, w.P, &q->st, tile, w.C, sc);
     } else {
-      search_tile<BT, 1>(w.C, J, &q->st, tile, w.anc, nullptr, sc);
+      resample_tile<T, BT, 1>(w.lw, J, a.fail_b, w.part, w.P, &q->st, tile, ntiles, w.anc, nullptr, nullptr, nullptr,
+                              sc);
     }
     __syncthreads();  // the shared scratch of one tile before the next
     }
@@ -473,8 +470,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
     if (kind == 0) {
       next_cur = q->cur ^ 1;
       if (weigh) {
-        fold_tiles<BT>(w.part, ntiles, J, a.log_like_min, w.P, &q->st, &q->acc, n, -1.0,
-                       plomrt::make_key(q->seed, 0u), nullptr, nullptr, sc.lse, sc.swarp);
+        fold_tiles<BT>(w.part, ntiles, J, a.log_like_min, w.P, &q->st, &q->acc, n, nullptr, nullptr, sc.lse,
+                       sc.swarp);
         if (n == T_obs - 1) finished = true;
         else next_kind = 1;
       } else {
@@ -482,8 +479,6 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         next_n = n + 1;
         if (next_n == T_obs) finished = true;
       }
-    } else if (kind == 1) {
-      next_kind = 2;
     } else {
       next_kind = 0;
       next_res = 1;

@@ -91,8 +91,10 @@ def build_model(model, name, force=False, verbose=False, out=None):
     os.makedirs(os.path.dirname(out), exist_ok=True)
     stamp_file = out + '.stamp'
     cmd = nvcc_command(name, S, out=out)
-    # the compile line (flags included, output path excluded) is part of the stamp
-    stamp = _stamp(name, {'S': S, 'arch': ARCH, 'cmd': [c for c in cmd if c != out]})
+    # the compile line (flags included, output path excluded, directories relative to
+    # the repository so that a moved checkout keeps its builds) is part of the stamp
+    stamp = _stamp(name, {'S': S, 'arch': ARCH,
+                          'cmd': [c.replace(REPO_ROOT, '<repo>') for c in cmd if c != out]})
     if not force and os.path.exists(out) and os.path.exists(stamp_file) and open(stamp_file).read() == stamp:
         return out
     if verbose:

@@ -99,6 +99,41 @@ def test_noalloc_single_precision_log_weights():
     assert np.array_equal(out32, out32b)
 
 
+@pytest.mark.parametrize('precision', [64, 32])
+def test_noalloc_concentrated_weights(precision):
+    """Weights concentrated on a few particles: the tiles holding them take far
+    more than 8 tiles' worth of systematic points, which the second resampling
+    launch spreads over all blocks.  Ancestors equal the oracle's weight() +
+    systematic_sampling() bit for bit, with failing particles mixed in, and
+    every particle failing gives identity ancestors."""
+    eng = models.engine('sir_short')
+    orc = models.build_oracle('sir_short')
+    rng = np.random.default_rng(7)
+    J = 200000
+    lw = -30.0 + rng.standard_normal(J)          # survive, but carry no points
+    lw[rng.integers(0, J, 5000)] = -45.0         # fail: exp(-45) <= LIKE_MIN
+    lw[51200:51500] = rng.uniform(-1.0, 0.0, 300)          # tile 50: most of the mass
+    lw[153700:153710] = rng.uniform(-2.0, -1.0, 10)        # tile 150: some of it
+    lw[2000:3000] = rng.uniform(-9.0, -8.0, 1000)          # tiles 1-2: a few points
+    if precision == 32:
+        lw = lw.astype(np.float32)
+    wide = lw.astype(np.float64)
+    for u in (0.25, 0.8125):
+        anc, out = _noalloc(eng, lw, u, precision=precision)
+        _, sel, ll, ess, fail = orc.weight_and_resample(np.exp(wide), (1.0 / J) * u)
+        assert not fail
+        np.testing.assert_array_equal(anc, sel)
+        assert out[0] == pytest.approx(ll, rel=1e-9)
+        assert out[1] == pytest.approx(ess, rel=1e-8)
+        assert out[2] == 0.0 and out[3] == 0.0
+        counts = np.bincount(anc // 1024, minlength=J // 1024 + 1)
+        assert counts[50] > 8 * 1024 and counts[150] > 0
+    dead = np.full(J, -50.0, dtype=lw.dtype)
+    anc, out = _noalloc(eng, dead, 0.5, precision=precision)
+    np.testing.assert_array_equal(anc, np.arange(J, dtype=np.uint32))
+    assert out[2] == 1.0
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     import torch
     eng = models.engine('sir_short')
