@@ -211,7 +211,9 @@ def ncu_issue(workload):
         with open(path) as f:
             d = json.load(f)
         return {'issue_slots_active_pct': d['issue_active_pct'], 'ipc': d['ipc'],
-                'warps_active_per_sm': d['warps_active_per_sm'], 'source': 'profiles/k_propagate_%s.md' % workload}
+                'warps_active_per_sm': d['warps_active_per_sm'],
+                'source': 'profiles/k_propagate_%s.md (ncu capture of %s, not this run)' % (workload,
+                                                                                        d.get('captured', '?'))}
     except (OSError, KeyError, ValueError):
         return None
 

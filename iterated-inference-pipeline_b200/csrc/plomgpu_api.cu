@@ -76,6 +76,12 @@ constexpr int kBtProp = 128;
 #define PLOM_TEAM 1
 #endif
 constexpr int kTeam = kSmem ? PLOM_TEAM : 1;
+// particles per thread of the register-state propagate launch (shared-memory
+// states: one)
+#ifndef PLOM_PROP_PPT
+#define PLOM_PROP_PPT 1
+#endif
+constexpr int kPropPpt = kSmem ? 1 : PLOM_PROP_PPT;
 constexpr int kBtOde = 64;
 constexpr int kOdeMaxSteps = 1000000;  // attempted RKF45 steps per interval
 static_assert(kTeam == 1 || kTeam == 2 || kTeam == 4 || kTeam == 8 || kTeam == 16 || kTeam == 32,
@@ -117,6 +123,9 @@ struct plomgpu_plan {
   double* C = nullptr;            // [R][J] cumulative normalised weights of tiles left to k_resample_heavy
   HeavyTile* heavy = nullptr;     // [R][ntiles] those tiles
   int heavy_blocks = 1;
+  int weight_blocks = 1;          // blocks of k_weight_tiles (each folds a share of the tiles)
+  SysTable* sys = nullptr;        // [R][n_obs] systematic points of every interval
+  double* crn_u_d = nullptr;      // [n_obs] injected resampling uniforms
   uint32_t* anc[2] = {nullptr, nullptr};
   LseAcc* part = nullptr;         // [R][ntiles] tile partials
   StepState* st = nullptr;
@@ -272,9 +281,9 @@ PropLaunch<T> pick4() {
     l.per_block = L::PB;
     l.smem = L::bytes();
   } else {
-    l.k = &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp, false, MULTI>;
+    l.k = &k_propagate<T, V, DRIFT, CRN, kSmem, MIF, kBtProp, false, MULTI, kPropPpt>;
     l.bt = kBtProp;
-    l.per_block = kBtProp;
+    l.per_block = kBtProp * kPropPpt;
     l.smem = propagate_smem_bytes<T, kSmem, kBtProp>();
   }
   return l;
@@ -390,6 +399,9 @@ int enqueue_filter(plomgpu_plan* p) {
   }
   k_reset_acc<<<1, 128, 0, s>>>(p->acc, R);
   ++kernels;
+  // every interval's systematic points (they depend on the seed alone)
+  k_sys_tables<<<(p->n_obs * R + 63) / 64, 64, 0, s>>>(J, p->n_obs, R, p->seed, 0u, p->crn_u_d, -1.0, p->sys, p->acc);
+  ++kernels;
   {
     const size_t total = (size_t)M::OFF_INC * RJ;
     const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
@@ -461,10 +473,9 @@ int enqueue_filter(plomgpu_plan* p) {
     if (p->mif) th_cur ^= 1;
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
-      const double Uc = p->crn_tab ? p->crn_u[n] : -1.0;
-      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n, Uc, p->seed, 0u,
-          p->llike, p->ess, p->n_obs);
+      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->weight_blocks, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->ntiles, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n, p->llike,
+          p->ess, p->n_obs);
       ++kernels;
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
@@ -474,10 +485,11 @@ int enqueue_filter(plomgpu_plan* p) {
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
       k_resample_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->fail_b, p->part, p->P, p->st, p->anc[nxt],
+          (const T*)p->lw, J, p->fail_b, p->part, p->P, p->st, p->sys + n, p->n_obs, p->anc[nxt],
           p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr, p->C, p->heavy);
       k_resample_heavy<256><<<dim3(p->heavy_blocks, R), 256, 0, s>>>(
-          p->C, J, p->ntiles, kTileRes, p->st, p->heavy, p->anc[nxt], p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+          p->C, J, p->ntiles, kTileRes, p->st, p->sys + n, p->n_obs, p->heavy, p->anc[nxt],
+          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
       kernels += 2;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);
@@ -605,6 +617,8 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(cudaMalloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
   CK(cudaMalloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
   p->heavy_blocks = std::min(p->ntiles, 2 * 148);
+  p->weight_blocks = std::min(p->ntiles, 4 * 148);
+  CK(cudaMalloc((void**)&p->sys, (size_t)p->R * p->n_obs * sizeof(SysTable)));
   CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
   CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
   CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
@@ -653,6 +667,7 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   if (d->crn_normals) {
     const size_t nd = (size_t)J * p->sub_total * draws_per_substep(d->noises_off);
     if ((rc = upload<double>(d->crn_normals, nd, &p->crn_tab, s))) return rc;
+    if ((rc = upload<double>(p->crn_u.data(), p->crn_u.size(), &p->crn_u_d, s))) return rc;
   }
   if (p->want_llike) {
     const size_t no = (size_t)p->R * (d->n_obs > 0 ? d->n_obs : 1);
@@ -738,7 +753,7 @@ void plan_free(plomgpu_plan* p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->C, p->heavy, p->anc[0], p->anc[1], p->part, p->st, p->acc,
+  void* bufs[] = {p->X[0], p->X[1], p->lw, p->P, p->C, p->heavy, p->sys, p->crn_u_d, p->anc[0], p->anc[1], p->part, p->st, p->acc,
                   p->par_cac, p->par_cac_d, p->cov_cac, p->coupling, p->drift_vol, p->drift_group,
                   p->drift_ngroups, p->drift_bt, p->par_ts, p->t_sub, p->cov_ts, p->data, p->x0, p->crn_tab,
                   p->seed, p->llike, p->ess, p->anc_hist, p->x_hist, p->x_final, p->theta[0], p->theta[1],
@@ -1349,8 +1364,9 @@ __global__ void k_noalloc_out(const StepState* st, const FilterAcc* acc, double*
   out[3] = (double)acc->error;
 }
 
-// the filters' own weighting / resampling launches (k_weight_tiles,
-// k_resample_tiles, k_resample_heavy) over tiles of 1024 particles
+// the filters' own weighting / resampling launches (k_sys_tables,
+// k_weight_tiles, k_resample_tiles, k_resample_heavy) over tiles of 1024
+// particles
 template <class T>
 int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, double* out, cudaStream_t s,
                 NoAllocScratch* sc) {
@@ -1359,11 +1375,14 @@ int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, do
   // the accumulator and its ticket must start at zero; the previous call's
   // contents are still there
   k_reset_acc<<<1, 1, 0, s>>>(&sc->acc);
-  k_weight_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(
-      lw, J, fail_b, log(like_min), sc->part, sc->P, &sc->st, &sc->acc, 0, u, nullptr, 0u, out, out + 1, 0);
-  k_resample_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(lw, J, fail_b, sc->part, sc->P, &sc->st,
-                                                                             anc, nullptr, sc->C, sc->heavy);
-  k_resample_heavy<256><<<ntiles, 256, 0, s>>>(sc->C, J, ntiles, kNoAllocTile, &sc->st, sc->heavy, anc, nullptr);
+  k_sys_tables<<<1, 32, 0, s>>>(J, 1, 1, nullptr, 0u, nullptr, u, &sc->st.tab, &sc->acc);
+  k_weight_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(lw, J, ntiles, fail_b, log(like_min),
+                                                                           sc->part, sc->P, &sc->st, &sc->acc, 0,
+                                                                           out, out + 1, 0);
+  k_resample_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(
+      lw, J, fail_b, sc->part, sc->P, &sc->st, &sc->st.tab, 0, anc, nullptr, sc->C, sc->heavy);
+  k_resample_heavy<256><<<ntiles, 256, 0, s>>>(sc->C, J, ntiles, kNoAllocTile, &sc->st, &sc->st.tab, 0, sc->heavy,
+                                               anc, nullptr);
   k_noalloc_out<<<1, 1, 0, s>>>(&sc->st, &sc->acc, out);
   CK(cudaGetLastError());
   return PLOMGPU_OK;

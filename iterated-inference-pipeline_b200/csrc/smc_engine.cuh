@@ -729,15 +729,20 @@ __device__ __forceinline__ LseAcc lse_shfl(LseAcc a, int off) {
   return lse_merge(a, b);
 }
 
+// The systematic points of one interval: U and the run table of ran += 1/J.
+struct SysTable {
+  double U;
+  int ns;  // runs (0 if the table overflowed)
+  int pad;
+  plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+};
+
 // Per-filter device state of the current interval.
 struct StepState {
   double m, s1, s2;
   int all_fail;
-  int nseg;
-  double U;
-  int nheavy;  // tiles whose points are left to k_resample_heavy
-  int pad;
-  plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  unsigned long long heavy;  // tiles left to k_resample_heavy << 32 | their points
+  SysTable tab;  // the interval's systematic points where no table array holds them (serving loop, no-allocation call)
 };
 
 struct FilterAcc {
@@ -791,9 +796,10 @@ __device__ __forceinline__ double surviving_exp(T l, double b, double m) {
 // points of a tile resampled by its own block; above, the tile goes to k_resample_heavy
 constexpr int kHeavyTiles = 8;  // in tiles' worth of points
 
-// (tile, first point, end of points, particles) of a tile left to k_resample_heavy
+// (tile, first point, end of points, particles, points of the tiles listed
+// before it) of a tile left to k_resample_heavy
 struct HeavyTile {
-  int b, jlo, jhi, n_in;
+  int b, jlo, jhi, n_in, off;
 };
 
 // #{j in [0, J) : point_j <= x}: points are U + j / J to within rounding far
@@ -869,20 +875,31 @@ __device__ __forceinline__ LseAcc block_lse_all(LseAcc a, LseAcc* sh) {
 
 // The systematic points of interval n (smc.c:97-101): U = inc * u and the
 // run table of the J points ran += inc.  They depend on the interval's
-// uniform alone, so one thread lays them out while the others reduce the
-// weights (before its block's ticket, so the fold and the resampling see them).
-__device__ inline void systematic_points(StepState* st, FilterAcc* acc, int J, int n, double U_crn,
-                                         plomrt::PhiloxKey key) {
+// uniform alone, not on the weights.
+__device__ inline void sys_table(SysTable* t, FilterAcc* acc, int J, int n, double U_crn, plomrt::PhiloxKey key) {
   const double inc = 1.0 / (double)J;
   const double u = (U_crn >= 0.0) ? U_crn : plomrt::resample_uniform(key, (uint32_t)n);
   const double U = inc * u;  // gsl_ran_flat(0, inc) = 0*(1-u) + inc*u
-  st->U = U;
-  int ns = plomrt::systematic_table(U, inc, J, st->seg, plomrt::SYS_MAX_SEG);
+  t->U = U;
+  int ns = plomrt::systematic_table(U, inc, J, t->seg, plomrt::SYS_MAX_SEG);
   if (ns < 0) {
     atomicOr(&acc->error, (int)ERR_SYS_TABLE);
     ns = 0;
   }
-  st->nseg = ns;
+  t->ns = ns;
+}
+
+// Every interval's systematic points of R filters, one thread per (filter,
+// interval), before the first interval: out[r * n_obs + n].  u_one >= 0
+// gives the uniform of a single interval; else crn_u[n] (common random
+// numbers) or the filter's Philox uniform (filter_id + r).
+__global__ void k_sys_tables(int J, int n_obs, int R, const uint64_t* seed, uint32_t filter_id,
+                             const double* __restrict__ crn_u, double u_one, SysTable* out, FilterAcc* acc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_obs * R) return;
+  const int r = t / n_obs, n = t - r * n_obs;
+  const double Uc = (u_one >= 0.0) ? u_one : (crn_u ? crn_u[n] : -1.0);
+  sys_table(out + t, acc + r, J, n, Uc, plomrt::make_key(seed ? *seed : 0ull, filter_id + (uint32_t)r));
 }
 
 // The fold of the tile partials by one block (all threads call it): the
@@ -896,11 +913,20 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
   // the partials of the other blocks are read from L2 (written before their
   // ticket, after a fence)
+  // the chunk's maximum, then its sums rescaled to it (one exponential per tile)
   LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+  for (int b = b0; b < b1; ++b)
+    if (__ldcg(&part[b].s1) > 0.0) a.m = fmax(a.m, __ldcg(&part[b].m));
   for (int b = b0; b < b1; ++b) {
     const LseAcc* p = part + b;
-    LseAcc v = {__ldcg(&p->m), __ldcg(&p->s1), __ldcg(&p->s2), __ldcg(&p->nfail)};
-    a = lse_merge(a, v);
+    const double s1b = __ldcg(&p->s1);
+    a.nfail += __ldcg(&p->nfail);
+    if (s1b > 0.0) {
+      const double mb = __ldcg(&p->m);
+      const double f = (mb == a.m) ? 1.0 : exp(mb - a.m);
+      a.s1 += s1b * f;
+      a.s2 += __ldcg(&p->s2) * f * f;
+    }
   }
   a = block_lse_all<BT>(a, sh);
   const int all_fail = (a.nfail == J);
@@ -959,20 +985,21 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
     st->all_fail = all_fail;
     if (llike_out) llike_out[n] = llike;
     if (ess_out) ess_out[n] = ess;
-    st->nheavy = 0;
+    st->heavy = 0ull;
   }
 }
 
+// ntiles tiles of BT * IPT particles per filter over gridDim.x blocks (a
+// block takes tiles b, b + gridDim.x, ...): the tile partials, then one
+// ticket per block; the last block folds them.
 template <class T, int BT, int IPT>
-__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, double fail_b,
+__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, int ntiles, double fail_b,
                                                      double log_like_min, LseAcc* part, double* P, StepState* st,
-                                                     FilterAcc* acc, int n, double U_crn, const uint64_t* seed,
-                                                     uint32_t filter_id, double* llike_out, double* ess_out,
+                                                     FilterAcc* acc, int n, double* llike_out, double* ess_out,
                                                      int out_stride) {
   __shared__ LseAcc sh[BT / 32];
   __shared__ double shd[BT / 32];
   __shared__ bool last;
-  const int ntiles = gridDim.x;
   {
     const int r = blockIdx.y;
     lw += (size_t)r * J;
@@ -982,37 +1009,35 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
     acc += r;
     if (llike_out) llike_out += (size_t)r * out_stride;
     if (ess_out) ess_out += (size_t)r * out_stride;
-    filter_id += (uint32_t)r;
   }
-  static_assert(BT >= 64, "a thread of the second warp lays out the systematic points");
-  if (blockIdx.x == 0 && threadIdx.x == 32)
-    systematic_points(st, acc, J, n, U_crn, plomrt::make_key(seed ? *seed : 0ull, filter_id));
-  const int base = blockIdx.x * BT * IPT;
-  // the thread's maximum, then its sums relative to it
-  T lv[IPT];
-  bool ok[IPT];
-  LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int base = b * BT * IPT;
+    // the thread's maximum, then its sums relative to it
+    T lv[IPT];
+    bool ok[IPT];
+    LseAcc a = {-INFINITY, 0.0, 0.0, 0};
 #pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    const int i = base + k * BT + threadIdx.x;
-    lv[k] = (i < J) ? lw[i] : T(0);
-    ok[k] = (i < J) && !weight_fails_at(lv[k], fail_b);
-    if (i < J && !ok[k]) a.nfail += 1;
-    if (ok[k]) a.m = fmax(a.m, (double)lv[k]);
-  }
+    for (int k = 0; k < IPT; ++k) {
+      const int i = base + k * BT + threadIdx.x;
+      lv[k] = (i < J) ? lw[i] : T(0);
+      ok[k] = (i < J) && !weight_fails_at(lv[k], fail_b);
+      if (i < J && !ok[k]) a.nfail += 1;
+      if (ok[k]) a.m = fmax(a.m, (double)lv[k]);
+    }
 #pragma unroll
-  for (int k = 0; k < IPT; ++k) {
-    if (!ok[k]) continue;
-    const double e = ((double)lv[k] == a.m) ? 1.0 : exp((double)lv[k] - a.m);
-    a.s1 += e;
-    a.s2 += e * e;
+    for (int k = 0; k < IPT; ++k) {
+      if (!ok[k]) continue;
+      const double e = ((double)lv[k] == a.m) ? 1.0 : exp((double)lv[k] - a.m);
+      a.s1 += e;
+      a.s2 += e * e;
+    }
+    a = block_lse_all<BT>(a, sh);
+    if (threadIdx.x == 0) part[b] = a;
   }
-  a = block_lse_all<BT>(a, sh);
   if (threadIdx.x == 0) {
-    part[blockIdx.x] = a;
     __threadfence();
     const unsigned t = atomicAdd(&acc->ticket, 1u);
-    last = (t == (unsigned)ntiles - 1u);
+    last = (t == gridDim.x - 1u);
   }
   __syncthreads();
   if (!last) return;
@@ -1021,17 +1046,24 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   fold_tiles<BT>(part, ntiles, J, log_like_min, P, st, acc, n, llike_out, ess_out, sh, shd);
 }
 
-// The propagate launch: one particle per thread.  (Merging the block's
-// log-weights here, so that no separate launch re-reads them, measured
-// slower: the epilogue's registers cost the propagate loop more, 0.563
-// against 0.505 ms per SEIR 20x2 interval, than the launch it saves.)
-template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false>
+// The propagate launch: PPT particles per thread, BT apart (one for
+// shared-memory states).  (Merging the block's log-weights here, so that no
+// separate launch re-reads them, measured slower: the epilogue's registers
+// cost the propagate loop more, 0.563 against 0.505 ms per SEIR 20x2
+// interval, than the launch it saves.)
+template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, bool PSR = false, bool MULTI = false,
+          int PPT = 1>
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  static_assert(PPT == 1 || !SMEM, "one particle per shared-memory state column");
   propagate_tables<T, BT>(tb, smem_raw, true);
-  const size_t g = (size_t)blockIdx.x * BT + threadIdx.x;  // particle of all runs
-  if (g >= (size_t)tb.R * tb.J) return;
-  propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
+  const size_t RJ = (size_t)tb.R * tb.J;
+  const size_t g0 = (size_t)blockIdx.x * BT * PPT + threadIdx.x;  // particle of all runs
+#pragma unroll
+  for (int p = 0; p < PPT; ++p) {
+    const size_t g = g0 + (size_t)p * BT;
+    if (g < RJ) propagate_particle<T, V, DRIFT, CRN, SMEM, MIF, BT, PSR, MULTI>(tb, a, g, smem_raw);
+  }
 }
 
 // Cumulative normalised weights of tile b: sC[i] = P[b] + (prefix of
@@ -1078,15 +1110,48 @@ __device__ void cum_tile(const T* __restrict__ lw, int J, double fail_b, const L
   }
 }
 
+// run of the table that holds point j: the last with j0 <= j
+__device__ __forceinline__ int sys_run(const plomrt::SysSeg* seg, int ns, int j) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg[mid].j0 <= j) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Ancestors of the consecutive points [ja, jb) over the cumulative weights
+// c[0, n) of the tile starting at particle `first`: the first i with
+// c[i] >= point (n - 1 if none), by one search for ja and a walk for the rest
+// (points and weights both ascend).  Point values are systematic_point's.
+__device__ __forceinline__ void place_points(const plomrt::SysSeg* seg, int ns, int ja, int jb, const double* c,
+                                             int n, int first, uint32_t* __restrict__ anc,
+                                             uint32_t* __restrict__ anc_hist) {
+  if (ja >= jb) return;
+  int sg = sys_run(seg, ns, ja);
+  double ran = seg[sg].x0 + (double)(ja - seg[sg].j0) * seg[sg].step;
+  int i = tile_lower_bound(c, n, ran);
+  for (int j = ja;;) {
+    const uint32_t r = (uint32_t)(first + i);
+    anc[j] = r;
+    if (anc_hist) anc_hist[j] = r;
+    if (++j >= jb) break;
+    while (sg + 1 < ns && seg[sg + 1].j0 <= j) ++sg;
+    ran = seg[sg].x0 + (double)(j - seg[sg].j0) * seg[sg].step;
+    while (i < n - 1 && ran > c[i]) ++i;
+  }
+}
+
 // Tile b of one filter: its cumulative weights and the ancestors of the
-// systematic points that fall in it (all threads of the block call it).
-// heavy == nullptr: the block places all of its points however many; else a
-// tile with more than kHeavyTiles * TILE points writes its cumulative weights
-// to C and is listed for k_resample_heavy.  Identity ancestors when every
-// particle failed (smc.c:55-69).
+// systematic points that fall in it (all threads of the block call it),
+// each thread a run of consecutive points.  heavy == nullptr: the block
+// places all of its points however many; else a tile with more than
+// kHeavyTiles * TILE points writes its cumulative weights to C and is listed
+// for k_resample_heavy.  Identity ancestors when every particle failed
+// (smc.c:55-69).
 template <class T, int BT, int IPT>
 __device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
-                              const double* __restrict__ P, StepState* st, int b, int ntiles,
+                              const double* __restrict__ P, StepState* st, const SysTable* tab, int b, int ntiles,
                               uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, double* __restrict__ C,
                               HeavyTile* heavy, TileScratch<BT, IPT>& sc) {
   constexpr int TILE = BT * IPT;
@@ -1094,7 +1159,7 @@ __device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, co
   const int base = b * TILE;
   const int n_in = min(TILE, J - base);
   if (threadIdx.x == 0) {
-    sc.ns = st->nseg;
+    sc.ns = tab->ns;
     sc.fail = st->all_fail;
   }
   __syncthreads();
@@ -1107,25 +1172,26 @@ __device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, co
     return;
   }
   const int ns = sc.ns;
-  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = st->seg[i];
+  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = tab->seg[i];
   __syncthreads();
   // the tile's points, P[b] < point <= P[b + 1] (the first tile from point 0,
   // the last to point J - 1), while the other warps start the weights
-  const double U = st->U;
+  const double U = tab->U;
   if (threadIdx.x == 0) sc.jlo = (b == 0) ? 0 : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b));
   if (threadIdx.x == 32) sc.jhi = (b == ntiles - 1) ? J : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b + 1));
   cum_tile<T, BT, IPT>(lw, J, fail_b, part, P, st, b, sc);
   const int jlo = sc.jlo, jhi = max(sc.jlo, sc.jhi);
-  if (heavy && jhi - jlo > kHeavyTiles * TILE) {
+  const int np = jhi - jlo;
+  if (heavy && np > kHeavyTiles * TILE) {
     for (int i = threadIdx.x; i < n_in; i += BT) C[base + i] = sc.sC[i];
-    if (threadIdx.x == 0) heavy[atomicAdd(&st->nheavy, 1)] = HeavyTile{b, jlo, jhi, n_in};
-  } else {
-    for (int j = jlo + threadIdx.x; j < jhi; j += BT) {
-      const double ran = plomrt::systematic_point(sc.seg, ns, j);
-      const uint32_t r = (uint32_t)(base + tile_lower_bound(sc.sC, n_in, ran));
-      anc[j] = r;
-      if (anc_hist) anc_hist[j] = r;
+    if (threadIdx.x == 0) {
+      const unsigned long long k = atomicAdd(&st->heavy, (1ull << 32) | (unsigned long long)np);
+      heavy[k >> 32] = HeavyTile{b, jlo, jhi, n_in, (int)(k & 0xffffffffull)};
     }
+  } else {
+    const int per = (np + BT - 1) / BT;
+    const int ja = jlo + threadIdx.x * per;
+    place_points(sc.seg, ns, ja, min(jhi, ja + per), sc.sC, n_in, base, anc, anc_hist);
   }
   __syncthreads();  // the scratch of one tile before the next
 }
@@ -1133,49 +1199,63 @@ __device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, co
 template <class T, int BT, int IPT>
 __global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw, int J, double fail_b,
                                                        const LseAcc* __restrict__ part, const double* __restrict__ P,
-                                                       StepState* st, uint32_t* __restrict__ anc,
-                                                       uint32_t* __restrict__ anc_hist, double* __restrict__ C,
-                                                       HeavyTile* heavy) {
+                                                       StepState* st, const SysTable* tab, int tab_stride,
+                                                       uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist,
+                                                       double* __restrict__ C, HeavyTile* heavy) {
   __shared__ TileScratch<BT, IPT> sc;
   const int ntiles = gridDim.x;
   const int r = blockIdx.y;
   resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, fail_b, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
-                            st + r, blockIdx.x, ntiles, anc + (size_t)r * J, anc_hist ? anc_hist + (size_t)r * J : nullptr,
-                            C + (size_t)r * J, heavy + (size_t)r * ntiles, sc);
+                            st + r, tab + (size_t)r * tab_stride, blockIdx.x, ntiles, anc + (size_t)r * J,
+                            anc_hist ? anc_hist + (size_t)r * J : nullptr, C + (size_t)r * J,
+                            heavy + (size_t)r * ntiles, sc);
 }
 
-// The points of the listed tiles (resample_tile), spread over all blocks:
-// the first i of the tile with C_i >= point, from C in global memory.
+// The points of the tiles listed by resample_tile, spread evenly over all
+// threads (each a run of consecutive listed points): the first i of the
+// tile with C_i >= point, from C in global memory.
 template <int BT>
 __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict__ C, int J, int ntiles, int tile,
-                                                       const StepState* st, const HeavyTile* __restrict__ heavy,
-                                                       uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist) {
+                                                       const StepState* st, const SysTable* tab, int tab_stride,
+                                                       const HeavyTile* __restrict__ heavy, uint32_t* __restrict__ anc,
+                                                       uint32_t* __restrict__ anc_hist) {
   __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  __shared__ int s_nh, s_ns;
+  __shared__ unsigned long long s_h;
+  __shared__ int s_ns;
   const int r = blockIdx.y;
   st += r;
+  tab += (size_t)r * tab_stride;
   if (threadIdx.x == 0) {
-    s_nh = st->all_fail ? 0 : st->nheavy;
-    s_ns = st->nseg;
+    s_h = st->all_fail ? 0ull : st->heavy;
+    s_ns = tab->ns;
   }
   __syncthreads();
-  const int nh = s_nh, ns = s_ns;
+  const int nh = (int)(s_h >> 32);
+  const long long total = (long long)(s_h & 0xffffffffull);
+  const int ns = s_ns;
   if (nh == 0) return;
   C += (size_t)r * J;
   heavy += (size_t)r * ntiles;
   anc += (size_t)r * J;
   if (anc_hist) anc_hist += (size_t)r * J;
-  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = st->seg[i];
+  for (int i = threadIdx.x; i < ns; i += BT) seg[i] = tab->seg[i];
   __syncthreads();
-  for (int e = 0; e < nh; ++e) {
+  const long long nthr = (long long)gridDim.x * BT;
+  const long long per = (total + nthr - 1) / nthr;
+  long long q = ((long long)blockIdx.x * BT + threadIdx.x) * per;
+  const long long qe = min(total, q + per);
+  if (q >= qe) return;
+  int lo = 0, hi = nh - 1;  // the listed tile holding point q: the last with off <= q
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((long long)__ldg(&heavy[mid].off) <= q) lo = mid; else hi = mid - 1;
+  }
+  for (int e = lo; q < qe && e < nh; ++e) {
     const HeavyTile h = heavy[e];
-    const double* c = C + (size_t)h.b * tile;
-    for (int j = h.jlo + blockIdx.x * BT + threadIdx.x; j < h.jhi; j += gridDim.x * BT) {
-      const double ran = plomrt::systematic_point(seg, ns, j);
-      const uint32_t a = (uint32_t)(h.b * tile + tile_lower_bound(c, h.n_in, ran));
-      anc[j] = a;
-      if (anc_hist) anc_hist[j] = a;
-    }
+    const int ja = h.jlo + (int)(q - h.off);
+    const int jb = (int)min((long long)h.jhi, (long long)ja + (qe - q));
+    place_points(seg, ns, ja, jb, C + (size_t)h.b * tile, h.n_in, h.b * tile, anc, anc_hist);
+    q += jb - ja;
   }
 }
 

@@ -439,8 +439,9 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       double l = NAN;
       if (g < (size_t)J) l = propagate_particle<T, V, DRIFT, false, kSmem, false, BT, false, false>(tb, sa, g, smem_raw);
       __syncthreads();  // the state columns are free again
+      // the interval's systematic points: one thread of the first tile, before its completion count
       if (weigh && tile == 0 && threadIdx.x == 32)
-        systematic_points(&q->st, &q->acc, J, n, -1.0, plomrt::make_key(q->seed, 0u));
+        sys_table(&q->st.tab, &q->acc, J, n, -1.0, plomrt::make_key(q->seed, 0u));
       if (weigh) {
         LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
         if (g < (size_t)J) {
@@ -451,8 +452,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         if (threadIdx.x == 0) w.part[tile] = acc;
       }
     } else {
-      resample_tile<T, BT, 1>(w.lw, J, a.fail_b, w.part, w.P, &q->st, tile, ntiles, w.anc, nullptr, nullptr, nullptr,
-                              sc);
+      resample_tile<T, BT, 1>(w.lw, J, a.fail_b, w.part, w.P, &q->st, &q->st.tab, tile, ntiles, w.anc, nullptr,
+                              nullptr, nullptr, sc);
     }
     __syncthreads();  // the shared scratch of one tile before the next
     }

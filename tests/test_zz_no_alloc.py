@@ -111,7 +111,7 @@ def test_noalloc_concentrated_weights(precision):
     rng = np.random.default_rng(7)
     J = 200000
     lw = -30.0 + rng.standard_normal(J)          # survive, but carry no points
-    lw[rng.integers(0, J, 5000)] = -45.0         # fail: exp(-45) <= LIKE_MIN
+    lw[rng.integers(0, J, 5000)] = -1000.0       # fail: exp(l) <= LIKE_MIN^N_TS
     lw[51200:51500] = rng.uniform(-1.0, 0.0, 300)          # tile 50: most of the mass
     lw[153700:153710] = rng.uniform(-2.0, -1.0, 10)        # tile 150: some of it
     lw[2000:3000] = rng.uniform(-9.0, -8.0, 1000)          # tiles 1-2: a few points
@@ -128,7 +128,7 @@ def test_noalloc_concentrated_weights(precision):
         assert out[2] == 0.0 and out[3] == 0.0
         counts = np.bincount(anc // 1024, minlength=J // 1024 + 1)
         assert counts[50] > 8 * 1024 and counts[150] > 0
-    dead = np.full(J, -50.0, dtype=lw.dtype)
+    dead = np.full(J, -1000.0, dtype=lw.dtype)
     anc, out = _noalloc(eng, dead, 0.5, precision=precision)
     np.testing.assert_array_equal(anc, np.arange(J, dtype=np.uint32))
     assert out[2] == 1.0
