@@ -220,6 +220,11 @@ void *plomgpu_plan_stream(plomgpu_plan *plan);
 int plomgpu_plan_kernel_count(plomgpu_plan *plan);
 void plomgpu_plan_destroy(plomgpu_plan *plan);
 
+/* Test hook (host only, no GPU needed): the largest double whose exponential
+ * is <= thresh, which the filters compare log-weights with for the failure
+ * test of weight() (exp(loglik) <= LIKE_MIN^N_TS, smc.c:44). */
+double plomgpu_debug_fail_boundary(double thresh);
+
 /* Test hook: the first J systematic-resampling points of offset U computed by
  * the device-side closed form (GPU) into out[J]. */
 int plomgpu_debug_systematic_points(double U, int J, double *out);

@@ -87,6 +87,7 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_create_ex', 'plomgpu_plan_propagate_time',
                'plomgpu_plan_update', 'plomgpu_plan_launch', 'plomgpu_plan_results', 'plomgpu_plan_stream',
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
+               'plomgpu_debug_fail_boundary',
                'plomgpu_resample_noalloc', 'plomgpu_last_error', 'plomgpu_batch_create', 'plomgpu_batch_launch',
                'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
                'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
@@ -219,6 +220,8 @@ def _declare(lib):
     lib.plomgpu_plan_destroy.argtypes = [C.c_void_p]
     lib.plomgpu_plan_destroy.restype = None
     lib.plomgpu_debug_systematic_points.argtypes = [C.c_double, C.c_int, _dp]
+    lib.plomgpu_debug_fail_boundary.argtypes = [C.c_double]
+    lib.plomgpu_debug_fail_boundary.restype = C.c_double
     lib.plomgpu_debug_draws.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, _dp]
     lib.plomgpu_resample_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                              C.c_void_p, C.c_void_p, C.c_void_p]

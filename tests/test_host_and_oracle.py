@@ -24,6 +24,24 @@ def test_header_symbols_are_bound():
     assert header_symbols() == sorted(native.API_SYMBOLS)
 
 
+def test_failure_boundary_is_exact():
+    """The filters fail a particle when loglik <= b, b the largest double with
+    exp(b) <= LIKE_MIN^N_TS (host code of the library, no GPU): on both sides
+    of b the host's exp decides as weight() does (smc.c:44), including
+    thresholds that underflow to zero and the all-survive edge."""
+    import math
+    models.build_gpu('sir')
+    lib = native.load(models.lib_name('sir'))
+    for like_min, n_ts in ((1e-17, 1), (1e-17, 2), (1e-17, 20), (1e-300, 3), (0.5, 1), (1e-5, 7)):
+        thresh = like_min ** n_ts
+        b = lib.plomgpu_debug_fail_boundary(thresh)
+        assert math.isfinite(b)
+        assert math.exp(b) <= thresh
+        assert math.exp(math.nextafter(b, math.inf)) > thresh
+    assert lib.plomgpu_debug_fail_boundary(0.0) < -700.0
+    assert lib.plomgpu_debug_fail_boundary(math.inf) == math.inf
+
+
 @pytest.mark.parametrize('name', ['sir', 'seir3'])
 def test_library_loads_and_exports_every_symbol(name):
     path = models.build_gpu(name)
