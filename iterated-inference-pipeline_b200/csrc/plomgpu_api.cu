@@ -91,12 +91,9 @@ static_assert(kTeam == 1 || kTeam == 2 || kTeam == 4 || kTeam == 8 || kTeam == 1
 // the propagate block's particles for shared-memory models (the tiles of the
 // serving loop, so that a served request and the plain filter reduce in the
 // same order), 1024 particles otherwise
-constexpr int kTileRes = kSmem ? kBtProp : 1024;
-// warps per block of the weighting launch (the fold runs on one such block:
-// 128 threads like the serving loop's CTA for shared-memory models) and of
-// the resampling launch (a warp per tile)
-constexpr int kWarpsWeight = kSmem ? kBtProp / 32 : 8;
-constexpr int kWarpsRes = 4;
+constexpr int kBtRes = kSmem ? kBtProp : 256;
+constexpr int kIptRes = kSmem ? 1 : 4;
+constexpr int kTileRes = kBtRes * kIptRes;
 
 int variant_of(int noises_off) { return noises_off & 3; }
 bool drift_on(int noises_off) { return M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT); }
@@ -477,7 +474,7 @@ int enqueue_filter(plomgpu_plan* p) {
     if (p->mif) th_cur ^= 1;
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
-      k_weight_tiles<T, kTileRes, kWarpsWeight><<<dim3(p->weight_blocks, R), kWarpsWeight * 32, 0, s>>>(
+      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->weight_blocks, R), kBtRes, 0, s>>>(
           (const T*)p->lw, J, p->ntiles, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n, p->llike,
           p->ess, p->n_obs);
       ++kernels;
@@ -488,9 +485,8 @@ int enqueue_filter(plomgpu_plan* p) {
         ++kernels;
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
-      k_resample_tiles<T, kTileRes, kWarpsRes><<<dim3((p->ntiles + kWarpsRes - 1) / kWarpsRes, R), kWarpsRes * 32, 0,
-                                                 s>>>(
-          (const T*)p->lw, J, p->ntiles, p->fail_b, p->part, p->P, p->st, p->sys + n, p->n_obs, p->anc[nxt],
+      k_resample_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
+          (const T*)p->lw, J, p->fail_b, p->part, p->P, p->st, p->sys + n, p->n_obs, p->anc[nxt],
           p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr, p->C, p->heavy);
       k_resample_heavy<256><<<dim3(p->heavy_blocks, R), 256, 0, s>>>(
           p->C, J, p->ntiles, kTileRes, p->st, p->sys + n, p->n_obs, p->heavy, p->anc[nxt],
@@ -622,7 +618,7 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(cudaMalloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
   CK(cudaMalloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
   p->heavy_blocks = std::min(p->ntiles, 2 * 148);
-  p->weight_blocks = std::min((p->ntiles + kWarpsWeight - 1) / kWarpsWeight, 4 * 148);
+  p->weight_blocks = std::min(p->ntiles, 4 * 148);
   CK(cudaMalloc((void**)&p->sys, (size_t)p->R * p->n_obs * sizeof(SysTable)));
   CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
   CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
@@ -1348,7 +1344,7 @@ extern "C" void plomgpu_mif_destroy(plomgpu_mif* p) { plan_free(p); }
 namespace {
 
 constexpr int kNoAllocMaxJ = 1 << 18;  // largest particle count the fixed scratch serves
-constexpr int kNoAllocTile = 1024;
+constexpr int kNoAllocBt = 256, kNoAllocIpt = 4, kNoAllocTile = kNoAllocBt * kNoAllocIpt;
 constexpr int kNoAllocTiles = (kNoAllocMaxJ + kNoAllocTile - 1) / kNoAllocTile;
 
 struct NoAllocScratch {
@@ -1383,10 +1379,11 @@ int noalloc_run(const T* lw, int J, double like_min, double u, uint32_t* anc, do
   // contents are still there
   k_reset_acc<<<1, 1, 0, s>>>(&sc->acc);
   k_sys_tables<<<1, 32, 0, s>>>(J, 1, 1, nullptr, 0u, nullptr, u, &sc->st.tab, &sc->acc);
-  k_weight_tiles<T, kNoAllocTile, 8><<<(ntiles + 7) / 8, 256, 0, s>>>(lw, J, ntiles, fail_b, log(like_min), sc->part,
-                                                                     sc->P, &sc->st, &sc->acc, 0, out, out + 1, 0);
-  k_resample_tiles<T, kNoAllocTile, 4><<<(ntiles + 3) / 4, 128, 0, s>>>(
-      lw, J, ntiles, fail_b, sc->part, sc->P, &sc->st, &sc->st.tab, 0, anc, nullptr, sc->C, sc->heavy);
+  k_weight_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(lw, J, ntiles, fail_b, log(like_min),
+                                                                           sc->part, sc->P, &sc->st, &sc->acc, 0,
+                                                                           out, out + 1, 0);
+  k_resample_tiles<T, kNoAllocBt, kNoAllocIpt><<<ntiles, kNoAllocBt, 0, s>>>(
+      lw, J, fail_b, sc->part, sc->P, &sc->st, &sc->st.tab, 0, anc, nullptr, sc->C, sc->heavy);
   k_resample_heavy<256><<<ntiles, 256, 0, s>>>(sc->C, J, ntiles, kNoAllocTile, &sc->st, &sc->st.tab, 0, sc->heavy,
                                                anc, nullptr);
   k_noalloc_out<<<1, 1, 0, s>>>(&sc->st, &sc->acc, out);

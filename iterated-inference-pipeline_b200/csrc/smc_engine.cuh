@@ -813,19 +813,26 @@ __device__ inline int points_at_or_below(const plomrt::SysSeg* seg, int ns, int 
   return c;
 }
 
-// Shared scratch of the weighting / resampling of WARPS tiles of TILE
-// particles, one per warp; placed by the caller (static in the stand-alone
-// kernels, inside the dynamic region of the serving loop).  A tile's values
-// sit at i + i / 32 (no two lanes of a run-per-lane access on one bank).
-constexpr __host__ __device__ int tile_pad(int i) { return i + (i >> 5); }
+// first i in [0, n) with !(x > c[i]), or n - 1 if every c[i] < x
+__device__ __forceinline__ int tile_lower_bound(const double* c, int n, double x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (x > c[mid]) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
 
-template <int TILE, int WARPS>
+// Shared scratch of the weighting / resampling of one tile (BT threads,
+// IPT particles each); placed by the caller (static in the stand-alone
+// kernels, inside the dynamic region of the serving loop).
+template <int BT, int IPT>
 struct TileScratch {
-  double sC[WARPS][TILE + TILE / 32];
-  double swarp[WARPS];
-  LseAcc lse[WARPS];
+  double sC[BT * IPT];
+  double swarp[BT / 32];
+  LseAcc lse[BT / 32];
   plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
-  int ns, fail;
+  int ns, fail, jlo, jhi;
 };
 
 // (max, sum exp(l - max), sum exp(2 (l - max)), failures) of the threads'
@@ -864,44 +871,6 @@ __device__ __forceinline__ LseAcc block_lse_all(LseAcc a, LseAcc* sh) {
   }
   __syncthreads();
   return r;
-}
-
-// (max, sum exp(l - max), sum exp(2 (l - max)), failures) of one tile of n
-// <= 32 * PL log-weights src[0, n) by one warp (every lane gets it): lane
-// takes src[lane + 32 k], the warp's maximum first, then one exponential
-// per weight relative to it, sums over the lanes in a fixed tree.
-template <class T, int PL>
-__device__ __forceinline__ LseAcc warp_tile_partial(const T* src, int n, double fail_b) {
-  const int lane = threadIdx.x & 31;
-  T v[PL];
-  bool ok[PL];
-  int nf = 0;
-  double m = -INFINITY;
-#pragma unroll
-  for (int k = 0; k < PL; ++k) {
-    const int i = lane + 32 * k;
-    v[k] = (i < n) ? src[i] : T(0);
-    ok[k] = (i < n) && !weight_fails_at(v[k], fail_b);
-    if (i < n && !ok[k]) ++nf;
-    if (ok[k]) m = fmax(m, (double)v[k]);
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
-  double s1 = 0.0, s2 = 0.0;
-#pragma unroll
-  for (int k = 0; k < PL; ++k) {
-    if (!ok[k]) continue;
-    const double e = ((double)v[k] == m) ? 1.0 : exp((double)v[k] - m);
-    s1 += e;
-    s2 += e * e;
-  }
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    s1 += __shfl_xor_sync(0xffffffffu, s1, off);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, off);
-    nf += __shfl_xor_sync(0xffffffffu, nf, off);
-  }
-  return LseAcc{m, s1, s2, nf};
 }
 
 // The systematic points of interval n (smc.c:97-101): U = inc * u and the
@@ -943,20 +912,42 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   const int chunk = (ntiles + BT - 1) / BT;
   const int b0 = threadIdx.x * chunk, b1 = min(ntiles, b0 + chunk);
   // the partials of the other blocks are read from L2 (written before their
-  // ticket, after a fence)
+  // ticket, after a fence), FC at a time with their loads issued together:
+  // each pass costs one round trip to L2 per FC tiles of the chunk
+  constexpr int FC = 8;
   // the chunk's maximum, then its sums rescaled to it (one exponential per tile)
   LseAcc a = {-INFINITY, 0.0, 0.0, 0};
-  for (int b = b0; b < b1; ++b)
-    if (__ldcg(&part[b].s1) > 0.0) a.m = fmax(a.m, __ldcg(&part[b].m));
-  for (int b = b0; b < b1; ++b) {
-    const LseAcc* p = part + b;
-    const double s1b = __ldcg(&p->s1);
-    a.nfail += __ldcg(&p->nfail);
-    if (s1b > 0.0) {
-      const double mb = __ldcg(&p->m);
-      const double f = (mb == a.m) ? 1.0 : exp(mb - a.m);
-      a.s1 += s1b * f;
-      a.s2 += __ldcg(&p->s2) * f * f;
+  for (int bb = b0; bb < b1; bb += FC) {
+    double s1v[FC], mv[FC];
+#pragma unroll
+    for (int k = 0; k < FC; ++k) {
+      const bool in = bb + k < b1;
+      s1v[k] = in ? __ldcg(&part[bb + k].s1) : 0.0;
+      mv[k] = in ? __ldcg(&part[bb + k].m) : -INFINITY;
+    }
+#pragma unroll
+    for (int k = 0; k < FC; ++k)
+      if (s1v[k] > 0.0) a.m = fmax(a.m, mv[k]);
+  }
+  for (int bb = b0; bb < b1; bb += FC) {
+    double s1v[FC], mv[FC], s2v[FC];
+    int nfv[FC];
+#pragma unroll
+    for (int k = 0; k < FC; ++k) {
+      const bool in = bb + k < b1;
+      s1v[k] = in ? __ldcg(&part[bb + k].s1) : 0.0;
+      mv[k] = in ? __ldcg(&part[bb + k].m) : -INFINITY;
+      s2v[k] = in ? __ldcg(&part[bb + k].s2) : 0.0;
+      nfv[k] = in ? __ldcg(&part[bb + k].nfail) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < FC; ++k) {
+      a.nfail += nfv[k];
+      if (s1v[k] > 0.0) {
+        const double f = (mv[k] == a.m) ? 1.0 : exp(mv[k] - a.m);
+        a.s1 += s1v[k] * f;
+        a.s2 += s2v[k] * f * f;
+      }
     }
   }
   a = block_lse_all<BT>(a, sh);
@@ -965,9 +956,17 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   // scan of them, then each chunk written in order
   double tot = 0.0;
   if (!all_fail) {
-    for (int b = b0; b < b1; ++b) {
-      const double s1b = __ldcg(&part[b].s1);
-      if (s1b > 0.0) tot += s1b * (exp(__ldcg(&part[b].m) - a.m) / a.s1);
+    for (int bb = b0; bb < b1; bb += FC) {
+      double s1v[FC], mv[FC];
+#pragma unroll
+      for (int k = 0; k < FC; ++k) {
+        const bool in = bb + k < b1;
+        s1v[k] = in ? __ldcg(&part[bb + k].s1) : 0.0;
+        mv[k] = in ? __ldcg(&part[bb + k].m) : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < FC; ++k)
+        if (s1v[k] > 0.0) tot += s1v[k] * (exp(mv[k] - a.m) / a.s1);
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -990,11 +989,21 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   }
   __syncthreads();
   double run = ((warp > 0) ? shd[warp - 1] : 0.0) + (v - tot);
-  for (int b = b0; b < b1; ++b) {
-    P[b] = run;
+  for (int bb = b0; bb < b1; bb += FC) {
+    double s1v[FC], mv[FC];
     if (!all_fail) {
-      const double s1b = __ldcg(&part[b].s1);
-      if (s1b > 0.0) run += s1b * (exp(__ldcg(&part[b].m) - a.m) / a.s1);
+#pragma unroll
+      for (int k = 0; k < FC; ++k) {
+        const bool in = bb + k < b1;
+        s1v[k] = in ? __ldcg(&part[bb + k].s1) : 0.0;
+        mv[k] = in ? __ldcg(&part[bb + k].m) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < FC; ++k) {
+      if (bb + k >= b1) break;
+      P[bb + k] = run;
+      if (!all_fail && s1v[k] > 0.0) run += s1v[k] * (exp(mv[k] - a.m) / a.s1);
     }
   }
   if (b1 == ntiles && b0 < b1) P[ntiles] = run;
@@ -1020,17 +1029,16 @@ __device__ void fold_tiles(const LseAcc* part, int ntiles, int J, double log_lik
   }
 }
 
-// ntiles tiles of TILE particles per filter, a warp per tile, over
-// gridDim.x blocks of WARPS warps (tiles b, b + gridDim.x * WARPS, ...): the
-// tile partials, then one ticket per block; the last block folds them.
-template <class T, int TILE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_weight_tiles(const T* __restrict__ lw, int J, int ntiles,
-                                                             double fail_b, double log_like_min, LseAcc* part,
-                                                             double* P, StepState* st, FilterAcc* acc, int n,
-                                                             double* llike_out, double* ess_out, int out_stride) {
-  static_assert(TILE % 32 == 0, "whole warps per tile");
-  __shared__ LseAcc sh[WARPS];
-  __shared__ double shd[WARPS];
+// ntiles tiles of BT * IPT particles per filter over gridDim.x blocks (a
+// block takes tiles b, b + gridDim.x, ...): the tile partials, then one
+// ticket per block; the last block folds them.
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, int J, int ntiles, double fail_b,
+                                                     double log_like_min, LseAcc* part, double* P, StepState* st,
+                                                     FilterAcc* acc, int n, double* llike_out, double* ess_out,
+                                                     int out_stride) {
+  __shared__ LseAcc sh[BT / 32];
+  __shared__ double shd[BT / 32];
   __shared__ bool last;
   {
     const int r = blockIdx.y;
@@ -1042,12 +1050,30 @@ __global__ void __launch_bounds__(WARPS * 32) k_weight_tiles(const T* __restrict
     if (llike_out) llike_out += (size_t)r * out_stride;
     if (ess_out) ess_out += (size_t)r * out_stride;
   }
-  const int warp = threadIdx.x >> 5;
-  for (int b = blockIdx.x * WARPS + warp; b < ntiles; b += gridDim.x * WARPS) {
-    const LseAcc a = warp_tile_partial<T, TILE / 32>(lw + (size_t)b * TILE, min(TILE, J - b * TILE), fail_b);
-    if ((threadIdx.x & 31) == 0) part[b] = a;
+  for (int b = blockIdx.x; b < ntiles; b += gridDim.x) {
+    const int base = b * BT * IPT;
+    // the thread's maximum, then its sums relative to it
+    T lv[IPT];
+    bool ok[IPT];
+    LseAcc a = {-INFINITY, 0.0, 0.0, 0};
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      const int i = base + k * BT + threadIdx.x;
+      lv[k] = (i < J) ? lw[i] : T(0);
+      ok[k] = (i < J) && !weight_fails_at(lv[k], fail_b);
+      if (i < J && !ok[k]) a.nfail += 1;
+      if (ok[k]) a.m = fmax(a.m, (double)lv[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < IPT; ++k) {
+      if (!ok[k]) continue;
+      const double e = ((double)lv[k] == a.m) ? 1.0 : exp((double)lv[k] - a.m);
+      a.s1 += e;
+      a.s2 += e * e;
+    }
+    a = block_lse_all<BT>(a, sh);
+    if (threadIdx.x == 0) part[b] = a;
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned t = atomicAdd(&acc->ticket, 1u);
@@ -1057,7 +1083,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_weight_tiles(const T* __restrict
   if (!last) return;
   __threadfence();
   if (threadIdx.x == 0) acc->ticket = 0u;
-  fold_tiles<WARPS * 32>(part, ntiles, J, log_like_min, P, st, acc, n, llike_out, ess_out, sh, shd);
+  fold_tiles<BT>(part, ntiles, J, log_like_min, P, st, acc, n, llike_out, ess_out, sh, shd);
 }
 
 // The propagate launch: PPT particles per thread, BT apart (one for
@@ -1080,46 +1106,48 @@ __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const Step
   }
 }
 
-// Cumulative normalised weights of tile b by one warp into c (padded,
-// tile_pad): c[i] = P[b] + (prefix of exp(l - max_b) in particle order) *
-// exp(max_b - max) / sum, i < n_in.  Lane takes the run of TILE / 32
-// consecutive particles from lane * TILE / 32: the exponentials (coalesced
-// loads), the lane's run sums, an exclusive scan of them over the lanes,
-// then each run's prefix.
-template <class T, int TILE>
-__device__ void warp_cum_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
-                              const double* __restrict__ P, const StepState* st, int b, double* c) {
-  constexpr int CH = TILE / 32;
-  const int lane = threadIdx.x & 31;
+// Cumulative normalised weights of tile b: sC[i] = P[b] + (prefix of
+// exp(l - max_b) in particle order) * exp(max_b - max) / sum, i < n_in
+// (all threads of the block call it).
+template <class T, int BT, int IPT>
+__device__ void cum_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
+                         const double* __restrict__ P, const StepState* st, int b, TileScratch<BT, IPT>& sc) {
+  constexpr int TILE = BT * IPT;
   const int base = b * TILE;
   const int n_in = min(TILE, J - base);
   const double mb = __ldcg(&part[b].m);
   const double s1b = __ldcg(&part[b].s1);
   const double f = (s1b > 0.0) ? exp(mb - st->m) / st->s1 : 0.0;
   const double Pb = __ldcg(P + b);
-#pragma unroll 4
-  for (int k = 0; k < CH; ++k) {
-    const int i = lane + 32 * k;
-    c[tile_pad(i)] = (i < n_in) ? surviving_exp(lw[base + i], fail_b, mb) : 0.0;
-  }
-  __syncwarp();
-  double tot = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < CH; ++k) tot += c[tile_pad(lane * CH + k)];
-  double ex = tot;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double carry = 0.0;
 #pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    const double o = __shfl_up_sync(0xffffffffu, ex, off);
-    if (lane >= off) ex += o;
+  for (int k = 0; k < IPT; ++k) {
+    const int ii = k * BT + threadIdx.x;
+    const double p = (ii < n_in) ? surviving_exp(lw[base + ii], fail_b, mb) : 0.0;
+    double v = p;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double o = __shfl_up_sync(0xffffffffu, v, off);
+      if (lane >= off) v += o;
+    }
+    if (lane == 31) sc.swarp[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      double w = (lane < BT / 32) ? sc.swarp[lane] : 0.0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double o = __shfl_up_sync(0xffffffffu, w, off);
+        if (lane >= off) w += o;
+      }
+      if (lane < BT / 32) sc.swarp[lane] = w;
+    }
+    __syncthreads();
+    const double incl = carry + ((warp > 0) ? sc.swarp[warp - 1] : 0.0) + v;
+    sc.sC[ii] = Pb + incl * f;
+    carry += sc.swarp[BT / 32 - 1];
+    __syncthreads();
   }
-  double run = ex - tot;  // the lanes before this one
-#pragma unroll 4
-  for (int k = 0; k < CH; ++k) {
-    const int i = tile_pad(lane * CH + k);
-    run += c[i];
-    c[i] = Pb + run * f;
-  }
-  __syncwarp();
 }
 
 // run of the table that holds point j: the last with j0 <= j
@@ -1133,24 +1161,16 @@ __device__ __forceinline__ int sys_run(const plomrt::SysSeg* seg, int ns, int j)
 }
 
 // Ancestors of the consecutive points [ja, jb) over the cumulative weights
-// c[0, n) (padded when PAD) of the tile starting at particle `first`: the
-// first i with c[i] >= point (n - 1 if none), by one search for ja and a
-// walk for the rest (points and weights both ascend).  Point values are
-// systematic_point's.
-template <bool PAD>
+// c[0, n) of the tile starting at particle `first`: the first i with
+// c[i] >= point (n - 1 if none), by one search for ja and a walk for the rest
+// (points and weights both ascend).  Point values are systematic_point's.
 __device__ __forceinline__ void place_points(const plomrt::SysSeg* seg, int ns, int ja, int jb, const double* c,
                                              int n, int first, uint32_t* __restrict__ anc,
                                              uint32_t* __restrict__ anc_hist) {
   if (ja >= jb) return;
-  auto at = [c](int i) { return PAD ? c[tile_pad(i)] : c[i]; };
   int sg = sys_run(seg, ns, ja);
   double ran = seg[sg].x0 + (double)(ja - seg[sg].j0) * seg[sg].step;
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (ran > at(mid)) lo = mid + 1; else hi = mid;
-  }
-  int i = lo;
+  int i = tile_lower_bound(c, n, ran);
   for (int j = ja;;) {
     const uint32_t r = (uint32_t)(first + i);
     anc[j] = r;
@@ -1158,94 +1178,81 @@ __device__ __forceinline__ void place_points(const plomrt::SysSeg* seg, int ns, 
     if (++j >= jb) break;
     while (sg + 1 < ns && seg[sg + 1].j0 <= j) ++sg;
     ran = seg[sg].x0 + (double)(j - seg[sg].j0) * seg[sg].step;
-    while (i < n - 1 && ran > at(i)) ++i;
+    while (i < n - 1 && ran > c[i]) ++i;
   }
 }
 
-// Tile b of one filter by one warp: its cumulative weights (warp_cum_tile,
-// into the warp's c) and the ancestors of the systematic points that fall in
-// it, P[b] < point <= P[b + 1] (the first tile from point 0, the last to
-// point J - 1), each lane a run of consecutive points.  heavy == nullptr:
-// the warp places all of its points however many; else a tile with more
-// than kHeavyTiles * TILE points writes its cumulative weights to C and is
-// listed for k_resample_heavy.  seg / ns / fail: the interval's table in
-// shared memory and the all-fail flag (identity ancestors, smc.c:55-69).
-template <class T, int TILE>
-__device__ void warp_resample_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
-                                   const double* __restrict__ P, StepState* st, const plomrt::SysSeg* seg, int ns,
-                                   bool fail, double U, int b, int ntiles, uint32_t* __restrict__ anc,
-                                   uint32_t* __restrict__ anc_hist, double* __restrict__ C, HeavyTile* heavy,
-                                   double* c) {
-  const int lane = threadIdx.x & 31;
+// Tile b of one filter: its cumulative weights and the ancestors of the
+// systematic points that fall in it (all threads of the block call it),
+// each thread a run of consecutive points.  heavy == nullptr: the block
+// places all of its points however many; else a tile with more than
+// kHeavyTiles * TILE points writes its cumulative weights to C and is listed
+// for k_resample_heavy.  Identity ancestors when every particle failed
+// (smc.c:55-69).
+template <class T, int BT, int IPT>
+__device__ void resample_tile(const T* __restrict__ lw, int J, double fail_b, const LseAcc* __restrict__ part,
+                              const double* __restrict__ P, StepState* st, const SysTable* tab, int b, int ntiles,
+                              uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist, double* __restrict__ C,
+                              HeavyTile* heavy, TileScratch<BT, IPT>& sc) {
+  constexpr int TILE = BT * IPT;
+  static_assert(BT >= 64, "two warps find the tile's points");
   const int base = b * TILE;
   const int n_in = min(TILE, J - base);
-  if (fail || ns == 0) {
-    for (int i = lane; i < n_in; i += 32) {
-      anc[base + i] = (uint32_t)(base + i);
-      if (anc_hist) anc_hist[base + i] = (uint32_t)(base + i);
-    }
-    return;
-  }
-  int jb = 0;
-  if (lane == 0) jb = (b == 0) ? 0 : points_at_or_below(seg, ns, J, U, __ldcg(P + b));
-  if (lane == 1) jb = (b == ntiles - 1) ? J : points_at_or_below(seg, ns, J, U, __ldcg(P + b + 1));
-  warp_cum_tile<T, TILE>(lw, J, fail_b, part, P, st, b, c);
-  const int jlo = __shfl_sync(0xffffffffu, jb, 0);
-  const int jhi = max(jlo, __shfl_sync(0xffffffffu, jb, 1));
-  const int np = jhi - jlo;
-  if (heavy && np > kHeavyTiles * TILE) {
-    for (int i = lane; i < n_in; i += 32) C[base + i] = c[tile_pad(i)];
-    if (lane == 0) {
-      const unsigned long long k = atomicAdd(&st->heavy, (1ull << 32) | (unsigned long long)np);
-      heavy[k >> 32] = HeavyTile{b, jlo, jhi, n_in, (int)(k & 0xffffffffull)};
-    }
-  } else {
-    const int per = (np + 31) / 32;
-    const int ja = jlo + lane * per;
-    place_points<true>(seg, ns, ja, min(jhi, ja + per), c, n_in, base, anc, anc_hist);
-  }
-  __syncwarp();
-}
-
-// The interval's table and all-fail flag into the block's scratch (all
-// threads call it).
-template <int TILE, int WARPS>
-__device__ __forceinline__ void load_sys_table(const SysTable* tab, const StepState* st,
-                                               TileScratch<TILE, WARPS>& sc) {
   if (threadIdx.x == 0) {
     sc.ns = tab->ns;
     sc.fail = st->all_fail;
   }
   __syncthreads();
-  if (!sc.fail)
-    for (int i = threadIdx.x; i < sc.ns; i += WARPS * 32) sc.seg[i] = tab->seg[i];
+  if (sc.fail || sc.ns == 0) {
+    for (int i = threadIdx.x; i < n_in; i += BT) {
+      anc[base + i] = (uint32_t)(base + i);
+      if (anc_hist) anc_hist[base + i] = (uint32_t)(base + i);
+    }
+    __syncthreads();
+    return;
+  }
+  const int ns = sc.ns;
+  for (int i = threadIdx.x; i < ns; i += BT) sc.seg[i] = tab->seg[i];
   __syncthreads();
+  // the tile's points, P[b] < point <= P[b + 1] (the first tile from point 0,
+  // the last to point J - 1), while the other warps start the weights
+  const double U = tab->U;
+  if (threadIdx.x == 0) sc.jlo = (b == 0) ? 0 : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b));
+  if (threadIdx.x == 32) sc.jhi = (b == ntiles - 1) ? J : points_at_or_below(sc.seg, ns, J, U, __ldcg(P + b + 1));
+  cum_tile<T, BT, IPT>(lw, J, fail_b, part, P, st, b, sc);
+  const int jlo = sc.jlo, jhi = max(sc.jlo, sc.jhi);
+  const int np = jhi - jlo;
+  if (heavy && np > kHeavyTiles * TILE) {
+    for (int i = threadIdx.x; i < n_in; i += BT) C[base + i] = sc.sC[i];
+    if (threadIdx.x == 0) {
+      const unsigned long long k = atomicAdd(&st->heavy, (1ull << 32) | (unsigned long long)np);
+      heavy[k >> 32] = HeavyTile{b, jlo, jhi, n_in, (int)(k & 0xffffffffull)};
+    }
+  } else {
+    const int per = (np + BT - 1) / BT;
+    const int ja = jlo + threadIdx.x * per;
+    place_points(sc.seg, ns, ja, min(jhi, ja + per), sc.sC, n_in, base, anc, anc_hist);
+  }
+  __syncthreads();  // the scratch of one tile before the next
 }
 
-template <class T, int TILE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_resample_tiles(const T* __restrict__ lw, int J, int ntiles,
-                                                               double fail_b, const LseAcc* __restrict__ part,
-                                                               const double* __restrict__ P, StepState* st,
-                                                               const SysTable* tab, int tab_stride,
-                                                               uint32_t* __restrict__ anc,
-                                                               uint32_t* __restrict__ anc_hist,
-                                                               double* __restrict__ C, HeavyTile* heavy) {
-  __shared__ TileScratch<TILE, WARPS> sc;
+template <class T, int BT, int IPT>
+__global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw, int J, double fail_b,
+                                                       const LseAcc* __restrict__ part, const double* __restrict__ P,
+                                                       StepState* st, const SysTable* tab, int tab_stride,
+                                                       uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist,
+                                                       double* __restrict__ C, HeavyTile* heavy) {
+  __shared__ TileScratch<BT, IPT> sc;
+  const int ntiles = gridDim.x;
   const int r = blockIdx.y;
-  st += r;
-  tab += (size_t)r * tab_stride;
-  load_sys_table<TILE, WARPS>(tab, st, sc);
-  const int warp = threadIdx.x >> 5;
-  const int b = blockIdx.x * WARPS + warp;
-  if (b < ntiles)
-    warp_resample_tile<T, TILE>(lw + (size_t)r * J, J, fail_b, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
-                                st, sc.seg, sc.ns, sc.fail != 0, tab->U, b, ntiles, anc + (size_t)r * J,
-                                anc_hist ? anc_hist + (size_t)r * J : nullptr, C + (size_t)r * J,
-                                heavy + (size_t)r * ntiles, sc.sC[warp]);
+  resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, fail_b, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
+                            st + r, tab + (size_t)r * tab_stride, blockIdx.x, ntiles, anc + (size_t)r * J,
+                            anc_hist ? anc_hist + (size_t)r * J : nullptr, C + (size_t)r * J,
+                            heavy + (size_t)r * ntiles, sc);
 }
 
-// The points of the tiles listed by warp_resample_tile, spread evenly over
-// all threads (each a run of consecutive listed points): the first i of the
+// The points of the tiles listed by resample_tile, spread evenly over all
+// threads (each a run of consecutive listed points): the first i of the
 // tile with C_i >= point, from C in global memory.
 template <int BT>
 __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict__ C, int J, int ntiles, int tile,
@@ -1287,7 +1294,7 @@ __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict_
     const HeavyTile h = heavy[e];
     const int ja = h.jlo + (int)(q - h.off);
     const int jb = (int)min((long long)h.jhi, (long long)ja + (qe - q));
-    place_points<false>(seg, ns, ja, jb, C + (size_t)h.b * tile, h.n_in, h.b * tile, anc, anc_hist);
+    place_points(seg, ns, ja, jb, C + (size_t)h.b * tile, h.n_in, h.b * tile, anc, anc_hist);
     q += jb - ja;
   }
 }

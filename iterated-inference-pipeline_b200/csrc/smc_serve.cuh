@@ -223,8 +223,7 @@ __device__ inline TileReqWs<T> tile_req_ws(unsigned char* base, int J) {
 template <class T, int BT>
 constexpr size_t serve_tiles_smem() {
   constexpr size_t prop = propagate_smem_bytes<T, kSmem, BT>();
-  constexpr size_t scratch =
-      ((size_t)(kSmemCoup + kSmemPar) * sizeof(T) + 15) / 16 * 16 + sizeof(TileScratch<BT, BT / 32>);
+  constexpr size_t scratch = ((size_t)(kSmemCoup + kSmemPar) * sizeof(T) + 15) / 16 * 16 + sizeof(TileScratch<BT, 1>);
   return prop > scratch ? prop : scratch;
 }
 
@@ -234,9 +233,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
                                                     unsigned char* pool, long long* live, long long idle_limit,
                                                     int task_budget) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  static_assert(kServeShortClaim <= BT / 32, "a warp per claimed short tile");
   // the tile scratch sits after the coupling / parameter tables
-  TileScratch<BT, BT / 32>& sc = *reinterpret_cast<TileScratch<BT, BT / 32>*>(
+  TileScratch<BT, 1>& sc = *reinterpret_cast<TileScratch<BT, 1>*>(
       smem_raw + ((size_t)(kSmemCoup + kSmemPar) * sizeof(T) + 15) / 16 * 16);
   __shared__ long long s_off;   // workspace of the claimed request, -1: none
   __shared__ int s_tile;        // first claimed tile, -1: admission of a new request
@@ -405,8 +403,8 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
     bool any = false;
     for (int ts = 0; ts < M::N_TS; ++ts) any |= !isnan(__ldg(y + ts));
     const bool weigh = a.filter_on && any;
+    for (int tile = s_tile; tile < s_tile + ntask; ++tile) {
     if (kind == 0) {
-      const int tile = s_tile;  // one propagate tile per claim
       Tables<T> tb{};
       tb.par_cac = w.par_cac;
       tb.cov_cac = a.cov_cac;
@@ -445,24 +443,20 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       if (weigh && tile == 0 && threadIdx.x == 32)
         sys_table(&q->st.tab, &q->acc, J, n, -1.0, plomrt::make_key(q->seed, 0u));
       if (weigh) {
-        // the tile's partial as the filters' k_weight_tiles forms it: one warp over the tile's log-weights
-        T* sl = reinterpret_cast<T*>(sc.sC[0]);
-        sl[threadIdx.x] = (g < (size_t)J) ? (T)l : T(0);
-        __syncthreads();
-        if (threadIdx.x < 32) {
-          const LseAcc pa = warp_tile_partial<T, BT / 32>(sl, min(BT, J - tile * BT), a.fail_b);
-          if (threadIdx.x == 0) w.part[tile] = pa;
+        LseAcc acc = {-INFINITY, 0.0, 0.0, 0};
+        if (g < (size_t)J) {
+          if (weight_fails_at(l, a.fail_b)) acc.nfail = 1;
+          else acc = LseAcc{l, 1.0, 1.0, 0};
         }
+        acc = block_lse_all<BT>(acc, sc.lse);
+        if (threadIdx.x == 0) w.part[tile] = acc;
       }
     } else {
-      // resample: a warp per claimed tile
-      load_sys_table<BT, BT / 32>(&q->st.tab, &q->st, sc);
-      const int wi = threadIdx.x >> 5;
-      if (wi < ntask)
-        warp_resample_tile<T, BT>(w.lw, J, a.fail_b, w.part, w.P, &q->st, sc.seg, sc.ns, sc.fail != 0, q->st.tab.U,
-                                  s_tile + wi, ntiles, w.anc, nullptr, nullptr, nullptr, sc.sC[wi]);
+      resample_tile<T, BT, 1>(w.lw, J, a.fail_b, w.part, w.P, &q->st, &q->st.tab, tile, ntiles, w.anc, nullptr,
+                              nullptr, nullptr, sc);
     }
-    __syncthreads();  // the shared scratch before the next claim
+    __syncthreads();  // the shared scratch of one tile before the next
+    }
     // the last tile of the phase does its serial part and publishes the next phase
     __threadfence();
     __syncthreads();
