@@ -68,6 +68,10 @@ def parse():
                     help='serve: offered load, as a fraction of the measured saturation rate, of the latency runs')
     ap.add_argument('--plan-pool', type=int, default=0, help='serve: run the shared-memory model on a pool of this '
                     'many concurrent plans instead of the tiled device loop (0: device loop)')
+    ap.add_argument('--particles', type=int, default=0,
+                    help='a smaller case of the workload for profiling captures: J (0: the workload\'s)')
+    ap.add_argument('--intervals', type=int, default=0,
+                    help='a smaller case of the workload for profiling captures: T (0: the workload\'s)')
     return ap.parse_args()
 
 
@@ -106,7 +110,7 @@ class Clocks(object):
         try:
             self.proc = subprocess.Popen(
                 ['nvidia-smi', '-i', str(self.dev), '--query-gpu=' + self.FIELDS, '--format=csv,noheader,nounits',
-                 '-lms', '200'], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 '-lms', '100'], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (OSError, ValueError):
@@ -557,7 +561,8 @@ def main():
     from plomgpu import build
     lib = WORKLOADS[args.workload][0]
     eng = Engine(lib)
-    prob = workload_problem(args.workload, precision=32, seed=1000 + rank)
+    prob = workload_problem(args.workload, precision=32, seed=1000 + rank, J=args.particles or None,
+                            nb_obs=args.intervals or -1)
     plan = Plan(eng, prob, timing=True)
     stream = torch.cuda.ExternalStream(plan.stream)
 

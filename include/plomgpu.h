@@ -174,7 +174,8 @@ int plomgpu_draws_per_substep(int noises_off);
 /* Runs one filter: replaces run_SMC (model_builder/C/core/smc.c:204-307) and
  * the per-particle loop of worker_routine_smc_inproc
  * (model_builder/C/core/worker_inproc.c:21-102).  Host buffers in and out;
- * allocates its device workspace for the call. */
+ * its device workspace comes from the library's memory pool for the call
+ * (see plomgpu_release_memory). */
 int plomgpu_smc_run(const plomgpu_smc_desc *desc, plomgpu_smc_result *result);
 
 /* Reusable plan: device buffers, uploaded inputs and a CUDA graph of the
@@ -219,6 +220,12 @@ void *plomgpu_plan_stream(plomgpu_plan *plan);
 /* Kernels launched by one plomgpu_plan_launch. */
 int plomgpu_plan_kernel_count(plomgpu_plan *plan);
 void plomgpu_plan_destroy(plomgpu_plan *plan);
+
+/* Plans and one-shot filters take their device buffers from a memory pool of
+ * the library (one per device, stream-ordered) that keeps the memory of
+ * destroyed plans for the next ones.  This returns the pool's unused memory
+ * on the current device to the driver. */
+int plomgpu_release_memory(void);
 
 /* Test hook (host only, no GPU needed): the largest double whose exponential
  * is <= thresh, which the filters compare log-weights with for the failure

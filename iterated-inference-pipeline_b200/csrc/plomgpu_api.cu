@@ -254,6 +254,76 @@ int upload(const U* h, size_t n, U** d, cudaStream_t s) {
   return PLOMGPU_OK;
 }
 
+// Plan buffers come from a stream-ordered memory pool of the library, one
+// per device, that keeps freed memory (release threshold: all of it): after
+// the first filter of a size a one-shot filter costs no cudaMalloc and no
+// cudaFree (they took 12-19 ms of a 0.28 s SEIR 20x2 filter).
+// plomgpu_release_memory trims it.  The pool belongs to the context that
+// created it; a handle that no longer answers (its context was reset) is
+// replaced.
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_plan_pool[kMaxDevices] = {};
+
+cudaError_t plan_mem_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (g_plan_pool[dev]) {
+    uint64_t v = 0;
+    if (cudaMemPoolGetAttribute(g_plan_pool[dev], cudaMemPoolAttrReleaseThreshold, &v) == cudaSuccess) {
+      *out = g_plan_pool[dev];
+      return cudaSuccess;
+    }
+    (void)cudaGetLastError();
+    g_plan_pool[dev] = nullptr;
+  }
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t mp = nullptr;
+  if ((e = cudaMemPoolCreate(&mp, &props)) != cudaSuccess) return e;
+  uint64_t keep = ~(uint64_t)0;
+  if ((e = cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+  g_plan_pool[dev] = mp;
+  *out = mp;
+  return cudaSuccess;
+}
+
+// the stream a plan being built allocates on (stream-ordered: its buffers
+// are valid on that stream at once, elsewhere after a synchronisation)
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
+template <class P>
+cudaError_t palloc(P** ptr, size_t bytes) {
+  cudaMemPool_t mp = nullptr;
+  cudaError_t e = plan_mem_pool(&mp);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync((void**)ptr, bytes > 0 ? bytes : 1, mp, g_alloc_stream);
+}
+
+template <class T>
+int pupload_as(const double* h, size_t n, void** d, cudaStream_t s) {
+  if (n == 0) return PLOMGPU_OK;
+  std::vector<T> tmp(n);
+  for (size_t i = 0; i < n; ++i) tmp[i] = (T)h[i];
+  CK(palloc(d, n * sizeof(T)));
+  CK(cudaMemcpyAsync(*d, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return PLOMGPU_OK;
+}
+
+template <class U>
+int pupload(const U* h, size_t n, U** d, cudaStream_t s) {
+  if (n == 0 || h == nullptr) return PLOMGPU_OK;
+  CK(palloc(d, n * sizeof(U)));
+  CK(cudaMemcpyAsync(*d, h, n * sizeof(U), cudaMemcpyHostToDevice, s));
+  return PLOMGPU_OK;
+}
+
 template <class T>
 using PropKernel = void (*)(const Tables<T>, const StepArgs);
 
@@ -603,25 +673,25 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   p->tsize = sizeof(T);
   int rc;
   const size_t RJ = (size_t)p->R * J;
-  CK(cudaMalloc(&p->X[0], (size_t)M::S * RJ * sizeof(T)));
-  CK(cudaMalloc(&p->X[1], (size_t)M::S * RJ * sizeof(T)));
-  CK(cudaMalloc(&p->lw, RJ * sizeof(T)));
-  CK(cudaMalloc((void**)&p->C, RJ * sizeof(double)));
-  CK(cudaMalloc((void**)&p->anc[0], RJ * sizeof(uint32_t)));
-  CK(cudaMalloc((void**)&p->anc[1], RJ * sizeof(uint32_t)));
+  CK(palloc(&p->X[0], (size_t)M::S * RJ * sizeof(T)));
+  CK(palloc(&p->X[1], (size_t)M::S * RJ * sizeof(T)));
+  CK(palloc(&p->lw, RJ * sizeof(T)));
+  CK(palloc((void**)&p->C, RJ * sizeof(double)));
+  CK(palloc((void**)&p->anc[0], RJ * sizeof(uint32_t)));
+  CK(palloc((void**)&p->anc[1], RJ * sizeof(uint32_t)));
   if (p->mif) {
-    CK(cudaMalloc(&p->theta[0], (size_t)p->Q * RJ * sizeof(T)));
-    CK(cudaMalloc(&p->theta[1], (size_t)p->Q * RJ * sizeof(T)));
+    CK(palloc(&p->theta[0], (size_t)p->Q * RJ * sizeof(T)));
+    CK(palloc(&p->theta[1], (size_t)p->Q * RJ * sizeof(T)));
   }
   p->ntiles = (J + kTileRes - 1) / kTileRes;
-  CK(cudaMalloc((void**)&p->part, (size_t)p->R * p->ntiles * sizeof(LseAcc)));
-  CK(cudaMalloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
-  CK(cudaMalloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
+  CK(palloc((void**)&p->part, (size_t)p->R * p->ntiles * sizeof(LseAcc)));
+  CK(palloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
+  CK(palloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
   p->heavy_blocks = std::min(p->ntiles, 2 * 148);
   p->weight_blocks = std::min(p->ntiles, 4 * 148);
-  CK(cudaMalloc((void**)&p->sys, (size_t)p->R * p->n_obs * sizeof(SysTable)));
-  CK(cudaMalloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
-  CK(cudaMalloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
+  CK(palloc((void**)&p->sys, (size_t)p->R * p->n_obs * sizeof(SysTable)));
+  CK(palloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
+  CK(palloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
   CK(cudaMemsetAsync(p->acc, 0, (size_t)p->R * sizeof(FilterAcc), s));
   // a reused plan reads its accumulator through pinned memory; a one-shot
   // filter reads it once, and pinning a page costs more than the copy
@@ -630,61 +700,61 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
 
   const size_t n_par = (size_t)M::N_PAR_PROC * M::N_CAC;
   if (n_par > 0) {
-    CK(cudaMalloc(&p->par_cac, n_par * sizeof(T)));
-    if ((rc = upload<double>(d->par_cac, n_par, &p->par_cac_d, s))) return rc;
+    CK(palloc(&p->par_cac, n_par * sizeof(T)));
+    if ((rc = pupload<double>(d->par_cac, n_par, &p->par_cac_d, s))) return rc;
   }
-  if ((rc = upload_as<T>(d->cov_cac, (size_t)p->sub_total * M::N_COV_CAC * M::N_CAC, &p->cov_cac, s))) return rc;
+  if ((rc = pupload_as<T>(d->cov_cac, (size_t)p->sub_total * M::N_COV_CAC * M::N_CAC, &p->cov_cac, s))) return rc;
   if (M::COUPLED) {
-    if ((rc = upload_as<T>(d->coupling, (size_t)M::N_CAC * M::N_CAC, &p->coupling, s))) return rc;
+    if ((rc = pupload_as<T>(d->coupling, (size_t)M::N_CAC * M::N_CAC, &p->coupling, s))) return rc;
   }
   if (drift_on(d->noises_off)) {
-    if ((rc = upload_as<T>(d->drift_vol, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_vol, s))) return rc;
-    if ((rc = upload<int>(d->drift_group, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_group, s))) return rc;
-    if ((rc = upload<int>(d->drift_ngroups, (size_t)M::N_DRIFT, &p->drift_ngroups, s))) return rc;
-    if ((rc = upload<plomrt::BackTransform>((const plomrt::BackTransform*)d->drift_bt, (size_t)M::N_DRIFT * M::N_CAC,
+    if ((rc = pupload_as<T>(d->drift_vol, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_vol, s))) return rc;
+    if ((rc = pupload<int>(d->drift_group, (size_t)M::N_DRIFT * M::N_CAC, &p->drift_group, s))) return rc;
+    if ((rc = pupload<int>(d->drift_ngroups, (size_t)M::N_DRIFT, &p->drift_ngroups, s))) return rc;
+    if ((rc = pupload<plomrt::BackTransform>((const plomrt::BackTransform*)d->drift_bt, (size_t)M::N_DRIFT * M::N_CAC,
                                             &p->drift_bt, s)))
       return rc;
   }
-  if ((rc = upload<double>(d->par_ts, (size_t)M::N_PAR_OBS * M::N_TS, &p->par_ts, s))) return rc;
-  if ((rc = upload<double>(d->t_sub, (size_t)p->sub_total, &p->t_sub, s))) return rc;
-  if ((rc = upload<double>(d->cov_ts, (size_t)d->n_obs * M::N_COV_TS * M::N_TS, &p->cov_ts, s))) return rc;
+  if ((rc = pupload<double>(d->par_ts, (size_t)M::N_PAR_OBS * M::N_TS, &p->par_ts, s))) return rc;
+  if ((rc = pupload<double>(d->t_sub, (size_t)p->sub_total, &p->t_sub, s))) return rc;
+  if ((rc = pupload<double>(d->cov_ts, (size_t)d->n_obs * M::N_COV_TS * M::N_TS, &p->cov_ts, s))) return rc;
   {
     // data rows: at least one row so that every interval has a valid pointer
     std::vector<double> rows((size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS, NAN);
     if (d->n_obs > 0) memcpy(rows.data(), d->data, (size_t)d->n_obs * M::N_TS * sizeof(double));
-    if ((rc = upload<double>(rows.data(), rows.size(), &p->data, s))) return rc;
+    if ((rc = pupload<double>(rows.data(), rows.size(), &p->data, s))) return rc;
     CK(cudaStreamSynchronize(s));
   }
-  if ((rc = upload<double>(d->x0, (size_t)M::S, &p->x0, s))) return rc;
-  if (d->x0_particles && (rc = upload<double>(d->x0_particles, (size_t)M::OFF_INC * J, &p->x0_cloud, s))) return rc;
+  if ((rc = pupload<double>(d->x0, (size_t)M::S, &p->x0, s))) return rc;
+  if (d->x0_particles && (rc = pupload<double>(d->x0_particles, (size_t)M::OFF_INC * J, &p->x0_cloud, s))) return rc;
   if (p->ode && M::N_COV_CAC > 0) {
-    if ((rc = upload<int>(d->cov_spline_meta, (size_t)3 * M::N_COV_CAC * M::N_CAC, &p->sp_meta, s))) return rc;
-    if ((rc = upload<double>(d->cov_spline_x, (size_t)d->cov_spline_knots, &p->sp_x, s))) return rc;
-    if ((rc = upload<double>(d->cov_spline_y, (size_t)d->cov_spline_knots, &p->sp_y, s))) return rc;
-    if ((rc = upload<double>(d->cov_spline_m2, (size_t)d->cov_spline_knots, &p->sp_m2, s))) return rc;
+    if ((rc = pupload<int>(d->cov_spline_meta, (size_t)3 * M::N_COV_CAC * M::N_CAC, &p->sp_meta, s))) return rc;
+    if ((rc = pupload<double>(d->cov_spline_x, (size_t)d->cov_spline_knots, &p->sp_x, s))) return rc;
+    if ((rc = pupload<double>(d->cov_spline_y, (size_t)d->cov_spline_knots, &p->sp_y, s))) return rc;
+    if ((rc = pupload<double>(d->cov_spline_m2, (size_t)d->cov_spline_knots, &p->sp_m2, s))) return rc;
   }
-  CK(cudaMalloc((void**)&p->seed, sizeof(uint64_t)));
+  CK(palloc((void**)&p->seed, sizeof(uint64_t)));
   CK(cudaMemcpyAsync(p->seed, &d->seed, sizeof(uint64_t), cudaMemcpyHostToDevice, s));
   if (d->crn_normals) {
     const size_t nd = (size_t)J * p->sub_total * draws_per_substep(d->noises_off);
-    if ((rc = upload<double>(d->crn_normals, nd, &p->crn_tab, s))) return rc;
-    if ((rc = upload<double>(p->crn_u.data(), p->crn_u.size(), &p->crn_u_d, s))) return rc;
+    if ((rc = pupload<double>(d->crn_normals, nd, &p->crn_tab, s))) return rc;
+    if ((rc = pupload<double>(p->crn_u.data(), p->crn_u.size(), &p->crn_u_d, s))) return rc;
   }
   if (p->want_llike) {
     const size_t no = (size_t)p->R * (d->n_obs > 0 ? d->n_obs : 1);
-    CK(cudaMalloc((void**)&p->llike, no * sizeof(double)));
-    CK(cudaMalloc((void**)&p->ess, no * sizeof(double)));
+    CK(palloc((void**)&p->llike, no * sizeof(double)));
+    CK(palloc((void**)&p->ess, no * sizeof(double)));
     CK(cudaMemsetAsync(p->llike, 0, no * sizeof(double), s));
     CK(cudaMemsetAsync(p->ess, 0, no * sizeof(double), s));
   }
   if (p->mif) {
     const size_t nq = (size_t)(d->n_obs > 0 ? d->n_obs : 1) * p->Q;
-    CK(cudaMalloc((void**)&p->theta_hat, (size_t)p->R * p->Q * sizeof(double)));
-    CK(cudaMalloc((void**)&p->sd_init, (size_t)p->Q * sizeof(double)));
-    CK(cudaMalloc((void**)&p->sd_mut, nq * sizeof(double)));
-    CK(cudaMalloc((void**)&p->vt_add, nq * sizeof(double)));
-    CK(cudaMalloc((void**)&p->bart, (size_t)p->R * nq * sizeof(double)));
-    CK(cudaMalloc((void**)&p->vt, (size_t)p->R * nq * sizeof(double)));
+    CK(palloc((void**)&p->theta_hat, (size_t)p->R * p->Q * sizeof(double)));
+    CK(palloc((void**)&p->sd_init, (size_t)p->Q * sizeof(double)));
+    CK(palloc((void**)&p->sd_mut, nq * sizeof(double)));
+    CK(palloc((void**)&p->vt_add, nq * sizeof(double)));
+    CK(palloc((void**)&p->bart, (size_t)p->R * nq * sizeof(double)));
+    CK(palloc((void**)&p->vt, (size_t)p->R * nq * sizeof(double)));
     CK(cudaMemsetAsync(p->theta_hat, 0, (size_t)p->R * p->Q * sizeof(double), s));
     CK(cudaMemsetAsync(p->sd_init, 0, (size_t)p->Q * sizeof(double), s));
     CK(cudaMemsetAsync(p->sd_mut, 0, nq * sizeof(double), s));
@@ -692,38 +762,38 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
     CK(cudaMemsetAsync(p->bart, 0, (size_t)p->R * nq * sizeof(double), s));
     CK(cudaMemsetAsync(p->vt, 0, (size_t)p->R * nq * sizeof(double), s));
   }
-  if (p->want_anc) CK(cudaMalloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
-  if (p->want_xpred) CK(cudaMalloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
+  if (p->want_anc) CK(palloc((void**)&p->anc_hist, (size_t)d->n_obs * J * sizeof(uint32_t)));
+  if (p->want_xpred) CK(palloc((void**)&p->x_hist, (size_t)d->n_obs * M::S * J * sizeof(double)));
   if (p->want_anc && p->want_xpred && p->R == 1) {
     std::vector<int> idx;
     for (int n = 0; n < d->n_obs; ++n)
       if (p->weigh[n]) idx.push_back(n);
     p->n_data = (int)idx.size();
     if (!idx.empty()) {
-      int rc2 = upload<int>(idx.data(), idx.size(), &p->data_idx, s);
+      int rc2 = pupload<int>(idx.data(), idx.size(), &p->data_idx, s);
       if (rc2) return rc2;
     }
-    CK(cudaMalloc((void**)&p->traj_t, (size_t)(d->n_obs + 2) * sizeof(int)));
-    CK(cudaMalloc((void**)&p->traj_j, (size_t)(d->n_obs + 2) * sizeof(int)));
-    CK(cudaMalloc((void**)&p->traj_n, sizeof(int)));
-    CK(cudaMalloc((void**)&p->traj_x, (size_t)(d->n_obs + 2) * M::S * sizeof(double)));
+    CK(palloc((void**)&p->traj_t, (size_t)(d->n_obs + 2) * sizeof(int)));
+    CK(palloc((void**)&p->traj_j, (size_t)(d->n_obs + 2) * sizeof(int)));
+    CK(palloc((void**)&p->traj_n, sizeof(int)));
+    CK(palloc((void**)&p->traj_x, (size_t)(d->n_obs + 2) * M::S * sizeof(double)));
   }
   if (p->want_hat) {
     if (p->R != 1) return fail(PLOMGPU_EINVAL, "filtered summaries need a single run");
     if (!M::POP_SIZE_EQ_SUM_SV && !d->pop_size) return fail(PLOMGPU_EINVAL, "summaries of a remainder need pop_size");
-    CK(cudaMalloc((void**)&p->vals, (size_t)kHatVals * J * sizeof(double)));
+    CK(palloc((void**)&p->vals, (size_t)kHatVals * J * sizeof(double)));
     p->hat_rank[0] = (double)equal_weight_rank(J, 0.025);
     p->hat_rank[1] = (double)equal_weight_rank(J, 0.975);
-    CK(cudaMalloc((void**)&p->hat, (size_t)(d->n_obs + 1) * kHatQ * 3 * sizeof(double)));
-    CK(cudaMalloc((void**)&p->pred, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS * 2 * sizeof(double)));
+    CK(palloc((void**)&p->hat, (size_t)(d->n_obs + 1) * kHatQ * 3 * sizeof(double)));
+    CK(palloc((void**)&p->pred, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS * 2 * sizeof(double)));
     CK(cudaMemsetAsync(p->pred, 0, (size_t)(d->n_obs > 0 ? d->n_obs : 1) * M::N_TS * 2 * sizeof(double), s));
     if (d->pop_size) {
-      int rc2 = upload<double>(d->pop_size, (size_t)(d->n_obs + 1) * M::N_CAC, &p->pop, s);
+      int rc2 = pupload<double>(d->pop_size, (size_t)(d->n_obs + 1) * M::N_CAC, &p->pop, s);
       if (rc2) return rc2;
     }
     if (M::N_COV_TS > 0) {
       if (!d->cov_ts0) return fail(PLOMGPU_EINVAL, "summaries of observations with covariates need cov_ts0");
-      int rc3 = upload<double>(d->cov_ts0, (size_t)M::N_COV_TS * M::N_TS, &p->cov_ts0, s);
+      int rc3 = pupload<double>(d->cov_ts0, (size_t)M::N_COV_TS * M::N_TS, &p->cov_ts0, s);
       if (rc3) return rc3;
     }
   }
@@ -763,7 +833,7 @@ void plan_free(plomgpu_plan* p) {
                   p->traj_j, p->traj_n, p->traj_x, p->x0_cloud, p->mx, p->vol_slot, p->x0_slot, p->pop0,
                   p->fls_out};
   for (void* b : bufs)
-    if (b) cudaFree(b);
+    if (b) cudaFreeAsync(b, p->stream);
   if (p->acc_h) {
     if (p->direct) delete p->acc_h;
     else cudaFreeHost(p->acc_h);
@@ -782,9 +852,9 @@ int mif_group_tables(const plomgpu_mif_desc* mif, plomgpu_plan* p) {
   if ((proc_multi && !mif->proc_cac_slot) || (obs_multi && !mif->obs_ts_slot))
     return fail(PLOMGPU_EINVAL, "a slot of -2 needs its per-group table");
   int rc = PLOMGPU_OK;
-  if (proc_multi && (rc = upload<int>(mif->proc_cac_slot, (size_t)M::N_PAR_PROC * M::N_CAC, &p->proc_cslot, p->stream)))
+  if (proc_multi && (rc = pupload<int>(mif->proc_cac_slot, (size_t)M::N_PAR_PROC * M::N_CAC, &p->proc_cslot, p->stream)))
     return rc;
-  if (obs_multi && (rc = upload<int>(mif->obs_ts_slot, (size_t)M::N_PAR_OBS * M::N_TS, &p->obs_tslot, p->stream)))
+  if (obs_multi && (rc = pupload<int>(mif->obs_ts_slot, (size_t)M::N_PAR_OBS * M::N_TS, &p->obs_tslot, p->stream)))
     return rc;
   return PLOMGPU_OK;
 }
@@ -797,7 +867,7 @@ int mif_fls_tables(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mif, plomg
   if (mif->vol_slot && M::N_DRIFT > 0) {
     for (int i = 0; i < M::N_DRIFT * M::N_CAC; ++i)
       if (mif->vol_slot[i] < -1 || mif->vol_slot[i] >= Q) return fail(PLOMGPU_EINVAL, "bad vol_slot");
-    if ((rc = upload<int>(mif->vol_slot, (size_t)M::N_DRIFT * M::N_CAC, &p->vol_slot, s))) return rc;
+    if ((rc = pupload<int>(mif->vol_slot, (size_t)M::N_DRIFT * M::N_CAC, &p->vol_slot, s))) return rc;
   }
   if (mif->x0_slot) {
     if (!mif->pop0) return fail(PLOMGPU_EINVAL, "x0_slot needs pop0");
@@ -805,8 +875,8 @@ int mif_fls_tables(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mif, plomg
       if (mif->x0_slot[w] < -1 || mif->x0_slot[w] >= Q) return fail(PLOMGPU_EINVAL, "bad x0_slot");
     for (int c = 0; c < M::N_CAC; ++c)
       if (!(mif->pop0[c] > 0.0)) return fail(PLOMGPU_EINVAL, "pop0 must be > 0");
-    if ((rc = upload<int>(mif->x0_slot, (size_t)M::OFF_INC, &p->x0_slot, s))) return rc;
-    if ((rc = upload<double>(mif->pop0, (size_t)M::N_CAC, &p->pop0, s))) return rc;
+    if ((rc = pupload<int>(mif->x0_slot, (size_t)M::OFF_INC, &p->x0_slot, s))) return rc;
+    if ((rc = pupload<double>(mif->pop0, (size_t)M::N_CAC, &p->pop0, s))) return rc;
   }
   if (mif->prior && (!mif->prior_kind || !mif->prior_lo || !mif->prior_hi || !mif->prior_finv))
     return fail(PLOMGPU_EINVAL, "the prior patch needs prior_kind / prior_lo / prior_hi / prior_finv");
@@ -825,7 +895,7 @@ int mif_fls_tables(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mif, plomg
       h.prior_hi[q] = mif->prior_hi[q];
       memcpy(&h.prior_finv[q], &mif->prior_finv[q], sizeof(plomrt::BackTransform));
     }
-    if ((rc = upload<MifTables>(&h, 1, &p->mx, s))) return rc;
+    if ((rc = pupload<MifTables>(&h, 1, &p->mx, s))) return rc;
     CK(cudaStreamSynchronize(s));
   }
   if (p->fls_mask) {
@@ -841,7 +911,7 @@ int mif_fls_tables(const plomgpu_smc_desc* d, const plomgpu_mif_desc* mif, plomg
         if (d->filter && any) p->fls_n = n;
       }
     }
-    CK(cudaMalloc((void**)&p->fls_out, (size_t)p->R * Q * sizeof(double)));
+    CK(palloc((void**)&p->fls_out, (size_t)p->R * Q * sizeof(double)));
     std::vector<double> nanv((size_t)p->R * Q, NAN);
     CK(cudaMemcpy(p->fls_out, nanv.data(), nanv.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
@@ -933,8 +1003,9 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
     delete p;
     return fail(PLOMGPU_ECUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
+  g_alloc_stream = p->stream;
   if (want_final) {
-    e = cudaMalloc((void**)&p->x_final, (size_t)M::S * d->J * sizeof(double));
+    e = palloc((void**)&p->x_final, (size_t)M::S * d->J * sizeof(double));
     if (e != cudaSuccess) {
       plan_free(p);
       return fail(PLOMGPU_ENOMEM, "x_final allocation failed");
@@ -942,10 +1013,10 @@ int plan_create(const plomgpu_smc_desc* d, plomgpu_plan** out, bool want_anc, bo
   }
   if (mif) {
     int rc2;
-    if ((rc2 = upload<plomrt::BackTransform>((const plomrt::BackTransform*)mif->theta_bt, (size_t)mif->n_theta,
+    if ((rc2 = pupload<plomrt::BackTransform>((const plomrt::BackTransform*)mif->theta_bt, (size_t)mif->n_theta,
                                              &p->theta_bt, p->stream)) ||
-        (rc2 = upload<int>(mif->proc_slot, (size_t)(M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 0), &p->proc_slot, p->stream)) ||
-        (rc2 = upload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream)) ||
+        (rc2 = pupload<int>(mif->proc_slot, (size_t)(M::N_PAR_PROC > 0 ? M::N_PAR_PROC : 0), &p->proc_slot, p->stream)) ||
+        (rc2 = pupload<int>(mif->obs_slot, (size_t)(M::N_PAR_OBS > 0 ? M::N_PAR_OBS : 0), &p->obs_slot, p->stream)) ||
         (rc2 = mif_group_tables(mif, p)) || (rc2 = mif_fls_tables(d, mif, p))) {
       std::string keep = g_err;
       plan_free(p);
@@ -1151,6 +1222,13 @@ int plomgpu_smc_run(const plomgpu_smc_desc* d, plomgpu_smc_result* r) {
   g_err = keep;
   r->status = rc;
   return rc;
+}
+
+int plomgpu_release_memory(void) {
+  cudaMemPool_t mp = nullptr;
+  CK(plan_mem_pool(&mp));
+  CK(cudaMemPoolTrimTo(mp, 0));
+  return PLOMGPU_OK;
 }
 
 double plomgpu_debug_fail_boundary(double thresh) { return fail_boundary(thresh); }

@@ -87,7 +87,7 @@ API_SYMBOLS = ['plomgpu_get_model_info', 'plomgpu_draws_per_substep', 'plomgpu_s
                'plomgpu_plan_create_ex', 'plomgpu_plan_propagate_time',
                'plomgpu_plan_update', 'plomgpu_plan_launch', 'plomgpu_plan_results', 'plomgpu_plan_stream',
                'plomgpu_plan_kernel_count', 'plomgpu_plan_destroy', 'plomgpu_debug_systematic_points',
-               'plomgpu_debug_fail_boundary',
+               'plomgpu_debug_fail_boundary', 'plomgpu_release_memory',
                'plomgpu_resample_noalloc', 'plomgpu_last_error', 'plomgpu_batch_create', 'plomgpu_batch_launch',
                'plomgpu_batch_results', 'plomgpu_batch_stream', 'plomgpu_batch_config', 'plomgpu_batch_destroy',
                'plomgpu_batch_run', 'plomgpu_mif_create', 'plomgpu_mif_iteration', 'plomgpu_mif_destroy',
@@ -296,6 +296,10 @@ class Engine(object):
 
     def draws_per_substep(self, noises_off):
         return self.lib.plomgpu_draws_per_substep(noises_off)
+
+    def release_memory(self):
+        """Returns the unused memory of the library's plan memory pool (current device) to the driver."""
+        check(self.lib, self.lib.plomgpu_release_memory())
 
     def particle_values(self, problem, X, rows):
         """[n_hat + n_ts][P]: summarised quantities then observation variances of particles X ([S][P]),
