@@ -474,7 +474,7 @@ int enqueue_filter(plomgpu_plan* p) {
   k_sys_tables<<<(p->n_obs * R + 63) / 64, 64, 0, s>>>(J, p->n_obs, R, p->seed, 0u, p->crn_u_d, -1.0, p->sys, p->acc);
   ++kernels;
   {
-    const size_t total = (size_t)M::OFF_INC * RJ;
+    const size_t total = (size_t)M::S * RJ;
     const int g = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
     if (p->x0_cloud) k_init_cloud<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0_cloud, (int)RJ, (T*)p->X[0]);
     else k_init_state<T><<<g > 0 ? g : 1, 256, 0, s>>>(p->x0, (int)RJ, (T*)p->X[0]);

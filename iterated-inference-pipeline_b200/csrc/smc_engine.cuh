@@ -1300,21 +1300,23 @@ __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict_
 }
 
 // ------------------------------------------------------------------ helpers
+// the initial particles: x0 in every particle, incidences zero (the time-0
+// summaries read them; the buffers come from a pool and hold old values)
 template <class T>
 __global__ void k_init_state(const double* __restrict__ x0, int J, T* __restrict__ X) {
-  const size_t total = (size_t)M::OFF_INC * J;
+  const size_t total = (size_t)M::S * J;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
     const int w = (int)(i / J);
-    X[i] = (T)x0[w];
+    X[i] = (w < M::OFF_INC) ? (T)x0[w] : T(0);
   }
 }
 
-// initial particles given one by one: cloud [OFF_INC][J] (FP64)
+// initial particles given one by one: cloud [OFF_INC][J] (FP64), incidences zero
 template <class T>
 __global__ void k_init_cloud(const double* __restrict__ cloud, int J, T* __restrict__ X) {
-  const size_t total = (size_t)M::OFF_INC * J;
+  const size_t total = (size_t)M::S * J, n_cloud = (size_t)M::OFF_INC * J;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x)
-    X[i] = (T)cloud[i];
+    X[i] = (i < n_cloud) ? (T)cloud[i] : T(0);
 }
 
 template <class T>
