@@ -99,7 +99,7 @@ struct plomgpu_server {
   long long* d_live = nullptr;  // its live-request table [kServeLive]
   int task_budget = 64;         // tasks a CTA of the tiled loop runs before it returns
   int bt = 256, grid = 0;
-  long long idle_limit = 20000;
+  long long idle_limit = 20000;  // microseconds a loop CTA waits for work before it returns
   // base problem (host copies; every request shares it)
   plomgpu_smc_desc base{};
   std::vector<int> n_sub_h;

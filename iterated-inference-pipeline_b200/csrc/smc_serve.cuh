@@ -6,8 +6,11 @@
 // flag), both at system scope.  Each CTA takes the next request as soon as
 // it finishes one, so requests that arrive while others run start on the
 // CTAs that free up (continuous batching).  Every wait is bounded: a CTA that
-// finds no request for `idle_limit` polls returns, and the host relaunches
-// the loop when new requests arrive.
+// finds no request for `idle_limit` microseconds (the GPU's global timer)
+// returns, and the host relaunches the loop when new requests arrive.  The
+// bound is in time, not in polls: polls of host memory by many idle CTAs
+// slow each other down, and a count of them kept a grown loop resident (and
+// its SMs from other kernels) for seconds after its last request.
 //
 // Callers: concurrent pmcmc chains evaluating one likelihood per iteration
 // (model_builder/C/pmcmc/pmcmc.c:186-266, run_propag at pmcmc.c:24-37).
@@ -19,6 +22,13 @@
 #include "smc_batch.cuh"
 
 namespace plomgpu {
+
+// nanoseconds of the GPU's global timer
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 constexpr int kServeParCac = (M::N_PAR_PROC * M::N_CAC) > 0 ? (M::N_PAR_PROC * M::N_CAC) : 1;
 constexpr int kServeParTs = (M::N_PAR_OBS * M::N_TS) > 0 ? (M::N_PAR_OBS * M::N_TS) : 1;
@@ -68,6 +78,7 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
     if (threadIdx.x == 0) {
       long long got = -1;
       long long spins = 0;
+      const unsigned long long t_idle = global_ns();
       for (;;) {
         if ((spins & 255) == 0 && stop_ref.load(cuda::memory_order_acquire)) break;
         const unsigned long long t = tail_ref.load(cuda::memory_order_acquire);
@@ -79,7 +90,8 @@ __global__ void __launch_bounds__(BT) k_serve(const BatchArgs<T> a, ServeSlot* s
           }
           continue;
         }
-        if (++spins > idle_limit) break;
+        ++spins;
+        if (global_ns() - t_idle > (unsigned long long)idle_limit * 1000ull) break;
         __nanosleep(1000);
       }
       s_req = got;
@@ -262,7 +274,7 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
       const int lane = threadIdx.x;
       if (lane == 0) s_off = -1;
       __syncwarp();
-      long long spins = 0;
+      const unsigned long long t_idle = global_ns();
       unsigned backoff = 128u;  // ns between polls that find nothing, doubling up to 8 us
       for (;;) {
         int stop = 0;
@@ -348,7 +360,7 @@ __global__ void __launch_bounds__(BT) k_serve_tiles(const BatchArgs<T> a, ServeS
         }
         // nothing to do now: while requests are live the wait is long (their
         // serial parts run on one CTA), else short; bounded either way
-        if (++spins > (any_live ? idle_limit * 2500 : idle_limit)) break;
+        if (global_ns() - t_idle > (unsigned long long)idle_limit * (any_live ? 2500000ull : 1000ull)) break;
         __nanosleep(backoff);
         backoff = backoff < 8192u ? 2u * backoff : 8192u;
       }
