@@ -207,17 +207,25 @@ def replica_throughput(psteps_per_rank, world, ms_step):
     return psteps_per_rank * world / (ms_step / 1000.0)
 
 
-def ncu_issue(workload):
+def ncu_issue(workload, J=None, avg_launch_ms=None, sm_mhz=None):
     """Issue-side utilisation of the propagate kernel from the committed ncu summary (the bound that
-    binds: the full-noise step is instruction-issue bound, not HBM bound)."""
+    binds: the full-noise step is instruction-issue bound, not HBM bound), and its issue roofline for
+    this run: the captured warp instructions per particle x J over 148 SMs x 4 schedulers x the SM
+    clock (one warp instruction per scheduler per cycle), against the measured launch time."""
     path = os.path.join(ROOT, 'profiles', 'k_propagate_%s.json' % workload)
     try:
         with open(path) as f:
             d = json.load(f)
-        return {'issue_slots_active_pct': d['issue_active_pct'], 'ipc': d['ipc'],
-                'warps_active_per_sm': d['warps_active_per_sm'],
-                'source': 'profiles/k_propagate_%s.md (ncu capture of %s, not this run)' % (workload,
-                                                                                        d.get('captured', '?'))}
+        out = {'issue_slots_active_pct': d['issue_active_pct'], 'ipc': d['ipc'],
+               'warps_active_per_sm': d['warps_active_per_sm'],
+               'source': '%s (ncu capture of %s, not this run)' % (
+                   d.get('summary', 'profiles/k_propagate_%s.md' % workload), d.get('captured', '?'))}
+        if J and avg_launch_ms and 'warp_instructions_per_particle' in d:
+            clock = (sm_mhz or 1965.0) * 1e6
+            floor_ms = d['warp_instructions_per_particle'] * J / (148 * 4 * clock) * 1e3
+            out.update({'floor_ms': floor_ms, 'frac': floor_ms / avg_launch_ms,
+                        'floor': 'warp instructions / (148 SMs x 4 schedulers x SM clock)'})
+        return out
     except (OSError, KeyError, ValueError):
         return None
 
@@ -637,7 +645,7 @@ def main():
                          'kernel': 'k_propagate', 'bytes_per_particle_step': B,
                          'avg_launch_ms': avg_prop_ms, 'peak_kind': peak_kind,
                          'propagate_share': tot_prop / (ms_total / args.steps),
-                         'issue': ncu_issue(args.workload)},
+                         'issue': ncu_issue(args.workload, prob.J, avg_prop_ms, clk.summary()['sm_mhz'])},
             'clocks': clk.summary(),
             'e2e': {'value': e2e_value, 'unit': 'particle-steps/s', 'h2d_bytes_per_step': h2d,
                     'd2h_bytes_per_step': d2h, 'call': 'plomgpu_smc_run (host buffers, one-shot)'},
