@@ -69,7 +69,7 @@ def nvcc_command(name, S, out=None, verbose_ptxas=False):
     smem = 1 if S > SMEM_STATE_WORDS else 0
     # single precision: flush denormals, hardware-rate sqrt and division, and the
     # special-function-unit forms of exp / log / sin / cos / pow (the FP32 path
-    # is judged statistically; its quantities that cancel are computed in
+    # is assessed statistically; its quantities that cancel are computed in
     # double, and FP64 arithmetic is unaffected).  The approximate forms took
     # the SEIR 20x2 sde step from 0.529 to 0.514 ms and its psr step from 12.4
     # to 11.1 ms per interval.

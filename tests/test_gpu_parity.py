@@ -184,7 +184,7 @@ def test_plan_reuse_matches_one_shot():
 def test_fp32_precision_bias_with_common_draws():
     """FP32 state vs the FP64 oracle on the same injected draws.  A single path
     comparison diverges once an ancestor flips at the last bits of a weight, so
-    the precision error is judged as the bias over replicates: the signed mean
+    the precision error is assessed as the bias over replicates: the signed mean
     difference stays well inside 0.5 nats, as does the median absolute one."""
     eng = models.engine('sir')
     orc = models.build_oracle('sir')
