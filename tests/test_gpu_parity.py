@@ -217,6 +217,21 @@ def test_crn_parity_shared_memory_state(noises_off):
     assert g.loglik == pytest.approx(o.loglik, rel=1e-9)
 
 
+def test_concentrated_weights_shared_memory_state_match_oracle():
+    """seir20x2 at J = 4000 (tiles of 128 particles): the weights of its 20 series concentrate on a
+    few particles, so single tiles take more than 8 tiles' worth of systematic points and are
+    finished by the second resampling launch; ancestors still equal the oracle's (FP64 Philox)."""
+    eng = models.engine('seir20x2')
+    orc = models.build_oracle('seir20x2')
+    p = models.make_problem('seir20x2', J=4000, dt=1.0, precision=64, seed=9, nb_obs=12)
+    g = eng.smc(p, ancestors=True)
+    o = orc.smc(p, ancestors=True)
+    np.testing.assert_array_equal(g.ancestors, o.ancestors)
+    assert g.loglik == pytest.approx(o.loglik, rel=1e-9)
+    per_tile = [np.bincount(a // 128, minlength=4000 // 128 + 1).max() for a in g.ancestors]
+    assert max(per_tile) > 8 * 128
+
+
 def test_philox_fp64_shared_memory_state_matches_oracle():
     """The shared-memory-state kernel consumes the same Philox blocks as the oracle (FP64)."""
     eng = models.engine('seir20x2')
