@@ -94,6 +94,7 @@ static_assert(kTeam == 1 || kTeam == 2 || kTeam == 4 || kTeam == 8 || kTeam == 1
 constexpr int kBtRes = kSmem ? kBtProp : 256;
 constexpr int kIptRes = kSmem ? 1 : 4;
 constexpr int kTileRes = kBtRes * kIptRes;
+static_assert(kTileRes <= kMaxTile, "k_resample_heavy stages a tile in shared memory");
 
 int variant_of(int noises_off) { return noises_off & 3; }
 bool drift_on(int noises_off) { return M::N_DRIFT > 0 && !(noises_off & PLOMGPU_NO_DRIFT); }
@@ -1424,6 +1425,7 @@ namespace {
 constexpr int kNoAllocMaxJ = 1 << 18;  // largest particle count the fixed scratch serves
 constexpr int kNoAllocBt = 256, kNoAllocIpt = 4, kNoAllocTile = kNoAllocBt * kNoAllocIpt;
 constexpr int kNoAllocTiles = (kNoAllocMaxJ + kNoAllocTile - 1) / kNoAllocTile;
+static_assert(kNoAllocTile <= kMaxTile, "k_resample_heavy stages a tile in shared memory");
 
 struct NoAllocScratch {
   LseAcc part[kNoAllocTiles];

@@ -1251,17 +1251,24 @@ __global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw,
                             heavy + (size_t)r * ntiles, sc);
 }
 
+// largest tile of the weighting / resampling launches (a listed tile's
+// cumulative weights are staged in shared memory)
+constexpr int kMaxTile = 1024;
+
 // The points of the tiles listed by resample_tile, spread evenly over all
-// threads (each a run of consecutive listed points): the first i of the
-// tile with C_i >= point, from C in global memory.
+// blocks: a block takes a contiguous share of the listed points, stages the
+// cumulative weights of each listed tile its share touches in shared memory
+// (one coalesced read) and gives each thread a run of consecutive points:
+// the first i of the tile with C_i >= point.
 template <int BT>
 __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict__ C, int J, int ntiles, int tile,
                                                        const StepState* st, const SysTable* tab, int tab_stride,
                                                        const HeavyTile* __restrict__ heavy, uint32_t* __restrict__ anc,
                                                        uint32_t* __restrict__ anc_hist) {
   __shared__ plomrt::SysSeg seg[plomrt::SYS_MAX_SEG];
+  __shared__ double sc[kMaxTile];
   __shared__ unsigned long long s_h;
-  __shared__ int s_ns;
+  __shared__ int s_ns, s_e;
   const int r = blockIdx.y;
   st += r;
   tab += (size_t)r * tab_stride;
@@ -1274,28 +1281,38 @@ __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict_
   const long long total = (long long)(s_h & 0xffffffffull);
   const int ns = s_ns;
   if (nh == 0) return;
+  const long long per_blk = (total + gridDim.x - 1) / gridDim.x;
+  long long q0 = (long long)blockIdx.x * per_blk;
+  const long long q1 = min(total, q0 + per_blk);
+  if (q0 >= q1) return;
   C += (size_t)r * J;
   heavy += (size_t)r * ntiles;
   anc += (size_t)r * J;
   if (anc_hist) anc_hist += (size_t)r * J;
   for (int i = threadIdx.x; i < ns; i += BT) seg[i] = tab->seg[i];
-  __syncthreads();
-  const long long nthr = (long long)gridDim.x * BT;
-  const long long per = (total + nthr - 1) / nthr;
-  long long q = ((long long)blockIdx.x * BT + threadIdx.x) * per;
-  const long long qe = min(total, q + per);
-  if (q >= qe) return;
-  int lo = 0, hi = nh - 1;  // the listed tile holding point q: the last with off <= q
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if ((long long)__ldg(&heavy[mid].off) <= q) lo = mid; else hi = mid - 1;
+  if (threadIdx.x == 0) {  // the listed tile holding point q0: the last with off <= q0
+    int lo = 0, hi = nh - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((long long)__ldg(&heavy[mid].off) <= q0) lo = mid; else hi = mid - 1;
+    }
+    s_e = lo;
   }
-  for (int e = lo; q < qe && e < nh; ++e) {
+  __syncthreads();
+  for (int e = s_e; q0 < q1 && e < nh; ++e) {
     const HeavyTile h = heavy[e];
-    const int ja = h.jlo + (int)(q - h.off);
-    const int jb = (int)min((long long)h.jhi, (long long)ja + (qe - q));
-    place_points(seg, ns, ja, jb, C + (size_t)h.b * tile, h.n_in, h.b * tile, anc, anc_hist);
-    q += jb - ja;
+    const long long e1 = min(q1, (long long)h.off + (h.jhi - h.jlo));  // this block's points of tile e: [q0, e1)
+    for (int i = threadIdx.x; i < h.n_in; i += BT) sc[i] = __ldg(C + (size_t)h.b * tile + i);
+    __syncthreads();
+    const long long np = e1 - q0;
+    const long long per = (np + BT - 1) / BT;
+    const long long qa = q0 + threadIdx.x * per;
+    const long long qb = min(e1, qa + per);
+    if (qa < qb)
+      place_points(seg, ns, h.jlo + (int)(qa - h.off), h.jlo + (int)(qb - h.off), sc, h.n_in, h.b * tile, anc,
+                   anc_hist);
+    __syncthreads();  // sc of the next listed tile
+    q0 = e1;
   }
 }
 
