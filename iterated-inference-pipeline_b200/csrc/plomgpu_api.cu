@@ -14,6 +14,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <utility>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -325,6 +326,27 @@ int pupload(const U* h, size_t n, U** d, cudaStream_t s) {
   return PLOMGPU_OK;
 }
 
+// A kernel of the per-interval chain (propagate, weighting, resampling),
+// launched with programmatic stream serialisation: it may be scheduled while
+// the previous kernel of the stream drains, and waits (griddepcontrol.wait,
+// wait_for_previous_kernel) before it reads that kernel's results.  Saves
+// the launch gap at each of the four kernel boundaries of an interval.
+template <class... KArgs, class... Args>
+cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                           Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <class T>
 using PropKernel = void (*)(const Tables<T>, const StepArgs);
 
@@ -537,7 +559,7 @@ int enqueue_filter(plomgpu_plan* p) {
       o.acc = p->acc;
       k_propagate_ode<T, kBtOde><<<(unsigned)((RJ + kBtOde - 1) / kBtOde), kBtOde, 0, s>>>(tb, a, o);
     } else {
-      kp.k<<<gprop, kp.bt, smem, s>>>(tb, a);
+      CK(launch_chained(kp.k, dim3(gprop), dim3(kp.bt), smem, s, tb, a));
     }
     if (p->timing) CK(cudaEventRecordWithFlags(p->ev[2 * n + 1], s, cudaEventRecordExternal));
     ++kernels;
@@ -545,9 +567,9 @@ int enqueue_filter(plomgpu_plan* p) {
     if (p->mif) th_cur ^= 1;
     if (a.weigh) {
       const int nxt = (anc_cur == 0) ? 1 : 0;
-      k_weight_tiles<T, kBtRes, kIptRes><<<dim3(p->weight_blocks, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->ntiles, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n, p->llike,
-          p->ess, p->n_obs);
+      CK(launch_chained(&k_weight_tiles<T, kBtRes, kIptRes>, dim3(p->weight_blocks, R), dim3(kBtRes), 0, s,
+                        (const T*)p->lw, J, p->ntiles, p->fail_b, p->log_like_min, p->part, p->P, p->st, p->acc, n,
+                        p->llike, p->ess, p->n_obs));
       ++kernels;
       if (p->mif) {
         k_mif_moments<T, 256><<<dim3(p->Q, R), 256, 0, s>>>((const T*)p->lw, (const T*)p->theta[th_cur], J, R,
@@ -556,12 +578,14 @@ int enqueue_filter(plomgpu_plan* p) {
         ++kernels;
       }
       if (p->want_hat) kernels += enqueue_hat<T>(p, (const T*)a.X_next, n + 1, a.cov_ts, a.t_obs, true, s);
-      k_resample_tiles<T, kBtRes, kIptRes><<<dim3(p->ntiles, R), kBtRes, 0, s>>>(
-          (const T*)p->lw, J, p->fail_b, p->part, p->P, p->st, p->sys + n, p->n_obs, p->anc[nxt],
-          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr, p->C, p->heavy);
-      k_resample_heavy<256><<<dim3(p->heavy_blocks, R), 256, 0, s>>>(
-          p->C, J, p->ntiles, kTileRes, p->st, p->sys + n, p->n_obs, p->heavy, p->anc[nxt],
-          p->anc_hist ? p->anc_hist + (size_t)n * J : nullptr);
+      CK(launch_chained(&k_resample_tiles<T, kBtRes, kIptRes>, dim3(p->ntiles, R), dim3(kBtRes), 0, s,
+                        (const T*)p->lw, J, p->fail_b, (const LseAcc*)p->part, (const double*)p->P, p->st,
+                        (const SysTable*)(p->sys + n), p->n_obs, p->anc[nxt],
+                        p->anc_hist ? p->anc_hist + (size_t)n * J : (uint32_t*)nullptr, p->C, p->heavy));
+      CK(launch_chained(&k_resample_heavy<256>, dim3(p->heavy_blocks, R), dim3(256), 0, s, (const double*)p->C, J,
+                        p->ntiles, kTileRes, (const StepState*)p->st, (const SysTable*)(p->sys + n), p->n_obs,
+                        (const HeavyTile*)p->heavy, p->anc[nxt],
+                        p->anc_hist ? p->anc_hist + (size_t)n * J : (uint32_t*)nullptr));
       kernels += 2;
       if (p->want_hat) {
         k_pred_res<256><<<M::N_TS, 256, 0, s>>>(p->vals, p->anc[nxt], J, a.y, p->pred + (size_t)n * M::N_TS * 2);

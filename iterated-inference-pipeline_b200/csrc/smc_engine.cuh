@@ -33,6 +33,12 @@ namespace plomgpu {
 using plomgen::Model;
 typedef Model M;
 
+// Launched with programmatic stream serialisation (launch_chained on the
+// host), a kernel may start while the previous kernel of the stream still
+// runs; it waits here, before it reads anything that kernel writes.  A
+// kernel launched without it passes straight through.
+__device__ __forceinline__ void wait_for_previous_kernel() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------ state stores
 template <class T, int S>
 struct RegState {
@@ -619,6 +625,7 @@ __global__ void __launch_bounds__(BT, PLOM_TEAM_MIN_BLOCKS) k_propagate_team(con
   }
   for (int i = threadIdx.x; i < M::N_PAR_PROC * M::N_CAC; i += BT) s_par[i] = tb.par_cac[i];
   __syncthreads();
+  wait_for_previous_kernel();
   const int J = tb.J;
   const size_t RJ = (size_t)tb.R * J;
   const int lp = threadIdx.x / TP;
@@ -1040,6 +1047,7 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   __shared__ LseAcc sh[BT / 32];
   __shared__ double shd[BT / 32];
   __shared__ bool last;
+  wait_for_previous_kernel();
   {
     const int r = blockIdx.y;
     lw += (size_t)r * J;
@@ -1096,7 +1104,8 @@ template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, boo
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   static_assert(PPT == 1 || !SMEM, "one particle per shared-memory state column");
-  propagate_tables<T, BT>(tb, smem_raw, true);
+  propagate_tables<T, BT>(tb, smem_raw, true);  // tables no kernel of the filter writes
+  wait_for_previous_kernel();
   const size_t RJ = (size_t)tb.R * tb.J;
   const size_t g0 = (size_t)blockIdx.x * BT * PPT + threadIdx.x;  // particle of all runs
 #pragma unroll
@@ -1243,6 +1252,7 @@ __global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw,
                                                        uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist,
                                                        double* __restrict__ C, HeavyTile* heavy) {
   __shared__ TileScratch<BT, IPT> sc;
+  wait_for_previous_kernel();
   const int ntiles = gridDim.x;
   const int r = blockIdx.y;
   resample_tile<T, BT, IPT>(lw + (size_t)r * J, J, fail_b, part + (size_t)r * ntiles, P + (size_t)r * (ntiles + 1),
@@ -1269,6 +1279,7 @@ __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict_
   __shared__ double sc[kMaxTile];
   __shared__ unsigned long long s_h;
   __shared__ int s_ns, s_e;
+  wait_for_previous_kernel();
   const int r = blockIdx.y;
   st += r;
   tab += (size_t)r * tab_stride;
