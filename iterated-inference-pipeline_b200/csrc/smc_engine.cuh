@@ -38,9 +38,6 @@ typedef Model M;
 // runs; it waits here, before it reads anything that kernel writes.  A
 // kernel launched without it passes straight through.
 __device__ __forceinline__ void wait_for_previous_kernel() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-// Lets the next chained kernel be scheduled once every block of this one has
-// started (it still waits for this kernel's completion before reading).
-__device__ __forceinline__ void release_next_kernel() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // ------------------------------------------------------------------ state stores
 template <class T, int S>
@@ -1050,7 +1047,6 @@ __global__ void __launch_bounds__(BT) k_weight_tiles(const T* __restrict__ lw, i
   __shared__ LseAcc sh[BT / 32];
   __shared__ double shd[BT / 32];
   __shared__ bool last;
-  release_next_kernel();
   wait_for_previous_kernel();
   {
     const int r = blockIdx.y;
@@ -1108,7 +1104,6 @@ template <class T, int V, bool DRIFT, bool CRN, bool SMEM, bool MIF, int BT, boo
 __global__ void __launch_bounds__(BT) k_propagate(const Tables<T> tb, const StepArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   static_assert(PPT == 1 || !SMEM, "one particle per shared-memory state column");
-  release_next_kernel();
   propagate_tables<T, BT>(tb, smem_raw, true);  // tables no kernel of the filter writes
   wait_for_previous_kernel();
   const size_t RJ = (size_t)tb.R * tb.J;
@@ -1257,7 +1252,6 @@ __global__ void __launch_bounds__(BT) k_resample_tiles(const T* __restrict__ lw,
                                                        uint32_t* __restrict__ anc, uint32_t* __restrict__ anc_hist,
                                                        double* __restrict__ C, HeavyTile* heavy) {
   __shared__ TileScratch<BT, IPT> sc;
-  release_next_kernel();
   wait_for_previous_kernel();
   const int ntiles = gridDim.x;
   const int r = blockIdx.y;
@@ -1285,7 +1279,6 @@ __global__ void __launch_bounds__(BT) k_resample_heavy(const double* __restrict_
   __shared__ double sc[kMaxTile];
   __shared__ unsigned long long s_h;
   __shared__ int s_ns, s_e;
-  release_next_kernel();
   wait_for_previous_kernel();
   const int r = blockIdx.y;
   st += r;
