@@ -713,7 +713,16 @@ int plan_build(const plomgpu_smc_desc* d, plomgpu_plan* p) {
   CK(palloc((void**)&p->P, (size_t)p->R * (p->ntiles + 1) * sizeof(double)));
   CK(palloc((void**)&p->heavy, (size_t)p->R * p->ntiles * sizeof(HeavyTile)));
   p->heavy_blocks = std::min(p->ntiles, 2 * 148);
-  p->weight_blocks = std::min(p->ntiles, 4 * 148);
+  // the weighting launch in one wave: its blocks loop over the tiles, and a
+  // second wave would repeat a block's whole share (256-thread blocks of 80
+  // registers: 3 per SM, so 4 x 148 blocks took 1.33 waves)
+  {
+    int dev = 0, sms = 148, per_sm = 1;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_weight_tiles<T, kBtRes, kIptRes>, kBtRes, 0));
+    p->weight_blocks = std::max(1, std::min(p->ntiles, std::max(1, per_sm) * sms));
+  }
   CK(palloc((void**)&p->sys, (size_t)p->R * p->n_obs * sizeof(SysTable)));
   CK(palloc((void**)&p->st, (size_t)p->R * sizeof(StepState)));
   CK(palloc((void**)&p->acc, (size_t)p->R * sizeof(FilterAcc)));
